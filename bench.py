@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark of the FDTD step: Gvoxel-updates/s and the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl virs|reference]
+
+One step = one time step of the simulation over the whole grid.  The default
+workload is the large hall, 1024x768x512 FP32 voxels (402.7 M) with two
+3-section absorbing materials, one Gaussian-pulse source and 8 receivers;
+all fields (1.6 GB each) are far larger than the 126 MB L2, so no flush is
+needed between steps.  With --gpus N under torchrun every rank runs its own
+hall (independent replicas, no collective on the data path; weak scaling);
+the time is the maximum over ranks.
+
+The JSON line carries:
+  value       Gvoxel-updates/s of the device-resident run (virs_run, CUDA
+              graph), inputs already in HBM
+  e2e         the same through virs_run_host with pinned host buffers: the
+              step's source samples in and the receiver samples out are
+              copied inside the timed region
+  roofline    algorithmic bytes of the stencil kernel (13 B per voxel
+              update in FP32: p 4 + p^{n-1} 4 + p^{n+1} 4 + cell code 1) over
+              its CUDA-event duration, against the measured HBM copy
+              bandwidth of MEASURED_PEAKS.json
+  cpu_baseline  the CPU oracle's FP32 step (OpenMP, all host threads) on a
+              crop of the hall
+  variants    the BF16-storage form of the same hall
+
+--impl reference times the reference's CPU implementation of this path.
+The reference's own CPU build cannot be compiled here (oneTBB, Embree,
+tinyobjloader, kfr, AudioFile are absent), so this arm runs the CPU
+restatement of its step (oracle/), on all host threads, on a crop of the
+same hall sized so that the run ends within a few minutes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_F32 = 13.0   # per voxel update: p 4 + p^{n-1} 4 + p^{n+1} 4 + code 1
+BYTES_16 = 7.0     # 16-bit storage: 2 + 2 + 2 + 1
+METRIC = "Gvoxel-updates/s"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---- clocks -------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.path:
+            return {"unavailable": "nvidia-smi not runnable"}
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"unavailable": "no samples"}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3][1:5]) if v.lower() == "active"})
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+# ---- the CUDA path ----------------------------------------------------------------
+
+def gpu_uuid(dev):
+    import torch
+    u = str(torch.cuda.get_device_properties(dev).uuid)
+    return u if u.startswith("GPU-") else "GPU-" + u
+
+
+def time_run(sim, steps, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.run(steps, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
+    """Warm up, then time K steps: device-resident graph run, a per-kernel
+    CUDA-event pass, and (optionally) the end-to-end host run."""
+    import torch
+    from virs_b200 import scenes
+    total = args.warmup + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
+    sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
+    sim.run(args.warmup, stream.cuda_stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    with Clocks(gpu_uuid(dev)) as clk:
+        ms = time_run(sim, args.steps, stream)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    out = {"ms": ms, "clocks": clk.summary(), "meta": meta}
+    # per-kernel events over K' steps (no graph; events around each stencil launch)
+    if args.kernel_steps:
+        sim.set_timing(True)
+        sim.run(args.kernel_steps, stream.cuda_stream)
+        sim.synchronize()
+        t = sim.timing()
+        sim.set_timing(False)
+        out["kernel_ms"] = t.step_kernel_ms / max(t.step_launches, 1)
+    if want_e2e:
+        nsrc, nrcv = len(sc.src_pos), len(sc.rcv_pos)
+        first = int(sim.info().steps_done)
+        sig = torch.empty((nsrc, args.steps), dtype=torch.float32, pin_memory=True)
+        sig.copy_(torch.from_numpy(np.ascontiguousarray(sc.src_sig[:, first:first + args.steps])))
+        ir = torch.empty((nrcv, args.steps), dtype=torch.float32, pin_memory=True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        sim.run_host_ptr(args.steps, sig.data_ptr(), ir.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        out["e2e_ms"] = ems
+        out["e2e_wall_ms"] = wall
+        out["h2d"] = 4 * nsrc
+        out["d2h"] = 4 * nrcv
+        out["ir_finite"] = bool(torch.isfinite(ir).all())
+    sim.close()
+    return out
+
+
+def cpu_sample(shape, steps_budget_s, threads):
+    """The oracle's FP32 step on a crop of the hall (same x, y extent, fewer
+    planes), timed on the host; returns (Gvox/s, description)."""
+    import oracle
+    from virs_b200 import scenes
+    sys.path.insert(0, str(ROOT / "tests"))
+    from helpers import oracle_grid, oracle_scene
+    oracle.set_threads(threads)
+    nx, ny, nz = shape
+    nzc = 16
+    sc = scenes.large_hall(steps=64, size=(nx, ny, nzc))
+    g = oracle_grid(sc)
+    osc = oracle_scene(sc, g)
+    n = nx * ny * nzc
+    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
+    osc.run(1, state=st)                               # touch the pages
+    t0 = time.perf_counter()
+    osc.run(2, state=st, step0=1)
+    per_step = (time.perf_counter() - t0) / 2
+    # grow the crop to fill the budget: steps of the crop until ~budget
+    k = max(2, min(200, int(steps_budget_s / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    osc.run(k, state=st, step0=3)
+    dt = time.perf_counter() - t0
+    return n * k / dt / 1e9, f"{k} steps of a {nx}x{ny}x{nzc} crop of the hall ({n * k / 1e9:.2f} G voxel updates)", dt
+
+
+def run_virs(args):
+    import torch
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    dev = local
+    torch.cuda.set_device(dev)
+    from virs_b200 import capi, scenes
+    total_steps = args.warmup + 3 * args.steps + args.kernel_steps + 16
+    sc = scenes.large_hall(steps=total_steps, size=tuple(args.size))
+    nvox = int(np.prod(args.size))
+    stream = torch.cuda.Stream(device=dev)
+    r32 = bench_storage(sc, capi.STORAGE_F32, args, stream, dev, world, dist, want_e2e=True)
+    variants = {}
+    if args.variants:
+        rb = bench_storage(sc, capi.STORAGE_BF16, args, stream, dev, world, dist, want_e2e=False)
+        gv = nvox * args.steps / (rb["ms"] * 1e-3) / 1e9 * world
+        peak, _ = peaks()
+        variants["bf16_storage"] = {
+            "value": gv, "ms_per_step": rb["ms"] / args.steps,
+            "speedup_vs_f32": (r32["ms"] / rb["ms"]),
+            "roofline_frac": (nvox * BYTES_16 / (rb["kernel_ms"] * 1e-3) / 1e9) / peak if rb.get("kernel_ms") else None,
+            "bytes_per_voxel": BYTES_16,
+        }
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = peaks()
+    value = nvox * args.steps / (r32["ms"] * 1e-3) / 1e9 * world
+    kernel_ms = r32.get("kernel_ms")
+    achieved = nvox * BYTES_F32 / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "Gvoxel-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r32["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded hall geometry, Gaussian-pulse source)",
+        "config": {
+            "workload": "large_hall %dx%dx%d FP32, 2 materials x 3-section cascades, sponge 1, 1 source, "
+                        "8 receivers, Courant 1/sqrt(3), centered boundary form" % tuple(args.size),
+            "voxels": nvox,
+            "boundary_voxels": int(r32["meta"]["info"].boundary_count),
+            "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * 4 / 1e9),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "timing": "CUDA events on the launching stream around virs_run (CUDA graph), max over ranks",
+        },
+        "roofline": {
+            "bound": "hbm",
+            "achieved": round(achieved, 1) if achieved else None,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+            "traffic": None,
+            "kernel": "k_step<float,8> (stencil + fused boundary filters)",
+            "kernel_ms": kernel_ms,
+            "bytes_per_voxel": BYTES_F32,
+        },
+        "e2e": {
+            "value": round(nvox * args.steps / (r32["e2e_ms"] * 1e-3) / 1e9 * world, 3),
+            "unit": "Gvoxel-updates/s",
+            "h2d_bytes_per_step": r32["h2d"],
+            "d2h_bytes_per_step": r32["d2h"],
+            "api": "virs_run_host (pinned host buffers)",
+            "wall_ms": r32["e2e_wall_ms"],
+        },
+        "gpu_launches": 2 * args.steps,
+        "clocks": r32["clocks"],
+        "variants": variants,
+    }
+    if args.traffic_json and Path(args.traffic_json).exists():
+        line["roofline"]["traffic"] = json.loads(Path(args.traffic_json).read_text()).get("bytes_per_launch")
+    if world == 1 and not args.no_cpu:
+        th = host_threads()
+        gv, desc, secs = cpu_sample(tuple(args.size), args.cpu_seconds, th)
+        line["cpu_baseline"] = {"value": round(gv, 4), "unit": "Gvoxel-updates/s", "cores": th, "kind": "port",
+                                "sample": desc + f", {secs:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    th = host_threads()
+    # size the crop so that warmup + steps fit in about two minutes
+    budget = 120.0 / max(args.steps + args.warmup, 1)
+    import oracle
+    from virs_b200 import scenes
+    sys.path.insert(0, str(ROOT / "tests"))
+    from helpers import oracle_grid, oracle_scene
+    oracle.set_threads(th)
+    nx, ny, nz = args.size
+    nzc = 8
+    sc = scenes.large_hall(steps=args.steps + args.warmup + 2, size=(nx, ny, nzc))
+    g = oracle_grid(sc)
+    osc = oracle_scene(sc, g)
+    n = nx * ny * nzc
+    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
+    t0 = time.perf_counter()
+    osc.run(1, state=st)
+    per = time.perf_counter() - t0
+    if per > budget:           # shrink to fewer rows
+        frac = max(budget / per, 1 / ny)
+        nyc = max(8, int(ny * frac))
+        sc = scenes.large_hall(steps=args.steps + args.warmup + 2, size=(nx, nyc, nzc))
+        g = oracle_grid(sc)
+        osc = oracle_scene(sc, g)
+        n = nx * nyc * nzc
+        st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
+        desc = f"{nx}x{nyc}x{nzc} crop of the hall"
+    else:
+        desc = f"{nx}x{ny}x{nzc} crop of the hall"
+    osc.run(args.warmup, state=st, step0=1)
+    t0 = time.perf_counter()
+    osc.run(args.steps, state=st, step0=1 + args.warmup)
+    secs = time.perf_counter() - t0
+    gv = n * args.steps / secs / 1e9
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(gv, 4),
+        "unit": "Gvoxel-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": secs * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded hall geometry)",
+        "config": {"workload": "large_hall %dx%dx%d FP32 (CPU arm runs a crop; one step = one time step of the crop)"
+                               % tuple(args.size)},
+        "cpu_baseline": {"value": round(gv, 4), "unit": "Gvoxel-updates/s", "cores": th, "kind": "port",
+                         "sample": f"{args.steps} steps of a {desc}; the reference CPU build (oneTBB, Embree, "
+                                   "tinyobjloader, kfr, AudioFile) cannot be compiled here, so this is the CPU "
+                                   "restatement of its step"},
+        "e2e": {"value": round(gv, 4), "unit": "Gvoxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["virs", "reference"], default="virs")
+    ap.add_argument("--size", type=int, nargs=3, default=[1024, 768, 512])
+    ap.add_argument("--kernel-steps", type=int, default=100, help="steps of the per-kernel CUDA-event pass")
+    ap.add_argument("--no-variants", dest="variants", action="store_false")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--traffic-json", default=str(ROOT / "profiles" / "step_traffic.json"))
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_virs(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,235 @@
+/*
+ * virs.h -- C ABI of the B200 implementation of the VIRS FDTD simulation path.
+ *
+ * One opaque handle (virs_sim) owns every device buffer of one simulation on
+ * one GPU.  All entry points return a virs_status; none of them exits the
+ * process or prints.  virs_last_error() gives the message of the last
+ * failure on the calling thread.  Plain pointers and sizes only: host
+ * buffers are read or written synchronously unless a call says otherwise.
+ *
+ * Layout of every voxel array exchanged through this ABI is the reference's:
+ *   idx = (z * ny + y) * nx + x            (src/simulator/vectorspace.h:200-203)
+ *
+ * Each declaration names the reference interface it replaces, as
+ * path:line in the Snipet/VIRS tree.
+ */
+#ifndef VIRS_H
+#define VIRS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VIRS_ABI_VERSION 1
+
+typedef enum virs_status {
+    VIRS_OK = 0,
+    VIRS_E_ARG = 1,      /* invalid argument: sizes, indices, ranges, order   */
+    VIRS_E_OOM = 2,      /* device or host allocation failed                  */
+    VIRS_E_CUDA = 3,     /* CUDA runtime error (message has the CUDA string)  */
+    VIRS_E_UNSTABLE = 4, /* non-finite receiver sample or energy blow-up      */
+    VIRS_E_TIMEOUT = 5,  /* a bounded device wait gave up                     */
+    VIRS_E_STATE = 6,    /* call out of order (e.g. run before classify)      */
+    VIRS_E_IO = 7        /* a file could not be read or parsed                */
+} virs_status;
+
+typedef struct virs_sim virs_sim;
+
+/* pressure storage precision (updates are always FP32) */
+enum { VIRS_STORAGE_F32 = 0, VIRS_STORAGE_F16 = 1, VIRS_STORAGE_BF16 = 2 };
+
+/* boundary correction of flag-2 voxels.  REFERENCE is simulator_gpu.cu:148:
+ * p+ -= K*g*w*(mix_filtered*y + mix_direct*(p - p-)), explicit.  CENTERED
+ * takes the direct damping term at the centre of the step, (p+ - p-)/2,
+ * which dissipates every mode; the explicit form can diverge in a boundary
+ * layer several voxels thick at the 3D Courant limit. */
+enum { VIRS_BOUNDARY_REFERENCE = 0, VIRS_BOUNDARY_CENTERED = 1 };
+
+/* roles of OBJ material ids (virs_set_material_roles) */
+#define VIRS_ROLE_IGNORE 0xFF /* triangles are not voxelised                     */
+#define VIRS_ROLE_SOURCE 0xFE /* "speaker": flag 3, hard source (simulator.cpp:445-449) */
+/* values 0..63: wall (flag 1) with that absorber material index (simulator.cpp:439-444) */
+
+typedef struct virs_params {
+    uint32_t struct_size;    /* sizeof(virs_params)                                   */
+    int32_t device;          /* CUDA device ordinal                                   */
+    float sound_speed;       /* c = 343 m/s            (simulator_gpu.cu:195)          */
+    float courant;           /* dt = courant*h/(c*sqrt 3); 0.5 (simulator_gpu.cu:196)  */
+    float cell_size;         /* h; 0 = 343/(22050*2*2) (simulator.cpp:17-18, 321)      */
+    float bbox_nudge;        /* 0.1 m                  (simulator.cpp:304)             */
+    int32_t sponge_width;    /* W = 1                  (sponge_kernel.cu:5)            */
+    int32_t storage;         /* VIRS_STORAGE_*                                         */
+    int32_t boundary_form;   /* VIRS_BOUNDARY_REFERENCE or VIRS_BOUNDARY_CENTERED        */
+    float storage_scale;     /* stored = p*scale for 16-bit storage; 0 = automatic     */
+    float boundary_gain;     /* 0.4f                   (simulator_gpu.cu:148)          */
+    float boundary_k;        /* 0 = (c*dt)/h*0.95 on the host (simulator_gpu.cu:147)  */
+    double mix_filtered;     /* 0.1                    (simulator_gpu.cu:148)          */
+    double mix_direct;       /* 0.9                    (simulator_gpu.cu:148)          */
+} virs_params;
+
+typedef struct virs_grid_info {
+    uint64_t nx, ny, nz;     /* grid dimensions                                       */
+    float cell_size;         /* h                                                     */
+    float bbox_min[3];       /* world position of voxel corner (0,0,0)                */
+    float dt;                /* time step (float, as the step kernel uses it)         */
+    double sample_rate;      /* 1/dt in double, as the filter design gets it          */
+    uint64_t boundary_count; /* flag-2 voxels after virs_classify                     */
+    uint64_t steps_done;     /* steps run since virs_start_simulation                 */
+} virs_grid_info;
+
+typedef struct virs_timing {
+    double step_kernel_ms;   /* summed CUDA-event time of the stencil kernel         */
+    uint64_t step_launches;  /* stencil launches timed                                */
+    uint64_t kernel_launches;/* all kernels this library launched while timing        */
+} virs_timing;
+
+/* ---- lifetime -------------------------------------------------------------- */
+
+/* Reference defaults for every field. */
+virs_status virs_params_default(virs_params *p);
+
+/* Replaces fdtd_setup / fdtd_gpu_setup (simulator_dispatch.cpp:12-19,
+ * simulator_gpu.cpp:7-235).  Device memory is allocated when a grid is set. */
+virs_status virs_create(const virs_params *p, virs_sim **out);
+
+/* Replaces fdtd_cleanup / fdtd_gpu_cleanup (simulator_dispatch.cpp:51-58,
+ * simulator_gpu.cpp:237-305).  NULL is accepted. */
+virs_status virs_destroy(virs_sim *sim);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *virs_last_error(void);
+
+/* ---- geometry -------------------------------------------------------------- */
+
+/* Material id -> role table used by the voxeliser.  Default {0: wall absorber
+ * 0, 1: source}, the reference's mapping (simulator.cpp:439-449). */
+virs_status virs_set_material_roles(virs_sim *sim, const uint8_t *roles, size_t n);
+
+/* Replaces the geometry half of Simulator::loadObj (simulator.cpp:262-452):
+ * parse an OBJ (+ its mtllib), bounding box with nudge, grid sizing,
+ * allocation, triangle/box voxelisation into flags 1 (wall) and 3 (source). */
+virs_status virs_load_obj(virs_sim *sim, const char *path);
+
+/* The same from an in-memory mesh: verts [nverts][3] (world metres),
+ * tris [ntris][3] vertex indices, tri_material [ntris] OBJ material ids. */
+virs_status virs_set_mesh(virs_sim *sim, const float *verts, size_t nverts, const uint32_t *tris,
+                          const int32_t *tri_material, size_t ntris);
+
+/* Replaces updateGPUFromGrid for the flags (simulator_dispatch.cpp:70-81):
+ * set the grid directly.  flags [nx*ny*nz] with values 0..3 (reference
+ * layout); wall_material [nx*ny*nz] or NULL (all absorber 0). */
+virs_status virs_set_grid(virs_sim *sim, uint64_t nx, uint64_t ny, uint64_t nz, float cell_size,
+                          const uint8_t *flags, const uint8_t *wall_material);
+
+virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);
+
+/* Replaces buildSpongeLayer / buildSpongeLayerGPU (simulator_dispatch.cpp:83-91,
+ * sponge_kernel.cu:65-99) plus the normals, boundary-list and filter-state
+ * steps of loadObj (simulator.cpp:472-610, uploadNormalsToGPU :102-109,
+ * uploadBoundaryIndicesToGPU :120-130, allocFilterStates :132-160).
+ * All on the GPU. */
+virs_status virs_classify(virs_sim *sim);
+
+/* Parity exports (reference layout). */
+virs_status virs_get_flags(const virs_sim *sim, uint8_t *out, size_t n);
+virs_status virs_get_normals(const virs_sim *sim, uint8_t *out, size_t n);
+virs_status virs_get_boundary_indices(const virs_sim *sim, uint32_t *out, size_t n);
+/* per boundary voxel (list order): material index and sponge weight */
+virs_status virs_get_boundary_materials(const virs_sim *sim, uint8_t *material, float *weight, size_t n);
+
+/* ---- filters, sources, receivers ----------------------------------------- */
+
+/* Replaces allocFilterCoeffs + uploadFilterCoeffsToGPU
+ * (simulator_dispatch.cpp:162-280): coeffs [n_materials][n_sections][5] as
+ * {b0, b1, b2, a1, a2}; sections run in series.  Resets filter states. */
+virs_status virs_set_filters(virs_sim *sim, uint32_t n_materials, uint32_t n_sections, const float *coeffs);
+
+/* computeHighpassBiquad / computeLowpassBiquad (biquad.cpp:3-43), with the
+ * reference's float/double promotions; out5 = {b0, b1, b2, a1, a2}. */
+virs_status virs_design_highpass(float sample_rate, float cutoff, float q, float gain, float *out5);
+virs_status virs_design_lowpass(float sample_rate, float cutoff, float q, float gain, float *out5);
+
+/* FP64 designs of absorbing-boundary filters (no reference counterpart; the
+ * reference designs one RBJ high-pass, simulator.cpp:955-967).
+ * First order: bilinear transform, prewarped at fc, of G*wc/(s + wc) with
+ * G = (1 - R)/(1 + R) for the reflection coefficient R; out5 as above.
+ * Octave cascade: low shelf / peak / high shelf at freqs (NULL = 250, 1000,
+ * 4000 Hz) with band gains G_b from absorption alpha[b]; out15 = 3 x out5. */
+virs_status virs_design_first_order(double sample_rate, double reflection, double fc, double *out5);
+virs_status virs_design_octave_cascade(double sample_rate, const double *alpha, const double *freqs, double *out15);
+
+/* Values given to flag-3 voxels at step n (n < len; 0 after).  Default: 10
+ * for steps 0..9 (simulator_gpu.cu:214-218). */
+virs_status virs_set_hard_source(virs_sim *sim, const float *values, size_t len);
+
+/* Additive point sources (no reference counterpart; the reference's
+ * commented audio-file source, simulator_gpu.cu:220-245).  idx [n] voxel
+ * indices, distinct, interior; signal [n][len]; p(idx) += signal[s][step]. */
+virs_status virs_set_sources(virs_sim *sim, uint32_t n, const uint64_t *idx, const float *signal, size_t len);
+
+/* Receivers (the reference reads the single voxel (334,225,270) after every
+ * step, simulator_gpu.cu:295-300).  idx [n] voxel indices. */
+virs_status virs_set_receivers(virs_sim *sim, uint32_t n, const uint64_t *idx);
+
+/* ---- running ---------------------------------------------------------------- */
+
+/* Replaces fdtd_start_simulation (simulator_dispatch.cpp:93-100): reserve
+ * receiver storage for `steps` steps and start from rest (fields, filter
+ * states and the step counter set to zero). */
+virs_status virs_start_simulation(virs_sim *sim, uint64_t steps);
+
+/* Replaces fdtd_step / fdtd_gpu_step (simulator_dispatch.cpp:21-29,
+ * simulator_gpu.cu:184-332): one step numbered `step`, then the first
+ * receiver's new sample is read back into *sample (may be NULL) and the
+ * reference's RMS stop rule (simulator_gpu.cu:303-330, on receiver 0) sets
+ * *keep_going (may be NULL). */
+virs_status virs_step(virs_sim *sim, uint32_t step, int *keep_going, float *sample);
+
+/* Run `steps` steps on `stream` (a cudaStream_t, NULL = the handle's own
+ * stream) with no host traffic; the step loop is a CUDA graph.  Returns
+ * when the work is queued. */
+virs_status virs_run(virs_sim *sim, uint64_t steps, void *stream);
+
+/* End-to-end form for host callers: copies `signal` [n_src][steps] (or NULL
+ * to keep the signals set before) for the next `steps` steps from host
+ * memory, runs, and copies the new receiver samples [n_rcv][steps] to
+ * `ir_out`; synchronous. */
+virs_status virs_run_host(virs_sim *sim, uint64_t steps, const float *signal, float *ir_out, void *stream);
+
+/* Wait for the handle's queued work. */
+virs_status virs_synchronize(virs_sim *sim);
+
+/* Receiver samples [n_rcv][steps] of steps first .. first+steps-1. */
+virs_status virs_get_ir(const virs_sim *sim, uint64_t first, uint64_t steps, float *out);
+
+/* Replaces updateCurrentGridFromGPU (simulator_dispatch.cpp:42-49): p^n
+ * (and p^{n-1} if prev != NULL) in the reference layout, unscaled. */
+virs_status virs_get_pressure(const virs_sim *sim, float *cur, float *prev, size_t n);
+virs_status virs_set_pressure(virs_sim *sim, const float *cur, const float *prev, size_t n);
+
+/* Replaces initPressureSphereGPU (init_sphere.cu:27-55). */
+virs_status virs_init_pressure_sphere(virs_sim *sim, uint64_t x, uint64_t y, uint64_t z, uint64_t radius,
+                                      float pressure, int init);
+
+/* FP64 discrete energy of the current state (the physics health monitor). */
+virs_status virs_energy(virs_sim *sim, double *out);
+
+/* ---- measurement ------------------------------------------------------------- */
+
+/* While enabled, virs_run launches without a graph and brackets every
+ * stencil launch with CUDA events; virs_get_timing sums them. */
+virs_status virs_set_timing(virs_sim *sim, int enable);
+virs_status virs_get_timing(virs_sim *sim, virs_timing *out);
+
+/* Kernel variant: tile height (4, 8 or 16 rows) and planes per block;
+ * 0 = the library's choice. */
+virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VIRS_H */

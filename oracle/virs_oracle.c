@@ -1,0 +1,670 @@
+/*
+ * virs_oracle.c -- CPU restatement of the VIRS room-acoustics FDTD path.
+ *
+ * TEST INFRASTRUCTURE, NOT PRODUCT CODE.  This library is the checker that the
+ * CUDA implementation under virs_b200/ is compared against.  Only tests/,
+ * __graft_entry__.smoke() and the cpu_baseline / reference legs of bench.py
+ * load it; the product library never links or calls it.
+ *
+ * What it restates (paths relative to the Snipet/VIRS source tree):
+ *   - triangle/box SAT test            src/simulator/simulator.cpp:45-141
+ *   - bounding box + grid sizing       src/simulator/simulator.cpp:288-329
+ *   - toVoxel                          src/simulator/simulator.h:39-45
+ *   - triangle sweep -> flags 1 / 3    src/simulator/simulator.cpp:396-452
+ *   - boundary ("sponge") marking      src/simulator/sponge_kernel.cu:8-62
+ *   - neighbour normals bitmask        src/simulator/simulator.cpp:480-531
+ *   - boundary index list              src/simulator/simulator.cpp:572-605
+ *   - RBJ high-pass design             src/simulator/biquad.cpp:24-43
+ *   - step constants                   src/simulator/simulator_gpu.cu:195-198, simulator.cpp:940-957
+ *   - interior leapfrog update         src/simulator/simulator_gpu.cu:38-103
+ *   - boundary biquad update           src/simulator/simulator_gpu.cu:105-150
+ *   - source value, rotation, receiver src/simulator/simulator_gpu.cu:214-218, 292-300
+ *
+ * Extensions with no reference counterpart (their definition lives here and
+ * the CUDA path must agree with it):
+ *   - sponge width W (the reference hard-codes N = 1, sponge_kernel.cu:5):
+ *     air voxels with a wall voxel at squared distance d2 <= W*W become
+ *     boundary voxels; W = 1 is exactly the reference rule;
+ *   - per-boundary-voxel material: material of the nearest wall voxel, ties
+ *     broken by the reference's scan order (dz, dy, dx ascending, strict <);
+ *   - per-material cascades of S biquad sections (series form; S = 1 is the
+ *     reference's single section);
+ *   - sponge weight w(d2) = ((W + 1 - sqrt(d2)) / W)^2 on the boundary
+ *     correction (w = 1 whenever W = 1);
+ *   - additive ("soft") point sources with per-step signals, R receivers.
+ *
+ * Floating point: the FP32 run follows the reference CUDA build's numerics:
+ * nvcc --use_fast_math flushes subnormals (FTZ) and contracts a*b+c into one
+ * fused multiply-add.  This file compiles with -ffp-contract=off, writes every
+ * fused operation explicitly with fmaf(), and sets the x86 FTZ/DAZ bits in
+ * every worker thread for the FP32 run.  The boundary correction is evaluated
+ * in double exactly as the reference does (simulator_gpu.cu:148, the double
+ * literals 0.1 and 0.9 promote the expression).
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <xmmintrin.h>
+#include <pmmintrin.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define VO_API __attribute__((visibility("default")))
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* threading / FTZ                                                           */
+/* ------------------------------------------------------------------------ */
+
+static int g_threads = 0; /* 0 = OpenMP default */
+
+VO_API void vo_set_threads(int n) { g_threads = n; }
+
+VO_API int vo_get_threads(void)
+{
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+static void ftz_on(void)
+{
+    _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_ON);
+    _MM_SET_DENORMALS_ZERO_MODE(_MM_DENORMALS_ZERO_ON);
+}
+
+static void ftz_off(void)
+{
+    _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_OFF);
+    _MM_SET_DENORMALS_ZERO_MODE(_MM_DENORMALS_ZERO_OFF);
+}
+
+/* ------------------------------------------------------------------------ */
+/* geometry                                                                  */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { float x, y, z; } v3;
+
+static v3 v3sub(v3 a, v3 b) { v3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static v3 v3abs(v3 a) { v3 r = {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; return r; }
+static float mn3(float a, float b, float c) { float m = a; if (b < m) m = b; if (c < m) m = c; return m; }
+static float mx3(float a, float b, float c) { float m = a; if (m < b) m = b; if (m < c) m = c; return m; }
+
+/* simulator.cpp:73-86 -- note the projection always uses the .y and .z
+ * components of the vertices, whatever the edge/axis pair; kept as written. */
+static int axis_test(float a, float b, float fa, float fb, v3 p0, v3 p1, v3 p2, float ex, float ey)
+{
+    float p0p = a * p0.y - b * p0.z;
+    float p1p = a * p1.y - b * p1.z;
+    float p2p = a * p2.y - b * p2.z;
+    float minp = mn3(p0p, p1p, p2p);
+    float maxp = mx3(p0p, p1p, p2p);
+    float rad = fa * ey + fb * ex;
+    return !(minp > rad || maxp < -rad);
+}
+
+/* simulator.cpp:45-141 */
+static int sat(v3 v0w, v3 v1w, v3 v2w, v3 bmin, v3 bmax)
+{
+    v3 c = {(bmin.x + bmax.x) * 0.5f, (bmin.y + bmax.y) * 0.5f, (bmin.z + bmax.z) * 0.5f};
+    v3 e = {(bmax.x - bmin.x) * 0.5f, (bmax.y - bmin.y) * 0.5f, (bmax.z - bmin.z) * 0.5f};
+    v3 v0 = v3sub(v0w, c), v1 = v3sub(v1w, c), v2 = v3sub(v2w, c);
+    v3 f0 = v3sub(v1, v0), f1 = v3sub(v2, v1), f2 = v3sub(v0, v2);
+    v3 a0 = v3abs(f0), a1 = v3abs(f1), a2 = v3abs(f2);
+
+    if (!axis_test(f0.z, f0.y, a0.z, a0.y, v0, v1, v2, e.y, e.z)) return 0;
+    if (!axis_test(f0.z, f0.x, a0.z, a0.x, v0, v1, v2, e.x, e.z)) return 0;
+    if (!axis_test(f0.y, f0.x, a0.y, a0.x, v0, v1, v2, e.x, e.y)) return 0;
+    if (!axis_test(f1.z, f1.y, a1.z, a1.y, v0, v1, v2, e.y, e.z)) return 0;
+    if (!axis_test(f1.z, f1.x, a1.z, a1.x, v0, v1, v2, e.x, e.z)) return 0;
+    if (!axis_test(f1.y, f1.x, a1.y, a1.x, v0, v1, v2, e.x, e.y)) return 0;
+    if (!axis_test(f2.z, f2.y, a2.z, a2.y, v0, v1, v2, e.y, e.z)) return 0;
+    if (!axis_test(f2.z, f2.x, a2.z, a2.x, v0, v1, v2, e.x, e.z)) return 0;
+    if (!axis_test(f2.y, f2.x, a2.y, a2.x, v0, v1, v2, e.x, e.y)) return 0;
+
+    float lo = mn3(v0.x, v1.x, v2.x), hi = mx3(v0.x, v1.x, v2.x);
+    if (lo > e.x || hi < -e.x) return 0;
+    lo = mn3(v0.y, v1.y, v2.y); hi = mx3(v0.y, v1.y, v2.y);
+    if (lo > e.y || hi < -e.y) return 0;
+    lo = mn3(v0.z, v1.z, v2.z); hi = mx3(v0.z, v1.z, v2.z);
+    if (lo > e.z || hi < -e.z) return 0;
+
+    v3 n = {f0.y * f1.z - f0.z * f1.y, f0.z * f1.x - f0.x * f1.z, f0.x * f1.y - f0.y * f1.x};
+    float d = -(n.x * v0.x + n.y * v0.y + n.z * v0.z);
+    float r = e.x * fabsf(n.x) + e.y * fabsf(n.y) + e.z * fabsf(n.z);
+    if (fabsf(d) > r) return 0;
+    return 1;
+}
+
+VO_API int vo_sat(const float *v0, const float *v1, const float *v2, const float *bmin, const float *bmax)
+{
+    v3 a = {v0[0], v0[1], v0[2]}, b = {v1[0], v1[1], v1[2]}, c = {v2[0], v2[1], v2[2]};
+    v3 lo = {bmin[0], bmin[1], bmin[2]}, hi = {bmax[0], bmax[1], bmax[2]};
+    return sat(a, b, c, lo, hi);
+}
+
+/* simulator.cpp:288-310.  The max corner starts at FLT_MIN (the smallest
+ * positive normal float, numeric_limits<float>::min()), not -FLT_MAX, so an
+ * axis whose vertices are all negative keeps max = FLT_MIN; reproduced. */
+VO_API void vo_bbox(const float *verts, uint64_t nverts, float nudge, float *bmin, float *bmax)
+{
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float hi[3] = {FLT_MIN, FLT_MIN, FLT_MIN};
+    for (uint64_t i = 0; i < nverts; ++i)
+        for (int a = 0; a < 3; ++a) {
+            float v = verts[3 * i + a];
+            if (v < lo[a]) lo[a] = v;
+            if (hi[a] < v) hi[a] = v;
+        }
+    for (int a = 0; a < 3; ++a) {
+        bmin[a] = lo[a] - nudge;
+        bmax[a] = hi[a] + nudge;
+    }
+}
+
+/* simulator.cpp:321-329: span * (1/h), truncated to size_t. */
+VO_API void vo_dims(const float *bmin, const float *bmax, float h, uint64_t *dims)
+{
+    float nvm = 1.f / h;
+    for (int a = 0; a < 3; ++a) {
+        float span = bmax[a] - bmin[a];
+        float s = span * nvm;
+        dims[a] = s > 0.f ? (uint64_t)s : 0;
+    }
+}
+
+/* simulator.h:39-45 */
+static v3 to_voxel(v3 p, const float *bmin, float h)
+{
+    v3 r = {(p.x - bmin[0]) / h, (p.y - bmin[1]) / h, (p.z - bmin[2]) / h};
+    return r;
+}
+
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* Roles of OBJ material ids.  roles[m] for m < nroles:
+ *   0xFF = ignored, 0xFE = source ("speaker", flag 3), k < 0xFE = wall with
+ *   absorber material k (flag 1).  Ids outside the table (including -1, a
+ *   face with no usemtl) are ignored.  The reference mapping is
+ *   {0: wall, 1: speaker} (simulator.cpp:439-449). */
+#define VO_ROLE_IGNORE 0xFF
+#define VO_ROLE_SOURCE 0xFE
+
+/* simulator.cpp:396-452.  tris: ntri * 9 floats (world coordinates). */
+VO_API int vo_voxelize(const float *tris, const int32_t *tri_mat, uint64_t ntri,
+                       const uint8_t *roles, uint64_t nroles, float h, const float *bmin,
+                       uint64_t nx, uint64_t ny, uint64_t nz, uint8_t *flags, uint8_t *wall_mat)
+{
+    if (nx == 0 || ny == 0 || nz == 0) return -1;
+    for (uint64_t t = 0; t < ntri; ++t) {
+        int m = tri_mat[t];
+        uint8_t role = (m >= 0 && (uint64_t)m < nroles) ? roles[m] : VO_ROLE_IGNORE;
+        const float *q = tris + 9 * t;
+        v3 w0 = {q[0], q[1], q[2]}, w1 = {q[3], q[4], q[5]}, w2 = {q[6], q[7], q[8]};
+        v3 g0 = to_voxel(w0, bmin, h), g1 = to_voxel(w1, bmin, h), g2 = to_voxel(w2, bmin, h);
+        int ix0 = clampi((int)floorf(mn3(g0.x, g1.x, g2.x)), 0, (int)nx - 1);
+        int iy0 = clampi((int)floorf(mn3(g0.y, g1.y, g2.y)), 0, (int)ny - 1);
+        int iz0 = clampi((int)floorf(mn3(g0.z, g1.z, g2.z)), 0, (int)nz - 1);
+        int ix1 = clampi((int)ceilf(mx3(g0.x, g1.x, g2.x)), 0, (int)nx - 1);
+        int iy1 = clampi((int)ceilf(mx3(g0.y, g1.y, g2.y)), 0, (int)ny - 1);
+        int iz1 = clampi((int)ceilf(mx3(g0.z, g1.z, g2.z)), 0, (int)nz - 1);
+        for (int k = iz0; k <= iz1; ++k)
+            for (int j = iy0; j <= iy1; ++j)
+                for (int i = ix0; i <= ix1; ++i) {
+                    v3 lo = {(float)i, (float)j, (float)k};
+                    v3 hi = {(float)i + 1.f, (float)j + 1.f, (float)k + 1.f};
+                    if (!sat(g0, g1, g2, lo, hi)) continue;
+                    uint64_t idx = ((uint64_t)k * ny + (uint64_t)j) * nx + (uint64_t)i;
+                    if (role == VO_ROLE_SOURCE) {
+                        flags[idx] = 3;
+                    } else if (role != VO_ROLE_IGNORE) {
+                        flags[idx] = 1;
+                        if (wall_mat) wall_mat[idx] = role;
+                    }
+                }
+    }
+    return 0;
+}
+
+/* sponge_kernel.cu:8-62 generalised to width W.  Interior voxels with flag 0
+ * scan the cube [-W, W]^3 for wall voxels (flag 1); the smallest squared
+ * distance d2 wins (first in dz, dy, dx order on ties, as the reference's
+ * strict "<" keeps the first).  d2 < W*W + 1 marks the voxel 2.  Voxels with
+ * flag != 0 are copied; the domain border is left as it was.  bmat / bd2
+ * receive, per voxel, the nearest wall's material and d2 (0 elsewhere). */
+VO_API void vo_classify(uint64_t nx, uint64_t ny, uint64_t nz, int W, const uint8_t *flags_in,
+                        const uint8_t *wall_mat, uint8_t *flags_out, uint8_t *bmat, uint16_t *bd2)
+{
+    const uint64_t n = nx * ny * nz;
+    if (flags_out != flags_in) memcpy(flags_out, flags_in, n);
+    if (bmat) memset(bmat, 0, n);
+    if (bd2) memset(bd2, 0, n * sizeof(uint16_t));
+    const int lim = W * W + 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(vo_get_threads())
+    for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+        for (int64_t y = 1; y < (int64_t)ny - 1; ++y)
+            for (int64_t x = 1; x < (int64_t)nx - 1; ++x) {
+                uint64_t id = ((uint64_t)z * ny + (uint64_t)y) * nx + (uint64_t)x;
+                if (flags_in[id] != 0) continue;
+                int best = 1 << 30;
+                uint64_t bestn = 0;
+                for (int dz = -W; dz <= W; ++dz) {
+                    int64_t zz = z + dz;
+                    if (zz < 0 || zz >= (int64_t)nz) continue;
+                    for (int dy = -W; dy <= W; ++dy) {
+                        int64_t yy = y + dy;
+                        if (yy < 0 || yy >= (int64_t)ny) continue;
+                        const uint8_t *row = flags_in + ((uint64_t)zz * ny + (uint64_t)yy) * nx;
+                        for (int dx = -W; dx <= W; ++dx) {
+                            int64_t xx = x + dx;
+                            if (xx < 0 || xx >= (int64_t)nx) continue;
+                            if (row[xx] != 1) continue;
+                            int d2 = dx * dx + dy * dy + dz * dz;
+                            if (d2 < best) {
+                                best = d2;
+                                bestn = ((uint64_t)zz * ny + (uint64_t)yy) * nx + (uint64_t)xx;
+                            }
+                        }
+                    }
+                }
+                if (best < lim) {
+                    flags_out[id] = 2;
+                    if (bmat) bmat[id] = wall_mat ? wall_mat[bestn] : 0;
+                    if (bd2) bd2[id] = (uint16_t)best;
+                } else {
+                    flags_out[id] = 0;
+                }
+            }
+}
+
+/* simulator.cpp:480-531: bit set for each of the 6 neighbours whose flag is 0
+ * (+x 1, -x 2, +y 4, -y 8, +z 16, -z 32), interior voxels only. */
+VO_API void vo_normals(uint64_t nx, uint64_t ny, uint64_t nz, const uint8_t *flags, uint8_t *normals)
+{
+    memset(normals, 0, nx * ny * nz);
+    const uint64_t sy = nx, sz = nx * ny;
+    for (uint64_t z = 1; z + 1 < nz; ++z)
+        for (uint64_t y = 1; y + 1 < ny; ++y)
+            for (uint64_t x = 1; x + 1 < nx; ++x) {
+                uint64_t i = z * sz + y * sy + x;
+                uint8_t c = 0;
+                if (flags[i - 1] == 0) c |= 2;
+                if (flags[i + 1] == 0) c |= 1;
+                if (flags[i - sy] == 0) c |= 8;
+                if (flags[i + sy] == 0) c |= 4;
+                if (flags[i - sz] == 0) c |= 32;
+                if (flags[i + sz] == 0) c |= 16;
+                normals[i] = c;
+            }
+}
+
+/* simulator.cpp:572-605: ascending indices of interior voxels with flag 2.
+ * Returns the count; out may be NULL (counting pass). */
+VO_API uint64_t vo_boundary_list(uint64_t nx, uint64_t ny, uint64_t nz, const uint8_t *flags, uint32_t *out)
+{
+    uint64_t k = 0;
+    for (uint64_t z = 1; z + 1 < nz; ++z)
+        for (uint64_t y = 1; y + 1 < ny; ++y)
+            for (uint64_t x = 1; x + 1 < nx; ++x) {
+                uint64_t i = (z * ny + y) * nx + x;
+                if (flags[i] == 2) {
+                    if (out) out[k] = (uint32_t)i;
+                    ++k;
+                }
+            }
+    return k;
+}
+
+/* ------------------------------------------------------------------------ */
+/* constants and coefficient design                                          */
+/* ------------------------------------------------------------------------ */
+
+/* simulator_gpu.cu:195-198 with the Courant factor made a parameter
+ * (reference: 0.5):  dt = s*h/(c*sqrt(3)), c2dt2 = c*c*dt*dt, inv_h2 = 1/h^2;
+ * simulator_gpu.cu:147: K = (c*dt)/h * 0.95 (evaluated here in IEEE single;
+ * the reference evaluates it on the device). */
+VO_API void vo_step_constants(float h, float c, float courant, float *out4)
+{
+    float dt = courant * h / (c * sqrtf(3.f));
+    float c2dt2 = c * c * dt * dt;
+    float inv_h2 = 1.f / (h * h);
+    float K = (c * dt) / h * 0.95f;
+    out4[0] = dt;
+    out4[1] = c2dt2;
+    out4[2] = inv_h2;
+    out4[3] = K;
+}
+
+/* simulator.cpp:940-952: the host computes dt again in double and the filter
+ * sample rate as 1/dt, narrowed to float at the call of the design. */
+VO_API double vo_filter_fs(float h, double c, double courant)
+{
+    double hd = (double)h;
+    double dt = courant * hd / (c * sqrt(3.0));
+    return 1.f / dt;
+}
+
+/* biquad.cpp:24-43 (RBJ high-pass), with the same float/double promotions:
+ * 2.f * M_PI is double, so omega is computed in double and stored to float;
+ * sin/cos of a float argument call the double functions. */
+VO_API void vo_rbj_highpass_ref(float fs, float cutoff, float q, float gain, float *out5)
+{
+    float omega = 2.f * M_PI * cutoff / fs;
+    float alpha = sin(omega) / (2.f * q);
+    float a0 = 1.f + alpha;
+    float b0 = (1.f + cos(omega)) / 2.f / a0;
+    float b1 = -(1.f + cos(omega)) / a0;
+    float b2 = b0;
+    float a1 = -2.f * cos(omega) / a0;
+    float a2 = (1.f - alpha) / a0;
+    b0 *= gain; b1 *= gain; b2 *= gain;
+    out5[0] = b0; out5[1] = b1; out5[2] = b2; out5[3] = a1; out5[4] = a2;
+}
+
+/* biquad.cpp:3-22 (RBJ low-pass) with the same promotions. */
+VO_API void vo_rbj_lowpass_ref(float fs, float cutoff, float q, float gain, float *out5)
+{
+    float omega = 2.f * M_PI * cutoff / fs;
+    float alpha = sin(omega) / (2.f * q);
+    float a0 = 1.f + alpha;
+    float b0 = (1.f - cos(omega)) / 2.f / a0;
+    float b1 = (1.f - cos(omega)) / a0;
+    float b2 = b0;
+    float a1 = -2.f * cos(omega) / a0;
+    float a2 = (1.f - alpha) / a0;
+    b0 *= gain; b1 *= gain; b2 *= gain;
+    out5[0] = b0; out5[1] = b1; out5[2] = b2; out5[3] = a1; out5[4] = a2;
+}
+
+/* sponge weight w(d2) = ((W + 1 - sqrt(d2)) / W)^2, 1 at d2 = 1. */
+VO_API float vo_sponge_weight(int W, int d2)
+{
+    double d = sqrt((double)d2);
+    double t = ((double)W + 1.0 - d) / (double)W;
+    if (t < 0.0) t = 0.0;
+    return (float)(t * t);
+}
+
+/* ------------------------------------------------------------------------ */
+/* time stepping                                                             */
+/* ------------------------------------------------------------------------ */
+
+typedef struct vo_run_args {
+    uint64_t nx, ny, nz;
+    const uint8_t *flags;          /* classified flags, N bytes            */
+    uint64_t nb;                   /* boundary voxels                      */
+    const uint32_t *bidx;          /* [nb] ascending indices               */
+    const uint8_t *bmat;           /* [nb] material of each boundary voxel */
+    const float *bw;               /* [nb] sponge weight (NULL = all 1)    */
+    uint32_t n_materials;
+    uint32_t n_sections;
+    const float *coef32;           /* [M][S][5] b0 b1 b2 a1 a2             */
+    const double *coef64;          /* same, FP64 run                       */
+    float c2dt2, inv_h2, K;        /* FP32 run constants                   */
+    double c2dt2_d, inv_h2_d, K_d; /* FP64 run constants                   */
+    double mix_y, mix_d;           /* 0.1, 0.9 (simulator_gpu.cu:148)      */
+    double gain;                   /* (double)0.4f                         */
+    int32_t form;                  /* 0 reference (explicit), 1 centered   */
+    const float *hard;             /* flag-3 value per step                */
+    uint64_t n_hard;
+    uint32_t n_src;
+    const uint64_t *src_idx;
+    const float *src_sig;          /* [n_src][sig_len]                     */
+    uint64_t sig_len;
+    uint32_t n_rcv;
+    const uint64_t *rcv_idx;
+    uint64_t steps;
+    uint64_t step0;                /* index of the first step (source time)*/
+    uint64_t ir_stride;            /* row stride of ir (>= steps)          */
+    float *ir;                     /* [n_rcv][ir_stride], written at [r][n]*/
+    void *p;                       /* in/out p^n      (float or double)    */
+    void *pprev;                   /* in/out p^{n-1}                       */
+    void *state;                   /* in/out [nb][S][4]                    */
+} vo_run_args;
+
+static inline float vsel(const uint8_t *fl, const float *p, uint64_t n, float c)
+{
+    return fl[n] == 1 ? c : p[n];
+}
+
+/* simulator_gpu.cu:38-103 -- one thread per interior voxel in the
+ * reference; here a z-parallel loop (the reference CPU step's structure,
+ * simulator_cpu.cpp:66).  FP32 with FTZ. */
+static void interior_f32(const vo_run_args *a, const float *pc, const float *pp, float *pn, float hard)
+{
+    const uint64_t nx = a->nx, ny = a->ny, nz = a->nz, sy = nx, sz = nx * ny;
+    const float c2dt2 = a->c2dt2, inv_h2 = a->inv_h2;
+    const uint8_t *fl = a->flags;
+#pragma omp parallel num_threads(vo_get_threads())
+    {
+        ftz_on();
+#pragma omp for schedule(static)
+        for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+            for (uint64_t y = 1; y + 1 < ny; ++y) {
+                const uint64_t row = (uint64_t)z * sz + y * sy;
+                for (uint64_t x = 1; x + 1 < nx; ++x) {
+                    const uint64_t i = row + x;
+                    const uint8_t f = fl[i];
+                    if (f == 1) { pn[i] = 0.f; continue; }
+                    if (f == 3) { pn[i] = hard; continue; }
+                    if (f != 0 && f != 2) continue;
+                    const float c = pc[i];
+                    float s = vsel(fl, pc, i + 1, c);
+                    s = s + vsel(fl, pc, i - 1, c);
+                    s = s + vsel(fl, pc, i + sy, c);
+                    s = s + vsel(fl, pc, i - sy, c);
+                    s = s + vsel(fl, pc, i + sz, c);
+                    s = s + vsel(fl, pc, i - sz, c);
+                    const float lap = fmaf(-6.f, c, s) * inv_h2;
+                    const float t = 2.f * c - pp[i];
+                    pn[i] = fmaf(c2dt2, lap, t);
+                }
+            }
+        ftz_off();
+    }
+}
+
+/* simulator_gpu.cu:105-150 with S sections in series and per-voxel
+ * materials; FP32 recursion, double correction. */
+static void boundary_f32(const vo_run_args *a, const float *pc, const float *pp, float *pn, float *st)
+{
+    const uint32_t S = a->n_sections;
+    const double K = (double)a->K, my = a->mix_y, md = a->mix_d, g = a->gain;
+#pragma omp parallel num_threads(vo_get_threads())
+    {
+        ftz_on();
+#pragma omp for schedule(static)
+        for (int64_t b = 0; b < (int64_t)a->nb; ++b) {
+            const uint64_t i = a->bidx[b];
+            const float d = pc[i] - pp[i];
+            float in = d;
+            const float *k = a->coef32 + (uint64_t)a->bmat[b] * S * 5;
+            float *s = st + (uint64_t)b * S * 4;
+            for (uint32_t q = 0; q < S; ++q, k += 5, s += 4) {
+                float y = k[0] * in;
+                y = fmaf(k[1], s[0], y);
+                y = fmaf(k[2], s[1], y);
+                y = fmaf(-k[3], s[2], y);
+                y = fmaf(-k[4], s[3], y);
+                s[1] = s[0];
+                s[0] = in;
+                s[3] = s[2];
+                s[2] = y;
+                in = y;
+            }
+            const double w = a->bw ? (double)a->bw[b] : 1.0;
+            if (a->form == 0) {
+                const double t = fma((double)in, my, (double)d * md);
+                const double u = ((K * t) * g) * w;
+                pn[i] = (float)((double)pn[i] - u);
+            } else {
+                /* centered damping: the direct term uses (p+ - p-)/2 */
+                const double kgw = (K * g) * w;
+                const double ac = (kgw * md) * 0.5;
+                const double num = ((double)pn[i] - kgw * ((double)in * my)) + ac * (double)pp[i];
+                pn[i] = (float)(num / (1.0 + ac));
+            }
+        }
+        ftz_off();
+    }
+}
+
+static float sig_at(const vo_run_args *a, uint32_t s, uint64_t n)
+{
+    return n < a->sig_len ? a->src_sig[(uint64_t)s * a->sig_len + n] : 0.f;
+}
+
+/* One run of a->steps FP32 steps.  a->p / a->pprev / a->state hold the
+ * initial state (NULL = zero) and receive the final one. */
+VO_API int vo_run_f32(const vo_run_args *a)
+{
+    const uint64_t N = a->nx * a->ny * a->nz;
+    float *b0 = calloc(N, sizeof(float)), *b1 = calloc(N, sizeof(float)), *b2 = calloc(N, sizeof(float));
+    const uint64_t nst = a->nb * a->n_sections * 4;
+    float *st = calloc(nst ? nst : 1, sizeof(float));
+    if (!b0 || !b1 || !b2 || !st) { free(b0); free(b1); free(b2); free(st); return -1; }
+    if (a->p) memcpy(b0, a->p, N * sizeof(float));
+    if (a->pprev) memcpy(b1, a->pprev, N * sizeof(float));
+    if (a->state) memcpy(st, a->state, nst * sizeof(float));
+    float *pc = b0, *pp = b1, *pn = b2;
+    /* the next buffer starts as the reference's p_next would: it holds the
+     * values the kernel never writes (the domain border stays 0). */
+    for (uint64_t n = 0; n < a->steps; ++n) {
+        const uint64_t sn = a->step0 + n;
+        const float hard = sn < a->n_hard ? a->hard[sn] : 0.f;
+        interior_f32(a, pc, pp, pn, hard);
+        if (a->nb) boundary_f32(a, pc, pp, pn, st);
+        ftz_on();
+        for (uint32_t s = 0; s < a->n_src; ++s) {
+            const uint64_t i = a->src_idx[s];
+            pn[i] = pn[i] + sig_at(a, s, sn);
+        }
+        ftz_off();
+        /* rotation (simulator_gpu.cu:292-293): prev <- curr <- next */
+        float *t = pp; pp = pc; pc = pn; pn = t;
+        for (uint32_t r = 0; r < a->n_rcv; ++r)
+            a->ir[(uint64_t)r * a->ir_stride + n] = pc[a->rcv_idx[r]];
+    }
+    if (a->p) memcpy(a->p, pc, N * sizeof(float));
+    if (a->pprev) memcpy(a->pprev, pp, N * sizeof(float));
+    if (a->state) memcpy(a->state, st, nst * sizeof(float));
+    free(b0); free(b1); free(b2); free(st);
+    return 0;
+}
+
+/* The same model in double precision: the truth the reduced-precision forms
+ * are measured against.  Coefficients come from a->coef64. */
+VO_API int vo_run_f64(const vo_run_args *a)
+{
+    const uint64_t N = a->nx * a->ny * a->nz, nx = a->nx, ny = a->ny, nz = a->nz, sy = nx, sz = nx * ny;
+    double *b0 = calloc(N, sizeof(double)), *b1 = calloc(N, sizeof(double)), *b2 = calloc(N, sizeof(double));
+    const uint64_t nst = a->nb * a->n_sections * 4;
+    double *st = calloc(nst ? nst : 1, sizeof(double));
+    if (!b0 || !b1 || !b2 || !st) { free(b0); free(b1); free(b2); free(st); return -1; }
+    if (a->p) memcpy(b0, a->p, N * sizeof(double));
+    if (a->pprev) memcpy(b1, a->pprev, N * sizeof(double));
+    if (a->state) memcpy(st, a->state, nst * sizeof(double));
+    double *pc = b0, *pp = b1, *pn = b2;
+    const uint8_t *fl = a->flags;
+    const uint32_t S = a->n_sections;
+    for (uint64_t n = 0; n < a->steps; ++n) {
+        const uint64_t sn = a->step0 + n;
+        const double hard = sn < a->n_hard ? (double)a->hard[sn] : 0.0;
+        const double c2dt2 = a->c2dt2_d, inv_h2 = a->inv_h2_d;
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+        for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+            for (uint64_t y = 1; y + 1 < ny; ++y)
+                for (uint64_t x = 1; x + 1 < nx; ++x) {
+                    const uint64_t i = (uint64_t)z * sz + y * sy + x;
+                    const uint8_t f = fl[i];
+                    if (f == 1) { pn[i] = 0.0; continue; }
+                    if (f == 3) { pn[i] = hard; continue; }
+                    if (f != 0 && f != 2) continue;
+                    const double c = pc[i];
+                    double s = (fl[i + 1] == 1 ? c : pc[i + 1]) + (fl[i - 1] == 1 ? c : pc[i - 1]) +
+                               (fl[i + sy] == 1 ? c : pc[i + sy]) + (fl[i - sy] == 1 ? c : pc[i - sy]) +
+                               (fl[i + sz] == 1 ? c : pc[i + sz]) + (fl[i - sz] == 1 ? c : pc[i - sz]);
+                    pn[i] = 2.0 * c - pp[i] + c2dt2 * ((s - 6.0 * c) * inv_h2);
+                }
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+        for (int64_t b = 0; b < (int64_t)a->nb; ++b) {
+            const uint64_t i = a->bidx[b];
+            const double d = pc[i] - pp[i];
+            double in = d;
+            const double *k = a->coef64 + (uint64_t)a->bmat[b] * S * 5;
+            double *s = st + (uint64_t)b * S * 4;
+            for (uint32_t q = 0; q < S; ++q, k += 5, s += 4) {
+                double y = k[0] * in + k[1] * s[0] + k[2] * s[1] - k[3] * s[2] - k[4] * s[3];
+                s[1] = s[0]; s[0] = in; s[3] = s[2]; s[2] = y; in = y;
+            }
+            const double w = a->bw ? (double)a->bw[b] : 1.0;
+            if (a->form == 0) {
+                pn[i] -= a->K_d * (in * a->mix_y + d * a->mix_d) * a->gain * w;
+            } else {
+                const double kgw = a->K_d * a->gain * w, ac = kgw * a->mix_d * 0.5;
+                pn[i] = (pn[i] - kgw * in * a->mix_y + ac * pp[i]) / (1.0 + ac);
+            }
+        }
+        for (uint32_t s = 0; s < a->n_src; ++s) pn[a->src_idx[s]] += (double)sig_at(a, s, sn);
+        double *t = pp; pp = pc; pc = pn; pn = t;
+        for (uint32_t r = 0; r < a->n_rcv; ++r)
+            a->ir[(uint64_t)r * a->ir_stride + n] = (float)pc[a->rcv_idx[r]];
+    }
+    if (a->p) memcpy(a->p, pc, N * sizeof(double));
+    if (a->pprev) memcpy(a->pprev, pp, N * sizeof(double));
+    if (a->state) memcpy(a->state, st, nst * sizeof(double));
+    free(b0); free(b1); free(b2); free(st);
+    return 0;
+}
+
+/* Discrete energy of the lossless interior scheme (FP64):
+ *   E = sum_{i active} (p_i - q_i)^2
+ *     + lambda2 * sum_{links i~j} (p_i - p_j)(q_i - q_j)
+ * Active voxels are interior voxels with flag 0/2 (the ones the leapfrog
+ * updates).  A link joins an active voxel to a face neighbour that is active
+ * (counted once) or held fixed (border voxels and flag-3 voxels, counted
+ * once); links to walls (flag 1) carry nothing, which is the mirror rule of
+ * simulator_gpu.cu:70-81.  Without boundary filtering and with the fixed
+ * voxels at zero, the leapfrog keeps E constant up to rounding.
+ * p = p^n, q = p^{n-1}. */
+static inline int vo_active(uint64_t nx, uint64_t ny, uint64_t nz, const uint8_t *fl, uint64_t j)
+{
+    const uint64_t x = j % nx, y = (j / nx) % ny, z = j / (nx * ny);
+    if (x == 0 || y == 0 || z == 0 || x + 1 >= nx || y + 1 >= ny || z + 1 >= nz) return 0;
+    return fl[j] == 0 || fl[j] == 2;
+}
+
+VO_API double vo_energy_f32(uint64_t nx, uint64_t ny, uint64_t nz, const uint8_t *flags,
+                            const float *p, const float *q, double lambda2)
+{
+    const uint64_t sy = nx, sz = nx * ny;
+    double kin = 0.0, pot = 0.0;
+#pragma omp parallel for reduction(+ : kin, pot) schedule(static) num_threads(vo_get_threads())
+    for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+        for (uint64_t y = 1; y + 1 < ny; ++y)
+            for (uint64_t x = 1; x + 1 < nx; ++x) {
+                const uint64_t i = (uint64_t)z * sz + y * sy + x;
+                if (!vo_active(nx, ny, nz, flags, i)) continue;
+                const double d = (double)p[i] - (double)q[i];
+                kin += d * d;
+                const uint64_t fwd[3] = {i + 1, i + sy, i + sz};
+                const uint64_t bwd[3] = {i - 1, i - sy, i - sz};
+                for (int a = 0; a < 3; ++a) {
+                    uint64_t j = fwd[a];
+                    if (flags[j] != 1)
+                        pot += ((double)p[i] - (double)p[j]) * ((double)q[i] - (double)q[j]);
+                    j = bwd[a];
+                    if (flags[j] != 1 && !vo_active(nx, ny, nz, flags, j))
+                        pot += ((double)p[i] - (double)p[j]) * ((double)q[i] - (double)q[j]);
+                }
+            }
+    return kin + lambda2 * pot;
+}

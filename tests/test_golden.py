@@ -1,0 +1,76 @@
+"""Golden vectors produced by the reference's own CUDA kernels
+(tests/golden/make_golden.py): the oracle must reproduce them on the CPU,
+and the CUDA path through the C ABI on the GPU."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import rel_l2
+
+GOLD = Path(__file__).resolve().parent / "golden"
+CASES = sorted(p.stem for p in GOLD.glob("ref_*.npz"))
+
+
+def _load(name):
+    d = np.load(GOLD / f"{name}.npz")
+    return {k: d[k] for k in d.files}
+
+
+def _oracle_run(d):
+    shape = tuple(int(s) for s in d["shape"])
+    c = d["consts"]
+    sc = oracle.Scene(shape, d["flags_ref"], d["bidx"], np.zeros(d["bidx"].size, np.uint8),
+                      np.ones(d["bidx"].size, np.float32), d["coef"], 1, hard=np.full(10, 10.0, np.float32),
+                      rcv_idx=d["rcv"], consts=(c[1], c[2], c[3]))
+    n = int(np.prod(shape))
+    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(d["bidx"].size * 4 + 1, np.float32))
+    ir = sc.run(d["ir"].shape[1], state=st)
+    return ir, st[0]
+
+
+def test_golden_present():
+    assert len(CASES) >= 2, "golden vectors missing: run tests/golden/make_golden.py on a GPU"
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_classification_matches_reference_gpu(name):
+    d = _load(name)
+    shape = tuple(int(s) for s in d["shape"])
+    flags, _, _ = oracle.classify(shape, 1, d["flags_raw"])
+    assert np.array_equal(flags, d["flags_ref"])
+    assert np.array_equal(oracle.boundary_list(shape, flags), d["bidx"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_step_matches_reference_gpu(name):
+    d = _load(name)
+    ir, p = _oracle_run(d)
+    assert np.abs(d["ir"]).max() > 0
+    assert rel_l2(ir, d["ir"]) <= 1e-6
+    assert rel_l2(p, d["p_final"]) <= 1e-6
+    print(name, "bit-identical samples:", float(np.mean(ir.view(np.uint32) == d["ir"].view(np.uint32))))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_cuda_path_matches_reference_gpu(name):
+    from virs_b200 import capi
+    d = _load(name)
+    shape = tuple(int(s) for s in d["shape"])
+    p = capi.default_params(boundary_k=float(d["consts"][3]))
+    sim = capi.Simulation(p)
+    sim.set_grid(shape, float(d["h"]), d["flags_raw"])
+    sim.classify()
+    assert np.array_equal(sim.flags(), d["flags_ref"])
+    assert np.array_equal(sim.boundary_indices(), d["bidx"])
+    sim.set_filters(d["coef"][None, None, :])
+    sim.set_receivers(d["rcv"])
+    steps = d["ir"].shape[1]
+    sim.start(steps)
+    sim.run(steps)
+    got = sim.ir()
+    assert rel_l2(got, d["ir"]) <= 1e-6
+    assert rel_l2(sim.pressure(), d["p_final"]) <= 1e-6
+    sim.close()

@@ -1,0 +1,339 @@
+"""ctypes binding of include/virs.h (the library's C ABI).
+
+Thin and literal: one method per entry point, numpy arrays for host
+buffers, a VirsError carrying the status code and the library's message on
+any failure.  The library must have been built (``python -m
+virs_b200.build``); there is no fallback when it is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libvirs_b200.so"
+
+OK, E_ARG, E_OOM, E_CUDA, E_UNSTABLE, E_TIMEOUT, E_STATE, E_IO = range(8)
+STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_OOM", 3: "E_CUDA", 4: "E_UNSTABLE", 5: "E_TIMEOUT", 6: "E_STATE", 7: "E_IO"}
+STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2
+ROLE_IGNORE, ROLE_SOURCE = 0xFF, 0xFE
+BOUNDARY_REFERENCE, BOUNDARY_CENTERED = 0, 1
+
+
+class VirsError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("device", C.c_int32), ("sound_speed", C.c_float), ("courant", C.c_float),
+        ("cell_size", C.c_float), ("bbox_nudge", C.c_float), ("sponge_width", C.c_int32), ("storage", C.c_int32),
+        ("boundary_form", C.c_int32),
+        ("storage_scale", C.c_float), ("boundary_gain", C.c_float), ("boundary_k", C.c_float),
+        ("mix_filtered", C.c_double), ("mix_direct", C.c_double),
+    ]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [
+        ("nx", C.c_uint64), ("ny", C.c_uint64), ("nz", C.c_uint64), ("cell_size", C.c_float),
+        ("bbox_min", C.c_float * 3), ("dt", C.c_float), ("sample_rate", C.c_double),
+        ("boundary_count", C.c_uint64), ("steps_done", C.c_uint64),
+    ]
+
+
+class Timing(C.Structure):
+    _fields_ = [("step_kernel_ms", C.c_double), ("step_launches", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+
+_P = C.c_void_p
+_SIGS = {
+    "virs_last_error": ([], C.c_char_p),
+    "virs_params_default": ([_P], C.c_int),
+    "virs_create": ([_P, _P], C.c_int),
+    "virs_destroy": ([_P], C.c_int),
+    "virs_set_material_roles": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_load_obj": ([_P, C.c_char_p], C.c_int),
+    "virs_set_mesh": ([_P, _P, C.c_size_t, _P, _P, C.c_size_t], C.c_int),
+    "virs_set_grid": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, _P, _P], C.c_int),
+    "virs_get_grid_info": ([_P, _P], C.c_int),
+    "virs_classify": ([_P], C.c_int),
+    "virs_get_flags": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_get_normals": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_get_boundary_indices": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_get_boundary_materials": ([_P, _P, _P, C.c_size_t], C.c_int),
+    "virs_set_filters": ([_P, C.c_uint32, C.c_uint32, _P], C.c_int),
+    "virs_design_highpass": ([C.c_float, C.c_float, C.c_float, C.c_float, _P], C.c_int),
+    "virs_design_lowpass": ([C.c_float, C.c_float, C.c_float, C.c_float, _P], C.c_int),
+    "virs_design_first_order": ([C.c_double, C.c_double, C.c_double, _P], C.c_int),
+    "virs_design_octave_cascade": ([C.c_double, _P, _P, _P], C.c_int),
+    "virs_set_hard_source": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_set_sources": ([_P, C.c_uint32, _P, _P, C.c_size_t], C.c_int),
+    "virs_set_receivers": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_start_simulation": ([_P, C.c_uint64], C.c_int),
+    "virs_step": ([_P, C.c_uint32, _P, _P], C.c_int),
+    "virs_run": ([_P, C.c_uint64, _P], C.c_int),
+    "virs_run_host": ([_P, C.c_uint64, _P, _P, _P], C.c_int),
+    "virs_synchronize": ([_P], C.c_int),
+    "virs_get_ir": ([_P, C.c_uint64, C.c_uint64, _P], C.c_int),
+    "virs_get_pressure": ([_P, _P, _P, C.c_size_t], C.c_int),
+    "virs_set_pressure": ([_P, _P, _P, C.c_size_t], C.c_int),
+    "virs_init_pressure_sphere": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_int], C.c_int),
+    "virs_energy": ([_P, _P], C.c_int),
+    "virs_set_timing": ([_P, C.c_int], C.c_int),
+    "virs_get_timing": ([_P, _P], C.c_int),
+    "virs_set_tiling": ([_P, C.c_int, C.c_int], C.c_int),
+}
+
+EXPORTED = tuple(_SIGS)
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m virs_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().virs_last_error().decode()
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise VirsError(status, last_error())
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    check(lib().virs_params_default(C.byref(p)))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"no parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+def design_highpass(fs: float, cutoff: float, q: float, gain: float = 1.0) -> np.ndarray:
+    out = np.zeros(5, np.float32)
+    check(lib().virs_design_highpass(fs, cutoff, q, gain, _ptr(out)))
+    return out
+
+
+def design_lowpass(fs: float, cutoff: float, q: float, gain: float = 1.0) -> np.ndarray:
+    out = np.zeros(5, np.float32)
+    check(lib().virs_design_lowpass(fs, cutoff, q, gain, _ptr(out)))
+    return out
+
+
+def design_first_order(fs: float, reflection: float, fc: float) -> np.ndarray:
+    out = np.zeros(5, np.float64)
+    check(lib().virs_design_first_order(fs, reflection, fc, _ptr(out)))
+    return out
+
+
+def design_octave_cascade(fs: float, alpha, freqs=None) -> np.ndarray:
+    a = _c(alpha, np.float64)
+    f = None if freqs is None else _c(freqs, np.float64)
+    out = np.zeros(15, np.float64)
+    check(lib().virs_design_octave_cascade(fs, _ptr(a), _ptr(f), _ptr(out)))
+    return out.reshape(3, 5)
+
+
+class Simulation:
+    """One virs_sim handle."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        if params is None:
+            params = default_params(**kw)
+        self._h = C.c_void_p()
+        check(lib().virs_create(C.byref(params), C.byref(self._h)))
+        self.params = params
+
+    # lifetime ---------------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().virs_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # geometry ---------------------------------------------------------------
+    def set_material_roles(self, roles):
+        r = _c(roles, np.uint8)
+        check(lib().virs_set_material_roles(self._h, _ptr(r), r.size))
+
+    def load_obj(self, path):
+        check(lib().virs_load_obj(self._h, str(path).encode()))
+
+    def set_mesh(self, verts, tris, tri_material):
+        v = _c(verts, np.float32).reshape(-1, 3)
+        t = _c(tris, np.uint32).reshape(-1, 3)
+        m = _c(tri_material, np.int32)
+        check(lib().virs_set_mesh(self._h, _ptr(v), v.shape[0], _ptr(t), _ptr(m), t.shape[0]))
+
+    def set_grid(self, shape, cell_size, flags, wall_material=None):
+        nx, ny, nz = shape
+        f = _c(flags, np.uint8)
+        w = None if wall_material is None else _c(wall_material, np.uint8)
+        check(lib().virs_set_grid(self._h, nx, ny, nz, cell_size, _ptr(f), _ptr(w)))
+
+    def info(self) -> GridInfo:
+        g = GridInfo()
+        check(lib().virs_get_grid_info(self._h, C.byref(g)))
+        return g
+
+    @property
+    def shape(self):
+        g = self.info()
+        return (int(g.nx), int(g.ny), int(g.nz))
+
+    @property
+    def nvox(self):
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    def classify(self):
+        check(lib().virs_classify(self._h))
+
+    def flags(self) -> np.ndarray:
+        out = np.empty(self.nvox, np.uint8)
+        check(lib().virs_get_flags(self._h, _ptr(out), out.size))
+        return out
+
+    def normals(self) -> np.ndarray:
+        out = np.empty(self.nvox, np.uint8)
+        check(lib().virs_get_normals(self._h, _ptr(out), out.size))
+        return out
+
+    def boundary_indices(self) -> np.ndarray:
+        n = int(self.info().boundary_count)
+        out = np.empty(max(n, 1), np.uint32)
+        check(lib().virs_get_boundary_indices(self._h, _ptr(out), n))
+        return out[:n]
+
+    def boundary_materials(self):
+        n = int(self.info().boundary_count)
+        m = np.empty(max(n, 1), np.uint8)
+        w = np.empty(max(n, 1), np.float32)
+        check(lib().virs_get_boundary_materials(self._h, _ptr(m), _ptr(w), n))
+        return m[:n], w[:n]
+
+    # filters, sources, receivers ------------------------------------------------
+    def set_filters(self, coeffs, n_sections=None):
+        c = _c(coeffs, np.float32)
+        if n_sections is None:
+            n_sections = c.shape[-2] if c.ndim == 3 else 1
+        c = c.reshape(-1)
+        nm = c.size // (5 * n_sections)
+        check(lib().virs_set_filters(self._h, nm, n_sections, _ptr(c)))
+
+    def set_hard_source(self, values):
+        v = _c(values, np.float32)
+        check(lib().virs_set_hard_source(self._h, _ptr(v), v.size))
+
+    def set_sources(self, idx, signal):
+        i = _c(np.atleast_1d(idx), np.uint64)
+        s = _c(signal, np.float32).reshape(i.size, -1)
+        check(lib().virs_set_sources(self._h, i.size, _ptr(i), _ptr(s), s.shape[1]))
+
+    def set_receivers(self, idx):
+        i = _c(np.atleast_1d(idx), np.uint64)
+        check(lib().virs_set_receivers(self._h, i.size, _ptr(i)))
+        self._nrcv = i.size
+
+    # running ------------------------------------------------------------------
+    def start(self, steps: int):
+        check(lib().virs_start_simulation(self._h, steps))
+
+    def step(self, step: int):
+        keep = C.c_int(1)
+        v = C.c_float(0)
+        check(lib().virs_step(self._h, step, C.byref(keep), C.byref(v)))
+        return bool(keep.value), float(v.value)
+
+    def run(self, steps: int, stream: int | None = None):
+        check(lib().virs_run(self._h, steps, stream))
+
+    def run_host(self, steps: int, signal=None, ir_out=None, stream: int | None = None):
+        s = None if signal is None else _c(signal, np.float32)
+        check(lib().virs_run_host(self._h, steps, _ptr(s), _ptr(ir_out), stream))
+
+    def run_host_ptr(self, steps: int, signal_ptr, ir_ptr, stream: int | None = None):
+        check(lib().virs_run_host(self._h, steps, signal_ptr, ir_ptr, stream))
+
+    def synchronize(self):
+        check(lib().virs_synchronize(self._h))
+
+    def ir(self, first: int = 0, steps: int | None = None) -> np.ndarray:
+        if steps is None:
+            steps = int(self.info().steps_done) - first
+        n = getattr(self, "_nrcv", 0)
+        out = np.zeros((max(n, 1), steps), np.float32)
+        check(lib().virs_get_ir(self._h, first, steps, _ptr(out)))
+        return out[:n]
+
+    def pressure(self, prev: bool = False):
+        cur = np.empty(self.nvox, np.float32)
+        pp = np.empty(self.nvox, np.float32) if prev else None
+        check(lib().virs_get_pressure(self._h, _ptr(cur), _ptr(pp), cur.size))
+        return (cur, pp) if prev else cur
+
+    def set_pressure(self, cur, prev=None):
+        c = _c(cur, np.float32)
+        p = None if prev is None else _c(prev, np.float32)
+        check(lib().virs_set_pressure(self._h, _ptr(c), _ptr(p), c.size))
+
+    def init_pressure_sphere(self, x, y, z, radius, pressure, init=True):
+        check(lib().virs_init_pressure_sphere(self._h, x, y, z, radius, pressure, int(init)))
+
+    def energy(self) -> float:
+        e = C.c_double()
+        check(lib().virs_energy(self._h, C.byref(e)))
+        return float(e.value)
+
+    def set_timing(self, enable: bool):
+        check(lib().virs_set_timing(self._h, int(enable)))
+
+    def timing(self) -> Timing:
+        t = Timing()
+        check(lib().virs_get_timing(self._h, C.byref(t)))
+        return t
+
+    def set_tiling(self, rows: int = 0, planes: int = 0):
+        check(lib().virs_set_tiling(self._h, rows, planes))

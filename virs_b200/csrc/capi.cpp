@@ -1,0 +1,1126 @@
+// The C ABI of include/virs.h: one handle per simulation, all device memory
+// owned by the handle, every failure returned as a status with a message.
+//
+// Flow (the reference's, simulator.cpp:262-1025):
+//   virs_create -> virs_load_obj / virs_set_mesh / virs_set_grid
+//   -> virs_classify (GPU: sponge layer, normals, codes, boundary list)
+//   -> virs_set_filters / virs_set_sources / virs_set_receivers
+//   -> virs_start_simulation -> virs_run (graph) or virs_step (per step)
+//   -> virs_get_ir -> virs_destroy
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.hpp"
+
+#define VIRS_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace virs {
+
+namespace {
+thread_local std::string g_err;
+}
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+virs_status fail(virs_status st, const std::string &msg)
+{
+    g_err = msg;
+    return st;
+}
+
+virs_status cuda_fail(cudaError_t e, const char *what)
+{
+    g_err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return VIRS_E_OOM;
+    return VIRS_E_CUDA;
+}
+
+virs_status DevBuf::alloc(size_t n, const char *what)
+{
+    release();
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        return fail(VIRS_E_OOM, std::string("cudaMalloc of ") + std::to_string(n) + " bytes for " + what + " failed: " +
+                                    cudaGetErrorString(e));
+    }
+    bytes = n;
+    e = cudaMemset(ptr, 0, n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
+    return VIRS_OK;
+}
+
+} // namespace virs
+
+using namespace virs;
+
+struct virs_sim {
+    virs_params prm{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+
+    // geometry
+    bool has_grid = false, classified = false;
+    uint32_t nx = 0, ny = 0, nz = 0, px = 0, spr = 0;
+    size_t nvox = 0;      // padded voxels
+    size_t nref = 0;      // nx*ny*nz
+    float h = 0.f;
+    float bmin[3] = {0, 0, 0};
+    std::vector<uint8_t> roles;
+    uint8_t max_wall_mat = 0;
+
+    DevBuf flags_raw, wall_mat, flags, code, normals, bseg;
+    DevBuf field[2];
+    int cur = 0;
+
+    // boundary
+    uint64_t nb = 0;
+    DevBuf bidx, bmat, bw, state;
+
+    // filters
+    uint32_t nmat = 0, nsec = 0;
+    DevBuf coef;
+    bool filters_set = false;
+
+    // sources / receivers
+    DevBuf hard;
+    uint32_t nhard = 0;
+    std::vector<float> hard_host;
+    DevBuf src, sig;
+    uint32_t nsrc = 0;
+    uint64_t siglen = 0;
+    std::vector<uint64_t> src_ref;
+    std::vector<float> sig_host;   // unscaled [nsrc][siglen]
+    float sig_peak = 0.f;
+    DevBuf rcv;
+    uint32_t nrcv = 0;
+    std::vector<uint64_t> rcv_ref;
+    DevBuf ir;
+    uint64_t ircap = 0;
+    DevBuf ctr;
+    uint64_t steps_done = 0;
+
+    // constants
+    float dt = 0, c2dt2 = 0, inv_h2 = 0, K = 0;
+    double fs = 0;
+    float scale = 1.f, inv_scale = 1.f;
+
+    // kernel variant
+    int tile_rows = 8, zc = 0;
+
+    // CUDA graphs for GRAPH_STEPS steps, one per parity of `cur`
+    static constexpr int GRAPH_STEPS = 32;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_dirty = true;
+
+    // timing
+    bool timing = false;
+    double t_ms = 0;
+    uint64_t t_steps = 0, t_launch = 0;
+
+    // virs_step's RMS rule (simulator_gpu.cu:303-330)
+    std::vector<float> out0;
+    float rms_state = 0.f;
+
+    DevBuf energy_partial;
+
+    ~virs_sim()
+    {
+        drop_graphs();
+        if (done) cudaEventDestroy(done);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void drop_graphs()
+    {
+        for (auto &g : graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        graph_dirty = true;
+    }
+
+    size_t storage_bytes() const { return prm.storage == VIRS_STORAGE_F32 ? 4 : 2; }
+};
+
+namespace {
+
+bool finite_pos(float v) { return std::isfinite(v) && v > 0.f; }
+
+virs_status use_device(const virs_sim *s)
+{
+    VIRS_CUDA(cudaSetDevice(s->prm.device));
+    return VIRS_OK;
+}
+
+// step constants, simulator_gpu.cu:195-198 and :147, simulator.cpp:940-952
+void compute_constants(virs_sim *s)
+{
+    const float c = s->prm.sound_speed, h = s->h;
+    s->dt = s->prm.courant * h / (c * std::sqrt(3.f));
+    s->c2dt2 = c * c * s->dt * s->dt;
+    s->inv_h2 = 1.f / (h * h);
+    s->K = s->prm.boundary_k != 0.f ? s->prm.boundary_k : (c * s->dt) / h * 0.95f;
+    const double dtd = (double)s->prm.courant * (double)h / ((double)c * std::sqrt(3.0));
+    s->fs = 1.f / dtd;
+}
+
+virs_status upload_hard(virs_sim *s)
+{
+    std::vector<float> v(s->hard_host.size());
+    for (size_t i = 0; i < v.size(); ++i) v[i] = s->hard_host[i] * s->scale;
+    VIRS_TRY(s->hard.alloc(v.size() * sizeof(float), "hard source schedule"));
+    if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->hard.ptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+    s->nhard = (uint32_t)v.size();
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+
+// reference default filter: RBJ high-pass 440 Hz, Q 0.1 at fs = 1/dt
+// (simulator.cpp:955-967)
+virs_status default_filters(virs_sim *s)
+{
+    float k[5];
+    rbj_highpass((float)s->fs, 440.f, 0.1f, 1.f, k);
+    s->nmat = 1;
+    s->nsec = 1;
+    VIRS_TRY(s->coef.alloc(5 * sizeof(float), "filter coefficients"));
+    VIRS_CUDA(cudaMemcpy(s->coef.ptr, k, sizeof(k), cudaMemcpyHostToDevice));
+    s->filters_set = true;
+    return VIRS_OK;
+}
+
+virs_status alloc_states(virs_sim *s)
+{
+    VIRS_TRY(s->state.alloc(std::max<uint64_t>(s->nb, 1) * s->nsec * 4 * sizeof(float), "filter states"));
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+
+uint64_t to_dev(const virs_sim *s, uint64_t ref)
+{
+    const uint64_t x = ref % s->nx, y = (ref / s->nx) % s->ny, z = ref / ((uint64_t)s->nx * s->ny);
+    return (z * s->ny + y) * s->px + x;
+}
+
+bool interior(const virs_sim *s, uint64_t ref)
+{
+    const uint64_t x = ref % s->nx, y = (ref / s->nx) % s->ny, z = ref / ((uint64_t)s->nx * s->ny);
+    return x > 0 && y > 0 && z > 0 && x + 1 < s->nx && y + 1 < s->ny && z + 1 < s->nz;
+}
+
+// pitched copies between the reference layout (rows of nx) and the device
+// layout (rows of px)
+virs_status h2d_rows(void *dst, const void *src, size_t elem, const virs_sim *s)
+{
+    VIRS_CUDA(cudaMemcpy2D(dst, (size_t)s->px * elem, src, (size_t)s->nx * elem, (size_t)s->nx * elem,
+                           (size_t)s->ny * s->nz, cudaMemcpyHostToDevice));
+    return VIRS_OK;
+}
+
+virs_status d2h_rows(void *dst, const void *src, size_t elem, const virs_sim *s)
+{
+    VIRS_CUDA(cudaMemcpy2D(dst, (size_t)s->nx * elem, src, (size_t)s->px * elem, (size_t)s->nx * elem,
+                           (size_t)s->ny * s->nz, cudaMemcpyDeviceToHost));
+    return VIRS_OK;
+}
+
+virs_status wait_done(const virs_sim *s)
+{
+    VIRS_CUDA(cudaEventSynchronize(s->done));
+    return VIRS_OK;
+}
+
+// allocate the grid-sized buffers and upload flags / wall materials
+virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h, const uint8_t *flags,
+                         const uint8_t *wmat)
+{
+    if (nx < 3 || ny < 3 || nz < 3) return fail(VIRS_E_ARG, "grid must be at least 3 voxels along each axis");
+    if (nx > (1u << 30) || ny > (1u << 30) || nz > (1u << 30) || nx * ny * nz >= (1ull << 32))
+        return fail(VIRS_E_ARG, "grid too large: boundary indices are 32-bit (nx*ny*nz < 2^32)");
+    if (!finite_pos(h)) return fail(VIRS_E_ARG, "cell size must be finite and positive");
+    const size_t n = nx * ny * nz;
+    uint8_t mx = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (flags[i] > 3) return fail(VIRS_E_ARG, "flags must be 0..3 (flag " + std::to_string(flags[i]) + " at " + std::to_string(i) + ")");
+    if (wmat)
+        for (size_t i = 0; i < n; ++i) mx = std::max(mx, wmat[i]);
+    s->drop_graphs();
+    s->has_grid = s->classified = false;
+    s->nx = (uint32_t)nx;
+    s->ny = (uint32_t)ny;
+    s->nz = (uint32_t)nz;
+    s->px = (uint32_t)((nx + 31) / 32 * 32);
+    s->spr = (s->px + SEG - 1) / SEG;
+    s->nvox = (size_t)s->px * ny * nz;
+    s->nref = n;
+    s->h = h;
+    s->max_wall_mat = mx;
+    compute_constants(s);
+    // release the old grid first so that peak memory stays at one grid
+    for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
+                      &s->field[1], &s->bidx, &s->bmat, &s->bw, &s->state})
+        b->release();
+    VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
+    VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
+    VIRS_TRY(h2d_rows(s->flags_raw.ptr, flags, 1, s));
+    if (wmat) VIRS_TRY(h2d_rows(s->wall_mat.ptr, wmat, 1, s));
+    VIRS_TRY(s->flags.alloc(s->nvox, "classified flags"));
+    VIRS_TRY(s->field[0].alloc(s->nvox * s->storage_bytes(), "pressure field"));
+    VIRS_TRY(s->field[1].alloc(s->nvox * s->storage_bytes(), "pressure field"));
+    s->cur = 0;
+    s->nb = 0;
+    s->steps_done = 0;
+    // sources and receivers refer to voxel indices of the previous grid
+    s->nsrc = s->nrcv = 0;
+    s->src_ref.clear();
+    s->rcv_ref.clear();
+    s->has_grid = true;
+    return VIRS_OK;
+}
+
+virs_status install_mesh(virs_sim *s, const Mesh &m)
+{
+    float bmin[3], bmax[3];
+    mesh_bbox(m, s->prm.bbox_nudge, bmin, bmax);
+    const float h = s->prm.cell_size > 0.f ? s->prm.cell_size : 343.f / (22050.f * 2.f * 2.f);
+    uint64_t d[3];
+    grid_dims(bmin, bmax, h, d);
+    if (d[0] < 3 || d[1] < 3 || d[2] < 3) return fail(VIRS_E_ARG, "mesh bounding box gives a grid below 3 voxels per axis");
+    if (d[0] * d[1] * d[2] >= (1ull << 32)) return fail(VIRS_E_ARG, "mesh gives a grid of 2^32 voxels or more");
+    const size_t n = d[0] * d[1] * d[2];
+    std::vector<uint8_t> flags, wmat;
+    try {
+        flags.assign(n, 0);
+        wmat.assign(n, 0);
+    } catch (const std::bad_alloc &) {
+        return fail(VIRS_E_OOM, "host allocation of the voxel grid failed");
+    }
+    voxelize(m, s->roles, h, bmin, d[0], d[1], d[2], flags.data(), wmat.data());
+    VIRS_TRY(install_grid(s, d[0], d[1], d[2], h, flags.data(), wmat.data()));
+    std::memcpy(s->bmin, bmin, sizeof(bmin));
+    return VIRS_OK;
+}
+
+virs_status ensure_ir(virs_sim *s, uint64_t need)
+{
+    if (need <= s->ircap) return VIRS_OK;
+    uint64_t cap = std::max<uint64_t>(need, s->ircap ? s->ircap * 2 : 1024);
+    DevBuf nb;
+    VIRS_TRY(nb.alloc(std::max<uint32_t>(s->nrcv, 1) * cap * sizeof(float), "receiver samples"));
+    if (s->ircap && s->nrcv)
+        VIRS_CUDA(cudaMemcpy2D(nb.ptr, cap * sizeof(float), s->ir.ptr, s->ircap * sizeof(float),
+                               s->ircap * sizeof(float), s->nrcv, cudaMemcpyDeviceToDevice));
+    std::swap(s->ir.ptr, nb.ptr);
+    std::swap(s->ir.bytes, nb.bytes);
+    s->ircap = cap;
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+
+virs_status ready_to_run(virs_sim *s)
+{
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid: call virs_load_obj, virs_set_mesh or virs_set_grid");
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified: call virs_classify");
+    if (!s->filters_set) VIRS_TRY(default_filters(s));
+    if (s->nb && s->max_wall_mat >= s->nmat)
+        return fail(VIRS_E_ARG, "wall material " + std::to_string(s->max_wall_mat) + " has no filter (" +
+                                    std::to_string(s->nmat) + " materials set)");
+    if (!s->state.ptr) VIRS_TRY(alloc_states(s));
+    if (!s->ctr.ptr) VIRS_TRY(s->ctr.alloc(sizeof(uint32_t), "step counter"));
+    return VIRS_OK;
+}
+
+StepArgs step_args(const virs_sim *s, int parity)
+{
+    StepArgs a{};
+    a.p = s->field[parity].ptr;
+    a.q = s->field[parity ^ 1].ptr;
+    a.code = s->code.as<uint8_t>();
+    a.bseg = s->bseg.as<uint32_t>();
+    a.bmat = s->bmat.as<uint8_t>();
+    a.bw = s->bw.as<float>();
+    a.state = s->state.as<float>();
+    a.coef = s->coef.as<float>();
+    a.hard = s->hard.as<float>();
+    a.ctr = s->ctr.as<uint32_t>();
+    a.nb = s->nb;
+    a.nhard = s->nhard;
+    a.nsec = s->nsec;
+    a.nx = s->nx;
+    a.ny = s->ny;
+    a.nz = s->nz;
+    a.px = s->px;
+    a.spr = s->spr;
+    a.zc = s->zc;
+    a.c2dt2 = s->c2dt2;
+    a.inv_h2 = s->inv_h2;
+    a.K = (double)s->K;
+    a.mix_y = s->prm.mix_filtered;
+    a.mix_d = s->prm.mix_direct;
+    a.gain = (double)s->prm.boundary_gain;
+    a.form = s->prm.boundary_form;
+    return a;
+}
+
+PostArgs post_args(const virs_sim *s, int parity)
+{
+    PostArgs a{};
+    a.q = s->field[parity ^ 1].ptr;
+    a.src = s->src.as<uint64_t>();
+    a.sig = s->sig.as<float>();
+    a.rcv = s->rcv.as<uint64_t>();
+    a.ir = s->ir.as<float>();
+    a.ctr = s->ctr.as<uint32_t>();
+    a.nsrc = s->nsrc;
+    a.nrcv = s->nrcv;
+    a.siglen = s->siglen;
+    a.cap = s->ircap;
+    a.inv_scale = s->inv_scale;
+    return a;
+}
+
+cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
+{
+    cudaError_t e = launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
+    if (e != cudaSuccess) return e;
+    return launch_post(s->prm.storage, post_args(s, parity), st);
+}
+
+virs_status build_graphs(virs_sim *s, cudaStream_t st)
+{
+    s->drop_graphs();
+    for (int par = 0; par < 2; ++par) {
+        cudaGraph_t g = nullptr;
+        VIRS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < virs_sim::GRAPH_STEPS && e == cudaSuccess; ++i) e = enqueue_step(s, par ^ (i & 1), st);
+        cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e, "capturing the step loop");
+        }
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&s->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    s->graph_dirty = false;
+    return VIRS_OK;
+}
+
+virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
+{
+    VIRS_TRY(ready_to_run(s));
+    VIRS_TRY(ensure_ir(s, s->steps_done + n));
+    if (s->timing) {
+        std::vector<cudaEvent_t> ev(2 * n);
+        for (auto &e : ev) VIRS_CUDA(cudaEventCreate(&e));
+        cudaError_t err = cudaSuccess;
+        for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
+            const int par = s->cur ^ (int)(i & 1);
+            cudaEventRecord(ev[2 * i], st);
+            err = launch_step(s->prm.storage, s->tile_rows, step_args(s, par), st);
+            cudaEventRecord(ev[2 * i + 1], st);
+            if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
+        }
+        if (err == cudaSuccess) err = cudaEventSynchronize(ev.back());
+        double ms = 0;
+        for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
+            float t = 0;
+            err = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+            ms += t;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        if (err != cudaSuccess) return cuda_fail(err, "timed step loop");
+        s->t_ms += ms;
+        s->t_steps += n;
+        s->t_launch += 2 * n;
+    } else {
+        uint64_t i = 0;
+        if (n >= (uint64_t)virs_sim::GRAPH_STEPS) {
+            if (s->graph_dirty) VIRS_TRY(build_graphs(s, st));
+            for (; i + virs_sim::GRAPH_STEPS <= n; i += virs_sim::GRAPH_STEPS)
+                VIRS_CUDA(cudaGraphLaunch(s->graph[s->cur ^ (int)(i & 1)], st));
+        }
+        for (; i < n; ++i) {
+            cudaError_t e = enqueue_step(s, s->cur ^ (int)(i & 1), st);
+            if (e != cudaSuccess) return cuda_fail(e, "step launch");
+        }
+    }
+    s->cur ^= (int)(n & 1);
+    s->steps_done += n;
+    VIRS_CUDA(cudaEventRecord(s->done, st));
+    return VIRS_OK;
+}
+
+} // namespace
+
+// ============================================================================
+// exported entry points
+// ============================================================================
+
+VIRS_EXPORT const char *virs_last_error(void) { return g_err.c_str(); }
+
+VIRS_EXPORT virs_status virs_params_default(virs_params *p)
+{
+    if (!p) return fail(VIRS_E_ARG, "virs_params_default: null");
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = sizeof(virs_params);
+    p->device = 0;
+    p->sound_speed = 343.f;
+    p->courant = 0.5f;
+    p->cell_size = 0.f;
+    p->bbox_nudge = 0.1f;
+    p->sponge_width = 1;
+    p->storage = VIRS_STORAGE_F32;
+    p->boundary_form = VIRS_BOUNDARY_REFERENCE;
+    p->storage_scale = 0.f;
+    p->boundary_gain = 0.4f;
+    p->boundary_k = 0.f;
+    p->mix_filtered = 0.1;
+    p->mix_direct = 0.9;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_create(const virs_params *p, virs_sim **out)
+{
+    if (!out) return fail(VIRS_E_ARG, "virs_create: null output");
+    *out = nullptr;
+    virs_params prm;
+    if (p) {
+        if (p->struct_size != sizeof(virs_params))
+            return fail(VIRS_E_ARG, "virs_params.struct_size mismatch (header and library disagree)");
+        prm = *p;
+    } else {
+        virs_params_default(&prm);
+    }
+    if (!finite_pos(prm.sound_speed)) return fail(VIRS_E_ARG, "sound speed must be positive");
+    if (!finite_pos(prm.courant) || prm.courant > 1.f)
+        return fail(VIRS_E_ARG, "courant must be in (0, 1]: dt = courant*h/(c*sqrt(3)) and 1 is the 3D stability limit");
+    if (!(prm.cell_size >= 0.f) || !std::isfinite(prm.cell_size)) return fail(VIRS_E_ARG, "cell size must be >= 0");
+    if (prm.sponge_width < 1 || prm.sponge_width > 31) return fail(VIRS_E_ARG, "sponge width must be 1..31");
+    if (prm.storage < VIRS_STORAGE_F32 || prm.storage > VIRS_STORAGE_BF16) return fail(VIRS_E_ARG, "unknown storage");
+    if (prm.boundary_form != VIRS_BOUNDARY_REFERENCE && prm.boundary_form != VIRS_BOUNDARY_CENTERED)
+        return fail(VIRS_E_ARG, "unknown boundary form");
+    if (!(prm.storage_scale >= 0.f) || !std::isfinite(prm.storage_scale)) return fail(VIRS_E_ARG, "storage scale must be >= 0");
+    int ndev = 0;
+    VIRS_CUDA(cudaGetDeviceCount(&ndev));
+    if (prm.device < 0 || prm.device >= ndev) return fail(VIRS_E_ARG, "no CUDA device " + std::to_string(prm.device));
+    std::unique_ptr<virs_sim> s(new (std::nothrow) virs_sim());
+    if (!s) return fail(VIRS_E_OOM, "virs_create: host allocation failed");
+    s->prm = prm;
+    VIRS_TRY(use_device(s.get()));
+    // a blocking stream: it orders after the synchronous copies and memsets
+    // of the setup calls, which run on the legacy default stream
+    VIRS_CUDA(cudaStreamCreate(&s->stream));
+    VIRS_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    s->roles.assign(2, VIRS_ROLE_IGNORE);
+    s->roles[0] = 0;
+    s->roles[1] = VIRS_ROLE_SOURCE;
+    // simulator_gpu.cu:214-218: 10 for the first 10 steps
+    s->hard_host.assign(10, 10.f);
+    *out = s.release();
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_destroy(virs_sim *s)
+{
+    if (!s) return VIRS_OK;
+    cudaSetDevice(s->prm.device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_material_roles(virs_sim *s, const uint8_t *roles, size_t n)
+{
+    if (!s || (!roles && n)) return fail(VIRS_E_ARG, "virs_set_material_roles: null argument");
+    for (size_t i = 0; i < n; ++i)
+        if (roles[i] >= 64 && roles[i] != VIRS_ROLE_IGNORE && roles[i] != VIRS_ROLE_SOURCE)
+            return fail(VIRS_E_ARG, "role must be 0..63, VIRS_ROLE_SOURCE or VIRS_ROLE_IGNORE");
+    s->roles.assign(roles, roles + n);
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_load_obj(virs_sim *s, const char *path)
+{
+    if (!s || !path) return fail(VIRS_E_ARG, "virs_load_obj: null argument");
+    VIRS_TRY(use_device(s));
+    Mesh m;
+    VIRS_TRY(load_obj(path, m));
+    return install_mesh(s, m);
+}
+
+VIRS_EXPORT virs_status virs_set_mesh(virs_sim *s, const float *verts, size_t nverts, const uint32_t *tris,
+                                      const int32_t *tri_material, size_t ntris)
+{
+    if (!s || !verts || !tris || !tri_material || !nverts || !ntris)
+        return fail(VIRS_E_ARG, "virs_set_mesh: null or empty argument");
+    VIRS_TRY(use_device(s));
+    Mesh m;
+    m.verts.assign(verts, verts + 3 * nverts);
+    m.tris.assign(tris, tris + 3 * ntris);
+    m.tri_mat.assign(tri_material, tri_material + ntris);
+    for (uint32_t v : m.tris)
+        if (v >= nverts) return fail(VIRS_E_ARG, "virs_set_mesh: triangle vertex index out of range");
+    for (float v : m.verts)
+        if (!std::isfinite(v)) return fail(VIRS_E_ARG, "virs_set_mesh: non-finite vertex coordinate");
+    return install_mesh(s, m);
+}
+
+VIRS_EXPORT virs_status virs_set_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h,
+                                      const uint8_t *flags, const uint8_t *wmat)
+{
+    if (!s || !flags) return fail(VIRS_E_ARG, "virs_set_grid: null argument");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(install_grid(s, nx, ny, nz, h, flags, wmat));
+    s->bmin[0] = s->bmin[1] = s->bmin[2] = 0.f;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_grid_info(const virs_sim *s, virs_grid_info *o)
+{
+    if (!s || !o) return fail(VIRS_E_ARG, "virs_get_grid_info: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    o->nx = s->nx;
+    o->ny = s->ny;
+    o->nz = s->nz;
+    o->cell_size = s->h;
+    std::memcpy(o->bbox_min, s->bmin, sizeof(s->bmin));
+    o->dt = s->dt;
+    o->sample_rate = s->fs;
+    o->boundary_count = s->nb;
+    o->steps_done = s->steps_done;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_classify(virs_sim *s)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_classify: null");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    s->drop_graphs();
+    s->classified = false;
+    cudaStream_t st = s->stream;
+    const int W = s->prm.sponge_width;
+    {
+        DevBuf k1, k2, bmat_full, bd2_full, segcnt_tmp, scan_tmp, total, wtab;
+        VIRS_TRY(k1.alloc(s->nvox * 4, "sponge scratch"));
+        VIRS_TRY(k2.alloc(s->nvox * 4, "sponge scratch"));
+        VIRS_TRY(bmat_full.alloc(s->nvox, "sponge scratch"));
+        VIRS_TRY(bd2_full.alloc(s->nvox * 2, "sponge scratch"));
+        ClassifyArgs ca{};
+        ca.flags_in = s->flags_raw.as<uint8_t>();
+        ca.wall_mat = s->wall_mat.as<uint8_t>();
+        ca.flags_out = s->flags.as<uint8_t>();
+        ca.bmat_full = bmat_full.as<uint8_t>();
+        ca.bd2_full = bd2_full.as<uint16_t>();
+        ca.k1 = k1.as<uint32_t>();
+        ca.k2 = k2.as<uint32_t>();
+        ca.nx = s->nx;
+        ca.ny = s->ny;
+        ca.nz = s->nz;
+        ca.px = s->px;
+        ca.W = W;
+        VIRS_CUDA(launch_sponge(ca, st));
+        k1.release();
+        k2.release();
+
+        const size_t nseg = (size_t)s->spr * s->ny * s->nz;
+        VIRS_TRY(s->code.alloc(s->nvox, "cell codes"));
+        VIRS_TRY(s->normals.alloc(s->nvox, "normals"));
+        VIRS_TRY(s->bseg.alloc(nseg * 4, "boundary prefix"));
+        CodesArgs co{};
+        co.flags = s->flags.as<uint8_t>();
+        co.code = s->code.as<uint8_t>();
+        co.normals = s->normals.as<uint8_t>();
+        co.segcnt = s->bseg.as<uint32_t>();
+        co.nx = s->nx;
+        co.ny = s->ny;
+        co.nz = s->nz;
+        co.px = s->px;
+        co.spr = s->spr;
+        VIRS_CUDA(launch_codes(co, st));
+        VIRS_TRY(scan_tmp.alloc(scan_tmp_words(nseg) * 4, "scan scratch"));
+        VIRS_TRY(total.alloc(4, "boundary count"));
+        VIRS_CUDA(launch_scan(s->bseg.as<uint32_t>(), nseg, scan_tmp.as<uint32_t>(), total.as<uint32_t>(), st));
+        uint32_t nb = 0;
+        VIRS_CUDA(cudaMemcpyAsync(&nb, total.ptr, 4, cudaMemcpyDeviceToHost, st));
+        VIRS_CUDA(cudaStreamSynchronize(st));
+        s->nb = nb;
+
+        std::vector<float> wt((size_t)W * W + 1);
+        for (int d = 0; d <= W * W; ++d) wt[d] = sponge_weight(W, d);
+        VIRS_TRY(wtab.alloc(wt.size() * 4, "sponge weights"));
+        VIRS_CUDA(cudaMemcpy(wtab.ptr, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice));
+        VIRS_TRY(s->bidx.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary indices"));
+        VIRS_TRY(s->bmat.alloc(std::max<uint64_t>(nb, 1), "boundary materials"));
+        VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
+        CompactArgs cp{};
+        cp.flags = s->flags.as<uint8_t>();
+        cp.bseg = s->bseg.as<uint32_t>();
+        cp.bmat_full = bmat_full.as<uint8_t>();
+        cp.bd2_full = bd2_full.as<uint16_t>();
+        cp.wtab = wtab.as<float>();
+        cp.bidx = s->bidx.as<uint32_t>();
+        cp.bmat = s->bmat.as<uint8_t>();
+        cp.bw = s->bw.as<float>();
+        cp.nx = s->nx;
+        cp.ny = s->ny;
+        cp.nz = s->nz;
+        cp.px = s->px;
+        cp.spr = s->spr;
+        VIRS_CUDA(launch_compact(cp, st));
+        VIRS_CUDA(cudaStreamSynchronize(st));
+    }
+    s->state.release();
+    if (s->filters_set) VIRS_TRY(alloc_states(s));
+    s->classified = true;
+    VIRS_CUDA(cudaEventRecord(s->done, st));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_flags(const virs_sim *s, uint8_t *out, size_t n)
+{
+    if (!s || !out) return fail(VIRS_E_ARG, "virs_get_flags: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    if (n < s->nref) return fail(VIRS_E_ARG, "virs_get_flags: buffer smaller than nx*ny*nz");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    return d2h_rows(out, (s->classified ? s->flags : s->flags_raw).ptr, 1, s);
+}
+
+VIRS_EXPORT virs_status virs_get_normals(const virs_sim *s, uint8_t *out, size_t n)
+{
+    if (!s || !out) return fail(VIRS_E_ARG, "virs_get_normals: null argument");
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified");
+    if (n < s->nref) return fail(VIRS_E_ARG, "virs_get_normals: buffer smaller than nx*ny*nz");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    return d2h_rows(out, s->normals.ptr, 1, s);
+}
+
+VIRS_EXPORT virs_status virs_get_boundary_indices(const virs_sim *s, uint32_t *out, size_t n)
+{
+    if (!s || (!out && s->nb)) return fail(VIRS_E_ARG, "virs_get_boundary_indices: null argument");
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified");
+    if (n < s->nb) return fail(VIRS_E_ARG, "virs_get_boundary_indices: buffer smaller than the boundary count");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    if (s->nb) VIRS_CUDA(cudaMemcpy(out, s->bidx.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_boundary_materials(const virs_sim *s, uint8_t *mat, float *w, size_t n)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_get_boundary_materials: null");
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified");
+    if (n < s->nb) return fail(VIRS_E_ARG, "virs_get_boundary_materials: buffer smaller than the boundary count");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    if (s->nb && mat) VIRS_CUDA(cudaMemcpy(mat, s->bmat.ptr, s->nb, cudaMemcpyDeviceToHost));
+    if (s->nb && w) VIRS_CUDA(cudaMemcpy(w, s->bw.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_filters(virs_sim *s, uint32_t nm, uint32_t ns, const float *coeffs)
+{
+    if (!s || !coeffs) return fail(VIRS_E_ARG, "virs_set_filters: null argument");
+    if (nm < 1 || nm > 64 || ns < 1 || ns > 16) return fail(VIRS_E_ARG, "need 1..64 materials and 1..16 sections");
+    for (size_t i = 0; i < (size_t)nm * ns * 5; ++i)
+        if (!std::isfinite(coeffs[i])) return fail(VIRS_E_ARG, "non-finite filter coefficient");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(s->coef.alloc((size_t)nm * ns * 5 * 4, "filter coefficients"));
+    VIRS_CUDA(cudaMemcpy(s->coef.ptr, coeffs, (size_t)nm * ns * 5 * 4, cudaMemcpyHostToDevice));
+    s->nmat = nm;
+    s->nsec = ns;
+    s->filters_set = true;
+    s->graph_dirty = true;
+    if (s->classified) VIRS_TRY(alloc_states(s));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_design_highpass(float fs, float fc, float q, float g, float *out5)
+{
+    if (!out5) return fail(VIRS_E_ARG, "virs_design_highpass: null output");
+    rbj_highpass(fs, fc, q, g, out5);
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_design_lowpass(float fs, float fc, float q, float g, float *out5)
+{
+    if (!out5) return fail(VIRS_E_ARG, "virs_design_lowpass: null output");
+    rbj_lowpass(fs, fc, q, g, out5);
+    return VIRS_OK;
+}
+
+namespace {
+
+// the per-run scale of 16-bit storage: the largest source amplitude maps to
+// 2^10, leaving 2^6 of head-room below the FP16 maximum
+void choose_scale(virs_sim *s)
+{
+    if (s->prm.storage == VIRS_STORAGE_F32) {
+        s->scale = s->inv_scale = 1.f;
+        return;
+    }
+    if (s->prm.storage_scale > 0.f) {
+        s->scale = s->prm.storage_scale;
+    } else {
+        float peak = 0.f;
+        for (float v : s->hard_host) peak = std::max(peak, std::fabs(v));
+        peak = std::max(peak, s->sig_peak);
+        s->scale = peak > 0.f ? std::exp2f(std::round(std::log2(1024.f / peak))) : 1.f;
+    }
+    s->inv_scale = 1.f / s->scale;
+}
+
+} // namespace
+
+VIRS_EXPORT virs_status virs_set_hard_source(virs_sim *s, const float *v, size_t len)
+{
+    if (!s || (!v && len)) return fail(VIRS_E_ARG, "virs_set_hard_source: null argument");
+    if (len >= (1ull << 32)) return fail(VIRS_E_ARG, "schedule too long");
+    for (size_t i = 0; i < len; ++i)
+        if (!std::isfinite(v[i])) return fail(VIRS_E_ARG, "non-finite hard source value");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    s->hard_host.assign(v, v + len);
+    s->hard.release();
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_sources(virs_sim *s, uint32_t n, const uint64_t *idx, const float *sig, size_t len)
+{
+    if (!s || (n && (!idx || (!sig && len)))) return fail(VIRS_E_ARG, "virs_set_sources: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    std::vector<uint64_t> dev(n), sorted(idx, idx + n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (idx[i] >= s->nref) return fail(VIRS_E_ARG, "source index out of range");
+        if (!interior(s, idx[i])) return fail(VIRS_E_ARG, "sources must be interior voxels");
+        dev[i] = to_dev(s, idx[i]);
+    }
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+        return fail(VIRS_E_ARG, "source voxels must be distinct");
+    float peak = 0.f;
+    for (size_t i = 0; i < (size_t)n * len; ++i) {
+        if (!std::isfinite(sig[i])) return fail(VIRS_E_ARG, "non-finite source sample");
+        peak = std::max(peak, std::fabs(sig[i]));
+    }
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    s->sig_host.assign(sig, sig + (size_t)n * len);
+    s->sig_peak = peak;
+    VIRS_TRY(s->src.alloc(std::max<uint32_t>(n, 1) * 8, "source indices"));
+    if (n) VIRS_CUDA(cudaMemcpy(s->src.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
+    s->nsrc = n;
+    s->siglen = len;
+    s->src_ref.assign(idx, idx + n);
+    s->sig.release();
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_receivers(virs_sim *s, uint32_t n, const uint64_t *idx)
+{
+    if (!s || (n && !idx)) return fail(VIRS_E_ARG, "virs_set_receivers: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    std::vector<uint64_t> dev(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (idx[i] >= s->nref) return fail(VIRS_E_ARG, "receiver index out of range");
+        dev[i] = to_dev(s, idx[i]);
+    }
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(s->rcv.alloc(std::max<uint32_t>(n, 1) * 8, "receiver indices"));
+    if (n) VIRS_CUDA(cudaMemcpy(s->rcv.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
+    s->nrcv = n;
+    s->rcv_ref.assign(idx, idx + n);
+    s->ir.release();
+    s->ircap = 0;
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+
+namespace {
+virs_status upload_signals(virs_sim *s)
+{
+    std::vector<float> v(s->sig_host.size());
+    for (size_t i = 0; i < v.size(); ++i) v[i] = s->sig_host[i] * s->scale;
+    VIRS_TRY(s->sig.alloc(std::max<size_t>(v.size(), 1) * 4, "source signals"));
+    if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->sig.ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+    s->graph_dirty = true;
+    return VIRS_OK;
+}
+} // namespace
+
+VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_start_simulation: null");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(ready_to_run(s));
+    choose_scale(s);
+    VIRS_TRY(upload_hard(s));
+    VIRS_TRY(upload_signals(s));
+    s->ir.release();
+    s->ircap = 0;
+    VIRS_TRY(ensure_ir(s, std::max<uint64_t>(steps, 1)));
+    VIRS_CUDA(cudaMemset(s->field[0].ptr, 0, s->field[0].bytes));
+    VIRS_CUDA(cudaMemset(s->field[1].ptr, 0, s->field[1].bytes));
+    VIRS_CUDA(cudaMemset(s->state.ptr, 0, s->state.bytes));
+    VIRS_CUDA(cudaMemset(s->ctr.ptr, 0, 4));
+    s->cur = 0;
+    s->steps_done = 0;
+    s->out0.clear();
+    s->rms_state = 0.f;
+    s->drop_graphs();
+    VIRS_CUDA(cudaDeviceSynchronize());
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    return VIRS_OK;
+}
+
+namespace {
+bool started(const virs_sim *s) { return s->sig.ptr && s->hard.ptr && s->ir.ptr; }
+} // namespace
+
+VIRS_EXPORT virs_status virs_run(virs_sim *s, uint64_t steps, void *stream)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_run: null");
+    if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
+    VIRS_TRY(use_device(s));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    if (steps == 0) return VIRS_OK;
+    if (s->steps_done + steps >= (1ull << 32)) return fail(VIRS_E_ARG, "step counter would pass 2^32");
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    VIRS_CUDA(cudaStreamWaitEvent(st, s->done, 0));
+    return run_steps(s, steps, st);
+}
+
+VIRS_EXPORT virs_status virs_synchronize(virs_sim *s)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_synchronize: null");
+    VIRS_TRY(use_device(s));
+    return wait_done(s);
+}
+
+VIRS_EXPORT virs_status virs_run_host(virs_sim *s, uint64_t steps, const float *signal, float *ir_out, void *stream)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_run_host: null");
+    if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
+    VIRS_TRY(use_device(s));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    const uint64_t first = s->steps_done;
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    VIRS_CUDA(cudaStreamWaitEvent(st, s->done, 0));
+    if (signal && s->nsrc) {
+        if (first + steps > s->siglen)
+            return fail(VIRS_E_ARG, "virs_run_host: source signals were set for fewer steps than requested");
+        // the host samples of these steps, scaled like the stored field
+        const float *src = signal;
+        std::vector<float> scaled;
+        if (s->scale != 1.f) {
+            scaled.assign(signal, signal + (size_t)s->nsrc * steps);
+            for (float &v : scaled) v *= s->scale;
+            src = scaled.data();
+        }
+        VIRS_CUDA(cudaMemcpy2DAsync(s->sig.as<float>() + first, s->siglen * 4, src, steps * 4, steps * 4, s->nsrc,
+                                    cudaMemcpyHostToDevice, st));
+    }
+    VIRS_TRY(run_steps(s, steps, st));
+    if (ir_out && s->nrcv)
+        VIRS_CUDA(cudaMemcpy2DAsync(ir_out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
+                                    cudaMemcpyDeviceToHost, st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_step(virs_sim *s, uint32_t step, int *keep_going, float *sample)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_step: null");
+    if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(ready_to_run(s));
+    VIRS_TRY(ensure_ir(s, (uint64_t)step + 1));
+    cudaStream_t st = s->stream;
+    // the reference uploads the source value every step (simulator_gpu.cu:250-258)
+    VIRS_CUDA(cudaMemcpyAsync(s->ctr.ptr, &step, 4, cudaMemcpyHostToDevice, st));
+    cudaError_t e = enqueue_step(s, s->cur, st);
+    if (e != cudaSuccess) return cuda_fail(e, "step launch");
+    s->cur ^= 1;
+    s->steps_done = std::max<uint64_t>(s->steps_done, (uint64_t)step + 1);
+    float v = 0.f;
+    if (s->nrcv) VIRS_CUDA(cudaMemcpyAsync(&v, s->ir.as<float>() + step, 4, cudaMemcpyDeviceToHost, st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    VIRS_CUDA(cudaEventRecord(s->done, st));
+    if (sample) *sample = v;
+    if (!std::isfinite(v)) return fail(VIRS_E_UNSTABLE, "receiver sample is not finite at step " + std::to_string(step));
+    if (s->out0.size() <= step) s->out0.resize((size_t)step + 1, 0.f);
+    s->out0[step] = v;
+    bool go = true;
+    // simulator_gpu.cu:303-330
+    constexpr uint32_t RMS_SIZE = 100, MIN_RMS_CHECK_STEP = 3000;
+    if (step > MIN_RMS_CHECK_STEP) {
+        float sum = 0.0f;
+        for (uint32_t i = step - RMS_SIZE; i < step; ++i) sum += s->out0[i] * s->out0[i];
+        float rms = std::sqrt(sum / (float)RMS_SIZE);
+        if (step == MIN_RMS_CHECK_STEP + 1) {
+            s->rms_state = rms;
+        } else {
+            const float g = 0.00008f;
+            const float vout = (g * rms + s->rms_state) / (g + 1.f);
+            s->rms_state = 2.f * vout - s->rms_state;
+            rms = vout;
+        }
+        if (rms < 0.0009f) go = false;
+    }
+    if (keep_going) *keep_going = go ? 1 : 0;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_ir(const virs_sim *s, uint64_t first, uint64_t steps, float *out)
+{
+    if (!s || (!out && steps && s->nrcv)) return fail(VIRS_E_ARG, "virs_get_ir: null argument");
+    if (first + steps > s->steps_done) return fail(VIRS_E_ARG, "virs_get_ir: steps not run yet");
+    if (!s->nrcv || !steps) return VIRS_OK;
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_CUDA(cudaMemcpy2D(out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
+                           cudaMemcpyDeviceToHost));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_pressure(const virs_sim *s, float *cur, float *prev, size_t n)
+{
+    if (!s || !cur) return fail(VIRS_E_ARG, "virs_get_pressure: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    if (n < s->nref) return fail(VIRS_E_ARG, "virs_get_pressure: buffer smaller than nx*ny*nz");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    float *outs[2] = {cur, prev};
+    for (int k = 0; k < 2; ++k) {
+        if (!outs[k]) continue;
+        const DevBuf &f = s->field[s->cur ^ k];
+        if (s->prm.storage == VIRS_STORAGE_F32) {
+            VIRS_TRY(d2h_rows(outs[k], f.ptr, 4, s));
+        } else {
+            DevBuf tmp;
+            VIRS_TRY(tmp.alloc(s->nref * 4, "pressure export"));
+            VIRS_CUDA(launch_pack(s->prm.storage, f.ptr, tmp.as<float>(), s->nx, s->ny, s->nz, s->px, s->inv_scale,
+                                  s->stream));
+            VIRS_CUDA(cudaMemcpyAsync(outs[k], tmp.ptr, s->nref * 4, cudaMemcpyDeviceToHost, s->stream));
+            VIRS_CUDA(cudaStreamSynchronize(s->stream));
+        }
+    }
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_pressure(virs_sim *s, const float *cur, const float *prev, size_t n)
+{
+    if (!s || !cur) return fail(VIRS_E_ARG, "virs_set_pressure: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    if (n < s->nref) return fail(VIRS_E_ARG, "virs_set_pressure: buffer smaller than nx*ny*nz");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    const float *ins[2] = {cur, prev};
+    for (int k = 0; k < 2; ++k) {
+        DevBuf &f = s->field[s->cur ^ k];
+        if (!ins[k]) {
+            VIRS_CUDA(cudaMemset(f.ptr, 0, f.bytes));
+            continue;
+        }
+        if (s->prm.storage == VIRS_STORAGE_F32) {
+            VIRS_TRY(h2d_rows(f.ptr, ins[k], 4, s));
+        } else {
+            DevBuf tmp;
+            VIRS_TRY(tmp.alloc(s->nref * 4, "pressure import"));
+            VIRS_CUDA(cudaMemcpy(tmp.ptr, ins[k], s->nref * 4, cudaMemcpyHostToDevice));
+            VIRS_CUDA(launch_unpack(s->prm.storage, tmp.as<float>(), f.ptr, s->nx, s->ny, s->nz, s->px, s->scale,
+                                    s->stream));
+            VIRS_CUDA(cudaStreamSynchronize(s->stream));
+        }
+    }
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_init_pressure_sphere(virs_sim *s, uint64_t x, uint64_t y, uint64_t z, uint64_t r,
+                                                  float value, int init)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_init_pressure_sphere: null");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    // vectorspace.cpp / simulator_cpu.cpp:86-90 range checks
+    if (x >= s->nx || y >= s->ny || z >= s->nz) return fail(VIRS_E_ARG, "initPressureSphere: position out of range");
+    if (r > s->nx / 2 || r > s->ny / 2 || r > s->nz / 2)
+        return fail(VIRS_E_ARG, "initPressureSphere: radius exceeds half of grid dimensions");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_CUDA(launch_sphere(s->prm.storage, s->field[s->cur].ptr, s->nx, s->ny, s->nz, s->px, x, y, z, r,
+                            value * s->scale, init, s->stream));
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_energy(virs_sim *s, double *out)
+{
+    if (!s || !out) return fail(VIRS_E_ARG, "virs_energy: null argument");
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    const int nblocks = 148 * 8;
+    if (!s->energy_partial.ptr) VIRS_TRY(s->energy_partial.alloc((nblocks + 1) * sizeof(double), "energy partials"));
+    const double lambda2 = (double)s->c2dt2 * (double)s->inv_h2;
+    const double is2 = (double)s->inv_scale * (double)s->inv_scale;
+    VIRS_CUDA(launch_energy(s->prm.storage, s->field[s->cur].ptr, s->field[s->cur ^ 1].ptr, s->code.as<uint8_t>(),
+                            s->nx, s->ny, s->nz, s->px, lambda2, is2, s->energy_partial.as<double>(), nblocks,
+                            s->stream));
+    VIRS_CUDA(cudaMemcpyAsync(out, s->energy_partial.as<double>() + nblocks, sizeof(double), cudaMemcpyDeviceToHost,
+                              s->stream));
+    VIRS_CUDA(cudaStreamSynchronize(s->stream));
+    if (!std::isfinite(*out)) return fail(VIRS_E_UNSTABLE, "energy is not finite");
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_timing(virs_sim *s, int enable)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_set_timing: null");
+    s->timing = enable != 0;
+    s->t_ms = 0;
+    s->t_steps = s->t_launch = 0;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_timing(virs_sim *s, virs_timing *o)
+{
+    if (!s || !o) return fail(VIRS_E_ARG, "virs_get_timing: null argument");
+    o->step_kernel_ms = s->t_ms;
+    o->step_launches = s->t_steps;
+    o->kernel_launches = s->t_launch;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_tiling(virs_sim *s, int rows, int planes)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_set_tiling: null");
+    if (rows != 0 && rows != 4 && rows != 8 && rows != 16) return fail(VIRS_E_ARG, "tile rows must be 4, 8 or 16");
+    if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
+    VIRS_TRY(wait_done(s));
+    s->tile_rows = rows ? rows : 8;
+    s->zc = planes;
+    s->drop_graphs();
+    return VIRS_OK;
+}

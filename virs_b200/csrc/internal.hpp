@@ -1,0 +1,174 @@
+// Internal types shared by the host code and the kernels of libvirs_b200.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "virs.h"
+
+namespace virs {
+
+// ---- errors ----------------------------------------------------------------
+
+void set_error(const std::string &msg);
+virs_status fail(virs_status st, const std::string &msg);
+virs_status cuda_fail(cudaError_t e, const char *what);
+
+#define VIRS_CUDA(call)                                          \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return ::virs::cuda_fail(e_, #call); \
+    } while (0)
+
+#define VIRS_TRY(call)                       \
+    do {                                     \
+        virs_status s_ = (call);             \
+        if (s_ != VIRS_OK) return s_;        \
+    } while (0)
+
+// ---- device buffer -----------------------------------------------------------
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    virs_status alloc(size_t n, const char *what);   // zero-filled
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// ---- cell codes (one byte per voxel, padded layout) -------------------------
+//
+// The step kernel reads one byte per voxel instead of seven flags: for air
+// and boundary voxels the low six bits say which face neighbours are walls
+// (their value is replaced by the centre value, the mirror rule of
+// simulator_gpu.cu:70-81) and bit 7 marks a boundary voxel.
+constexpr uint8_t CODE_NONE = 0xFF;   // border / padding: never written
+constexpr uint8_t CODE_WALL = 0xFE;   // flag 1: p+ = 0
+constexpr uint8_t CODE_HARD = 0xFD;   // flag 3: p+ = hard source value
+constexpr uint8_t CODE_BND = 0x80;    // flag 2 (with the wall mask in bits 0-5)
+// wall-mask bits, in the reference's summation order
+constexpr uint8_t W_XP = 1, W_XM = 2, W_YP = 4, W_YM = 8, W_ZP = 16, W_ZM = 32;
+
+constexpr int SEG = 128;              // voxels per boundary-prefix segment
+
+// ---- kernel argument blocks -------------------------------------------------
+
+struct StepArgs {
+    const void *p;          // p^n (storage type)
+    void *q;                // in p^{n-1}, out p^{n+1}
+    const uint8_t *code;
+    const uint32_t *bseg;   // exclusive boundary prefix per 128-voxel segment
+    const uint8_t *bmat;
+    const float *bw;
+    float *state;           // [S][4][nb]
+    const float *coef;      // [M][S][5]
+    const float *hard;      // per-step hard source values (scaled)
+    const uint32_t *ctr;    // device step counter
+    uint64_t nb;
+    uint32_t nhard;
+    uint32_t nsec;
+    uint32_t nx, ny, nz, px, spr;
+    int zc;                 // planes per block
+    int form;               // VIRS_BOUNDARY_*
+    float c2dt2, inv_h2;
+    double K, mix_y, mix_d, gain;
+};
+
+struct PostArgs {
+    void *q;                // p^{n+1}
+    const uint64_t *src;    // device indices
+    const float *sig;       // [nsrc][siglen] (scaled)
+    const uint64_t *rcv;    // device indices
+    float *ir;              // [nrcv][cap]
+    uint32_t *ctr;
+    uint32_t nsrc, nrcv;
+    uint64_t siglen, cap;
+    float inv_scale;
+};
+
+// kernel launchers (kernels_step.cu)
+cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
+cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
+int default_planes(uint32_t nz);
+
+// classification launchers (kernels_classify.cu)
+struct ClassifyArgs {
+    const uint8_t *flags_in;   // padded
+    const uint8_t *wall_mat;   // padded
+    uint8_t *flags_out;        // padded
+    uint8_t *bmat_full;        // padded scratch
+    uint16_t *bd2_full;        // padded scratch
+    uint32_t *k1, *k2;         // padded scratch
+    uint32_t nx, ny, nz, px;
+    int W;
+};
+cudaError_t launch_sponge(const ClassifyArgs &a, cudaStream_t s);
+
+struct CodesArgs {
+    const uint8_t *flags;      // padded, classified
+    uint8_t *code;             // padded
+    uint8_t *normals;          // padded
+    uint32_t *segcnt;          // [nseg]
+    uint32_t nx, ny, nz, px, spr;
+};
+cudaError_t launch_codes(const CodesArgs &a, cudaStream_t s);
+// exclusive scan of n u32 values in place; tmp needs scan_tmp_words(n) words
+size_t scan_tmp_words(size_t n);
+cudaError_t launch_scan(uint32_t *data, size_t n, uint32_t *tmp, uint32_t *total, cudaStream_t s);
+
+struct CompactArgs {
+    const uint8_t *flags;      // padded, classified
+    const uint32_t *bseg;
+    const uint8_t *bmat_full;
+    const uint16_t *bd2_full;
+    const float *wtab;         // sponge weight per d2
+    uint32_t *bidx;
+    uint8_t *bmat;
+    float *bw;
+    uint32_t nx, ny, nz, px, spr;
+};
+cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);
+
+// misc kernels (kernels_misc.cu)
+cudaError_t launch_energy(int storage, const void *p, const void *q, const uint8_t *code, uint32_t nx, uint32_t ny,
+                          uint32_t nz, uint32_t px, double lambda2, double inv_scale2, double *partial,
+                          int nblocks, cudaStream_t s);
+cudaError_t launch_sphere(int storage, void *p, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px, uint64_t cx,
+                          uint64_t cy, uint64_t cz, uint64_t r, float value, int init, cudaStream_t s);
+cudaError_t launch_pack(int storage, const void *field, float *out, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t px,
+                        float inv_scale, cudaStream_t s);
+cudaError_t launch_unpack(int storage, const float *in, void *field, uint32_t nx, uint32_t ny, uint32_t nz,
+                          uint32_t px, float scale, cudaStream_t s);
+
+// ---- host-side geometry (voxelize.cpp, design.cpp) ---------------------------
+
+struct Mesh {
+    std::vector<float> verts;          // [n][3]
+    std::vector<uint32_t> tris;        // [t][3]
+    std::vector<int32_t> tri_mat;      // [t]
+};
+
+virs_status load_obj(const char *path, Mesh &out);
+void mesh_bbox(const Mesh &m, float nudge, float bmin[3], float bmax[3]);
+void grid_dims(const float bmin[3], const float bmax[3], float h, uint64_t dims[3]);
+void voxelize(const Mesh &m, const std::vector<uint8_t> &roles, float h, const float bmin[3], uint64_t nx,
+              uint64_t ny, uint64_t nz, uint8_t *flags, uint8_t *wall_mat);
+
+void rbj_highpass(float fs, float cutoff, float q, float gain, float out5[5]);
+void rbj_lowpass(float fs, float cutoff, float q, float gain, float out5[5]);
+float sponge_weight(int W, int d2);
+
+} // namespace virs

@@ -1,0 +1,403 @@
+// The FDTD step on the GPU: one fused kernel per time step.
+//
+// Semantics follow the reference step (src/simulator/simulator_gpu.cu):
+//   interior leapfrog with the wall mirror rule       :38-103
+//   boundary biquad correction, evaluated in double   :105-150
+// fused into one pass.  Layout and mapping:
+//   * fields are [nz][ny][px] with px = nx rounded up to 32 (rows start on
+//     128-byte lines); two buffers, p^{n+1} overwrites p^{n-1} in place
+//     (each output depends on p^{n-1} at its own voxel only);
+//   * a block owns a tile of TX = 32*VEC columns x TY rows and streams it
+//     along z over `zc` planes: p at z-1, z, z+1 live in registers, the
+//     plane z of the tile (plus one halo row above and below) sits in shared
+//     memory for the y neighbours, x neighbours come from warp shuffles and
+//     two halo loads per row; every load of plane z+1 is issued one plane
+//     ahead of its use;
+//   * one byte per voxel (the cell code) replaces the flags and the six
+//     neighbour flags of the reference;
+//   * boundary voxels are found without any index list: a warp covers
+//     consecutive voxels of one row, so a warp-wide exclusive scan of its
+//     boundary counts plus the per-128-voxel prefix `bseg` gives each
+//     boundary voxel its slot in the compacted (ascending index) order; the
+//     filter states are stored [section][4][slot] so the slots of one warp
+//     touch consecutive words.
+//
+// Arithmetic order is fixed with _rn intrinsics so that the result is
+// bit-identical to the CPU oracle: the reference CUDA build contracts
+// s - 6*p and t + c2dt2*lap into fused multiply-adds and flushes subnormals
+// (--use_fast_math); this file is compiled with -ftz=true.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "internal.hpp"
+
+namespace virs {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- storage types ------------------------------------------------------------
+
+template <typename T> struct Io;
+
+template <> struct Io<float> {
+    static constexpr int VEC = 4;
+    __device__ static void ld(const float *p, float (&r)[VEC])
+    {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+    }
+    __device__ static void ld_stream(const float *p, float (&r)[VEC])
+    {
+        const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+        r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+    }
+    __device__ static void st(float *p, const float (&r)[VEC])
+    {
+        __stcs(reinterpret_cast<float4 *>(p), make_float4(r[0], r[1], r[2], r[3]));
+    }
+    __device__ static float ld1(const float *p) { return *p; }
+    __device__ static float get(float v) { return v; }
+    __device__ static float put(float v) { return v; }
+};
+
+template <> struct Io<__half> {
+    static constexpr int VEC = 8;
+    __device__ static void unpack(const uint4 v, float (&r)[VEC])
+    {
+        const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(h[i]);
+            r[2 * i] = f.x;
+            r[2 * i + 1] = f.y;
+        }
+    }
+    __device__ static void ld(const __half *p, float (&r)[VEC]) { unpack(*reinterpret_cast<const uint4 *>(p), r); }
+    __device__ static void ld_stream(const __half *p, float (&r)[VEC]) { unpack(__ldcs(reinterpret_cast<const uint4 *>(p)), r); }
+    __device__ static void st(__half *p, const float (&r)[VEC])
+    {
+        uint4 v;
+        __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2half2_rn(r[2 * i], r[2 * i + 1]);
+        __stcs(reinterpret_cast<uint4 *>(p), v);
+    }
+    __device__ static float ld1(const __half *p) { return __half2float(*p); }
+    __device__ static float get(__half v) { return __half2float(v); }
+    __device__ static __half put(float v) { return __float2half_rn(v); }
+};
+
+template <> struct Io<__nv_bfloat16> {
+    static constexpr int VEC = 8;
+    __device__ static void unpack(const uint4 v, float (&r)[VEC])
+    {
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            r[2 * i] = f.x;
+            r[2 * i + 1] = f.y;
+        }
+    }
+    __device__ static void ld(const __nv_bfloat16 *p, float (&r)[VEC]) { unpack(*reinterpret_cast<const uint4 *>(p), r); }
+    __device__ static void ld_stream(const __nv_bfloat16 *p, float (&r)[VEC])
+    {
+        unpack(__ldcs(reinterpret_cast<const uint4 *>(p)), r);
+    }
+    __device__ static void st(__nv_bfloat16 *p, const float (&r)[VEC])
+    {
+        uint4 v;
+        __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(r[2 * i], r[2 * i + 1]);
+        __stcs(reinterpret_cast<uint4 *>(p), v);
+    }
+    __device__ static float ld1(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    __device__ static float get(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
+};
+
+template <int VEC> __device__ inline void ld_code(const uint8_t *p, uint8_t (&c)[VEC]);
+template <> __device__ inline void ld_code<4>(const uint8_t *p, uint8_t (&c)[4])
+{
+    const uchar4 v = __ldcs(reinterpret_cast<const uchar4 *>(p));
+    c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+}
+template <> __device__ inline void ld_code<8>(const uint8_t *p, uint8_t (&c)[8])
+{
+    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        c[i] = (v.x >> (8 * i)) & 0xff;
+        c[4 + i] = (v.y >> (8 * i)) & 0xff;
+    }
+}
+
+__device__ __forceinline__ float pick(uint8_t code, uint8_t bit, float centre, float nb)
+{
+    return (code & bit) ? centre : nb;
+}
+
+// simulator_gpu.cu:70-88 with the contractions of the reference build.
+__device__ __forceinline__ float leapfrog(uint8_t c, float ce, float xp, float xm, float yp, float ym, float zp,
+                                          float zm, float qv, float c2dt2, float inv_h2)
+{
+    float s = pick(c, W_XP, ce, xp);
+    s = __fadd_rn(s, pick(c, W_XM, ce, xm));
+    s = __fadd_rn(s, pick(c, W_YP, ce, yp));
+    s = __fadd_rn(s, pick(c, W_YM, ce, ym));
+    s = __fadd_rn(s, pick(c, W_ZP, ce, zp));
+    s = __fadd_rn(s, pick(c, W_ZM, ce, zm));
+    const float lap = __fmul_rn(__fmaf_rn(-6.0f, ce, s), inv_h2);
+    const float t = __fsub_rn(__fmul_rn(2.0f, ce), qv);
+    return __fmaf_rn(c2dt2, lap, t);
+}
+
+// simulator_gpu.cu:126-148: biquad sections in series on d = p - p^{n-1},
+// then p+ -= K*(0.1*y + 0.9*d)*0.4 (times the sponge weight) in double, or
+// the centered form of the same correction.
+__device__ __forceinline__ float boundary(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+{
+    const float d = __fsub_rn(ce, qv);
+    float in = d;
+    const uint64_t nb = a.nb;
+    const float *kc = a.coef + (uint64_t)__ldg(a.bmat + slot) * a.nsec * 5;
+    float *st = a.state + slot;
+    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5, st += 4 * nb) {
+        const float s0 = st[0], s1 = st[nb], s2 = st[2 * nb], s3 = st[3 * nb];
+        float y = __fmul_rn(__ldg(kc), in);
+        y = __fmaf_rn(__ldg(kc + 1), s0, y);
+        y = __fmaf_rn(__ldg(kc + 2), s1, y);
+        y = __fmaf_rn(-__ldg(kc + 3), s2, y);
+        y = __fmaf_rn(-__ldg(kc + 4), s3, y);
+        st[0] = in;
+        st[nb] = s0;
+        st[2 * nb] = y;
+        st[3 * nb] = s2;
+        in = y;
+    }
+    const double w = (double)__ldg(a.bw + slot);
+    if (a.form == VIRS_BOUNDARY_REFERENCE) {
+        const double t = __fma_rn((double)in, a.mix_y, __dmul_rn((double)d, a.mix_d));
+        const double u = __dmul_rn(__dmul_rn(__dmul_rn(a.K, t), a.gain), w);
+        return __double2float_rn(__dsub_rn((double)r, u));
+    }
+    // centered: the direct damping term at (p+ - p-)/2, solved for p+
+    const double kgw = __dmul_rn(__dmul_rn(a.K, a.gain), w);
+    const double ac = __dmul_rn(__dmul_rn(kgw, a.mix_d), 0.5);
+    const double num = __dadd_rn(__dsub_rn((double)r, __dmul_rn(kgw, __dmul_rn((double)in, a.mix_y))),
+                                 __dmul_rn(ac, (double)qv));
+    return __double2float_rn(__ddiv_rn(num, __dadd_rn(1.0, ac)));
+}
+
+template <typename T, int TY>
+__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const StepArgs a)
+{
+    using IO = Io<T>;
+    constexpr int VEC = IO::VEC;
+    constexpr int TX = 32 * VEC;
+    __shared__ __align__(16) float sm[2][TY + 2][TX];
+
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * TX;
+    const int x = x0 + lane * VEC;
+    const int y0 = blockIdx.y * TY;
+    const int y = y0 + ty;
+    const int z0 = 1 + blockIdx.z * a.zc;
+    const int z1 = min(z0 + a.zc, (int)a.nz - 1);
+    if (z0 >= z1) return; // uniform over the block
+
+    const int px = (int)a.px, ny = (int)a.ny;
+    const bool xin = x < px;
+    const bool act = xin && y < ny;
+    const size_t plane = (size_t)px * ny;
+    const T *P = static_cast<const T *>(a.p);
+    T *Q = static_cast<T *>(a.q);
+    const size_t own = (size_t)y * px + x;
+
+    // warp 0 also carries the halo row above the tile, the last warp the one below
+    int hslot = -1, hrow = 0;
+    if (ty == 0 && y0 >= 1) { hslot = 0; hrow = y0 - 1; }
+    if (ty == TY - 1 && y0 + TY < ny) { hslot = TY + 1; hrow = y0 + TY; }
+    const bool hact = hslot >= 0 && xin;
+    const size_t hoff = (size_t)hrow * px + x;
+    const bool has_l = lane == 0 && x0 >= 1;
+    const bool has_r = lane == 31 && x0 + TX < px;
+
+    for (int i = threadIdx.y * 32 + lane; i < 2 * (TY + 2) * TX; i += 32 * TY) (&sm[0][0][0])[i] = 0.f;
+    __syncthreads();
+
+    float cm[VEC], cc[VEC], cp[VEC], qv[VEC], qn[VEC], hv[VEC];
+    uint8_t cd[VEC], cdn[VEC];
+    float hl = 0.f, hr = 0.f, hln = 0.f, hrn = 0.f;
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) { cm[k] = cc[k] = cp[k] = qv[k] = qn[k] = hv[k] = 0.f; cd[k] = cdn[k] = CODE_NONE; }
+
+    {
+        const size_t zo = (size_t)z0 * plane;
+        if (act) {
+            IO::ld(P + zo - plane + own, cm);
+            IO::ld(P + zo + own, cc);
+            IO::ld_stream(Q + zo + own, qv);
+            ld_code<VEC>(a.code + zo + own, cd);
+            if (has_l) hl = IO::ld1(P + zo + own - 1);
+            if (has_r) hr = IO::ld1(P + zo + own + VEC);
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) sm[0][ty + 1][lane * VEC + k] = cc[k];
+        }
+        if (hact) {
+            IO::ld(P + zo + hoff, hv);
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) sm[0][hslot][lane * VEC + k] = hv[k];
+        }
+    }
+    __syncthreads();
+
+    const uint64_t seg0 = (uint64_t)x0 / SEG;
+    for (int z = z0; z < z1; ++z) {
+        const int b = (z - z0) & 1;
+        const size_t zc = (size_t)z * plane, zn = zc + plane;
+        // loads for plane z+1, consumed in the next iteration
+        if (act) {
+            IO::ld(P + zn + own, cp);
+            if (z + 1 < z1) {
+                IO::ld_stream(Q + zn + own, qn);
+                ld_code<VEC>(a.code + zn + own, cdn);
+            }
+            if (has_l) hln = IO::ld1(P + zn + own - 1);
+            if (has_r) hrn = IO::ld1(P + zn + own + VEC);
+        }
+        if (hact) IO::ld(P + zn + hoff, hv);
+
+        float left = __shfl_up_sync(FULL, cc[VEC - 1], 1);
+        float right = __shfl_down_sync(FULL, cc[0], 1);
+        if (lane == 0) left = hl;
+        if (lane == 31) right = hr;
+
+        float r[VEC];
+        unsigned bmask = 0;
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            const uint8_t c = cd[k];
+            const float ym = sm[b][ty][lane * VEC + k];
+            const float yp = sm[b][ty + 2][lane * VEC + k];
+            const float xm = k == 0 ? left : cc[k - 1];
+            const float xp = k == VEC - 1 ? right : cc[k + 1];
+            if (c >= CODE_HARD) {
+                if (c == CODE_NONE) r[k] = qv[k];
+                else if (c == CODE_WALL) r[k] = 0.f;
+                else {
+                    const uint32_t sn = __ldg(a.ctr);
+                    r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
+                }
+            } else {
+                r[k] = leapfrog(c, cc[k], xp, xm, yp, ym, cp[k], cm[k], qv[k], a.c2dt2, a.inv_h2);
+                if (c & CODE_BND) bmask |= 1u << k;
+            }
+        }
+
+        const int cnt = __popc(bmask);
+        if (__any_sync(FULL, cnt != 0)) {
+            int inc = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (cnt) {
+                uint64_t slot = (uint64_t)__ldg(a.bseg + ((uint64_t)z * ny + y) * a.spr + seg0) + (inc - cnt);
+#pragma unroll
+                for (int k = 0; k < VEC; ++k)
+                    if (bmask & (1u << k)) r[k] = boundary(a, r[k], cc[k], qv[k], slot++);
+            }
+        }
+
+        if (act) {
+            IO::st(Q + zc + own, r);
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) sm[b ^ 1][ty + 1][lane * VEC + k] = cp[k];
+        }
+        if (hact) {
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) sm[b ^ 1][hslot][lane * VEC + k] = hv[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+            cm[k] = cc[k];
+            cc[k] = cp[k];
+            qv[k] = qn[k];
+            cd[k] = cdn[k];
+        }
+        hl = hln;
+        hr = hrn;
+    }
+}
+
+// Additive sources, then receivers, then the step counter
+// (simulator_gpu.cu:292-300: the receiver reads the new field).
+template <typename T> __global__ void k_post(const PostArgs a)
+{
+    using IO = Io<T>;
+    T *Q = static_cast<T *>(a.q);
+    const uint32_t sn = *a.ctr;
+    for (uint32_t i = threadIdx.x; i < a.nsrc; i += blockDim.x) {
+        const float v = sn < a.siglen ? a.sig[(uint64_t)i * a.siglen + sn] : 0.f;
+        const uint64_t j = a.src[i];
+        Q[j] = IO::put(__fadd_rn(IO::get(Q[j]), v));
+    }
+    __syncthreads();
+    if (sn < a.cap)
+        for (uint32_t r = threadIdx.x; r < a.nrcv; r += blockDim.x)
+            a.ir[(uint64_t)r * a.cap + sn] = __fmul_rn(IO::get(Q[a.rcv[r]]), a.inv_scale);
+    __syncthreads();
+    if (threadIdx.x == 0) *a.ctr = sn + 1;
+}
+
+template <typename T>
+cudaError_t launch_step_t(int tile_rows, const StepArgs &a, cudaStream_t s)
+{
+    constexpr int TX = 32 * Io<T>::VEC;
+    if (a.nz < 3 || a.ny < 3 || a.nx < 3) return cudaSuccess;
+    const int zc = a.zc > 0 ? a.zc : default_planes(a.nz);
+    StepArgs b = a;
+    b.zc = zc;
+    const unsigned gx = (a.px + TX - 1) / TX;
+    const unsigned gz = (a.nz - 2 + zc - 1) / zc;
+    switch (tile_rows) {
+    case 4: k_step<T, 4><<<dim3(gx, (a.ny + 3) / 4, gz), dim3(32, 4), 0, s>>>(b); break;
+    case 16: k_step<T, 16><<<dim3(gx, (a.ny + 15) / 16, gz), dim3(32, 16), 0, s>>>(b); break;
+    default: k_step<T, 8><<<dim3(gx, (a.ny + 7) / 8, gz), dim3(32, 8), 0, s>>>(b); break;
+    }
+    return cudaGetLastError();
+}
+
+} // namespace
+
+int default_planes(uint32_t nz)
+{
+    (void)nz;
+    return 32;
+}
+
+cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s)
+{
+    switch (storage) {
+    case VIRS_STORAGE_F16: return launch_step_t<__half>(tile_rows, a, s);
+    case VIRS_STORAGE_BF16: return launch_step_t<__nv_bfloat16>(tile_rows, a, s);
+    default: return launch_step_t<float>(tile_rows, a, s);
+    }
+}
+
+cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s)
+{
+    switch (storage) {
+    case VIRS_STORAGE_F16: k_post<__half><<<1, 256, 0, s>>>(a); break;
+    case VIRS_STORAGE_BF16: k_post<__nv_bfloat16><<<1, 256, 0, s>>>(a); break;
+    default: k_post<float><<<1, 256, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+} // namespace virs

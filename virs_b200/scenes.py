@@ -1,0 +1,248 @@
+"""Seeded synthetic scenes for the FDTD path.
+
+There are no public datasets for this path; every workload is generated here
+from a documented seed: axis-aligned room meshes (12 triangles per box, the
+shape of a Blender-exported shoebox), per-face OBJ material ids, source
+signals, receiver positions, and absorbing-filter designs.
+
+Workloads (sizes as the benchmark configurations name them):
+  plain_small      4.0 x 3.0 x 2.5 m shoebox at h = 0.025 m -> 160x120x100,
+                   Courant 1/sqrt(3), 6 walls with one first-order absorber
+                   each (reflection uniform in [0.6, 0.95]), sponge width 8,
+                   differentiated-Gaussian source (sigma 8 steps), 1 receiver,
+                   2000 steps
+  furnished_room   8 x 6 x 3 m shoebox + 20 boxes (0.3-2 m) at h = 1/64 m ->
+                   512x384x192, 4 materials of 3-section octave cascades
+                   (absorption in [0.05, 0.8]), sponge 16, 4 receivers, 10000
+                   steps
+  large_hall       16 x 12 x 8 m hall at h = 1/64 m -> 1024x768x512, 2
+                   materials of 3-section cascades, Gaussian pulse source, 8
+                   receivers, 4000 steps, sponge width 1
+  reference_room   the reference's defaults on a small grid: one material, RBJ
+                   high-pass 440 Hz Q 0.1, a speaker box voxelised as hard
+                   source (flag 3, 10 for 10 steps), sponge 1, Courant 0.5/sqrt 3
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# face order of box(): -x, +x, -y, +y, -z, +z (two triangles each)
+FACES = ("-x", "+x", "-y", "+y", "-z", "+z")
+
+
+def box(lo, hi, face_materials):
+    """Axis-aligned box as 8 vertices and 12 triangles; face_materials is one
+    OBJ material id per face (FACES order) or one id for all faces."""
+    x0, y0, z0 = (float(v) for v in lo)
+    x1, y1, z1 = (float(v) for v in hi)
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x0, y1, z0], [x1, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x0, y1, z1], [x1, y1, z1]], np.float32)
+    quads = [(0, 2, 6, 4), (1, 5, 7, 3), (0, 4, 5, 1), (2, 3, 7, 6), (0, 1, 3, 2), (4, 6, 7, 5)]
+    fm = np.broadcast_to(np.asarray(face_materials, np.int32), (6,))
+    tris, mats = [], []
+    for q, m in zip(quads, fm):
+        tris += [(q[0], q[1], q[2]), (q[0], q[2], q[3])]
+        mats += [m, m]
+    return v, np.array(tris, np.uint32), np.array(mats, np.int32)
+
+
+def merge(*meshes):
+    vs, ts, ms, off = [], [], [], 0
+    for v, t, m in meshes:
+        vs.append(v)
+        ts.append(t + off)
+        ms.append(m)
+        off += v.shape[0]
+    return np.concatenate(vs), np.concatenate(ts), np.concatenate(ms)
+
+
+def diff_gaussian(n: int, sigma: float, amp: float = 1.0, delay: float | None = None) -> np.ndarray:
+    """Differentiated Gaussian pulse -(t - t0)/sigma^2 exp(-(t - t0)^2 / 2 sigma^2),
+    scaled to peak |amp|, t in steps, t0 = 4 sigma."""
+    t0 = 4.0 * sigma if delay is None else delay
+    t = np.arange(n, dtype=np.float64)
+    s = -(t - t0) / sigma**2 * np.exp(-((t - t0) ** 2) / (2 * sigma**2))
+    return (amp * s / np.abs(s).max()).astype(np.float32)
+
+
+def gaussian(n: int, sigma: float, amp: float = 1.0, delay: float | None = None) -> np.ndarray:
+    t0 = 4.0 * sigma if delay is None else delay
+    t = np.arange(n, dtype=np.float64)
+    return (amp * np.exp(-((t - t0) ** 2) / (2 * sigma**2))).astype(np.float32)
+
+
+@dataclass
+class Scene:
+    """A complete workload: mesh, parameters, filters, sources, receivers."""
+    name: str
+    verts: np.ndarray
+    tris: np.ndarray
+    tri_mat: np.ndarray
+    roles: np.ndarray
+    cell_size: float
+    nudge: float
+    courant: float
+    sponge_width: int
+    steps: int
+    n_materials: int
+    n_sections: int
+    coef64: np.ndarray | None = None       # [M][S][5] FP64 design (None = reference high-pass)
+    src_pos: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))   # world metres
+    src_sig: np.ndarray | None = None      # [n_src][steps]
+    rcv_pos: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    hard: np.ndarray | None = None         # flag-3 schedule (None = reference 10 x 10)
+    seed: int = 0
+
+    @property
+    def coef32(self):
+        return None if self.coef64 is None else self.coef64.astype(np.float32)
+
+
+def _interior_points(rng, lo, hi, n, margin):
+    lo = np.asarray(lo, np.float64) + margin
+    hi = np.asarray(hi, np.float64) - margin
+    return rng.uniform(lo, hi, (n, 3))
+
+
+def plain_small(seed: int = 1, steps: int = 2000) -> Scene:
+    rng = np.random.default_rng(seed)
+    L = (4.0, 3.0, 2.5)
+    h = 0.025
+    v, t, m = box((0, 0, 0), L, np.arange(6))
+    fs = fs_of(h, 1.0)
+    R = rng.uniform(0.6, 0.95, 6)
+    coef = np.stack([design_first_order_np(fs, r, 1000.0) for r in R])[:, None, :]
+    src = _interior_points(rng, (0, 0, 0), L, 1, 0.5)
+    rcv = _interior_points(rng, (0, 0, 0), L, 1, 0.5)
+    sig = diff_gaussian(steps, 8.0)[None, :]
+    return Scene("plain_small", v, t, m, np.arange(6, dtype=np.uint8), h, 0.0, 1.0, 8, steps, 6, 1, coef,
+                 src, sig, rcv, seed=seed)
+
+
+def furnished_room(seed: int = 2, steps: int = 10000, n_boxes: int = 20) -> Scene:
+    rng = np.random.default_rng(seed)
+    L = np.array([8.0, 6.0, 3.0])
+    h = 1.0 / 64.0
+    meshes = [box((0, 0, 0), L, [2, 2, 3, 3, 0, 1])]      # walls 2/3, floor 0, ceiling 1
+    boxes = []
+    for _ in range(n_boxes):
+        size = rng.uniform(0.3, 2.0, 3)
+        size[2] = min(size[2], 2.2)
+        lo = rng.uniform([0.3, 0.3, 0.0], L - size - [0.3, 0.3, 0.5])
+        lo[2] = 0.0                                         # on the floor
+        lo = np.round(lo * 64) / 64
+        hi = np.round((lo + size) * 64) / 64
+        boxes.append((lo, hi))
+        meshes.append(box(lo, hi, int(rng.integers(0, 4))))
+    v, t, m = merge(*meshes)
+    fs = fs_of(h, 1.0)
+    alpha = rng.uniform(0.05, 0.8, (4, 3))
+    coef = np.stack([design_octave_cascade_np(fs, a) for a in alpha])
+    pts = _free_points(rng, L, boxes, 5, 0.6)
+    sig = diff_gaussian(steps, 8.0)[None, :]
+    return Scene("furnished_room", v, t, m, np.arange(4, dtype=np.uint8), h, 0.0, 1.0, 16, steps, 4, 3, coef,
+                 pts[:1], sig, pts[1:], seed=seed)
+
+
+def large_hall(seed: int = 3, steps: int = 4000, size=(1024, 768, 512), h: float = 1.0 / 64.0) -> Scene:
+    rng = np.random.default_rng(seed)
+    L = np.array(size, np.float64) * h
+    v, t, m = box((0, 0, 0), L, [0, 0, 0, 0, 1, 0])        # floor material 1, the rest 0
+    fs = fs_of(h, 1.0)
+    alpha = rng.uniform(0.05, 0.8, (2, 3))
+    coef = np.stack([design_octave_cascade_np(fs, a) for a in alpha])
+    src = _interior_points(rng, (0, 0, 0), L, 1, 1.0)
+    rcv = _interior_points(rng, (0, 0, 0), L, 8, 1.0)
+    sig = gaussian(steps, 8.0)[None, :]
+    return Scene("large_hall", v, t, m, np.array([0, 1], np.uint8), h, 0.0, 1.0, 1, steps, 2, 3, coef,
+                 src, sig, rcv, seed=seed)
+
+
+def reference_room(seed: int = 4, steps: int = 300, size=(48, 40, 32), h: float = 0.05) -> Scene:
+    """The reference's configuration on a small grid: material 0 walls,
+    material 1 a speaker box (hard source), default filter and constants."""
+    rng = np.random.default_rng(seed)
+    L = np.array(size, np.float64) * h
+    room = box((0, 0, 0), L, 0)
+    c = rng.uniform(L * 0.3, L * 0.5)
+    spk = box(c, c + 2.2 * h, 1)
+    v, t, m = merge(room, spk)
+    rcv = _interior_points(rng, (0, 0, 0), L, 3, 4 * h)
+    return Scene("reference_room", v, t, m, np.array([0, 0xFE], np.uint8), h, 0.1, 0.5, 1, steps, 1, 1, None,
+                 np.zeros((0, 3)), None, rcv, seed=seed)
+
+
+def _free_points(rng, L, boxes, n, margin):
+    out = []
+    while len(out) < n:
+        p = rng.uniform(margin, L - margin)
+        if all(not np.all((p > lo - margin) & (p < hi + margin)) for lo, hi in boxes):
+            out.append(p)
+    return np.array(out)
+
+
+# ---- small helpers that only need numpy (the library has the same designs) ----
+
+def fs_of(h: float, courant: float, c: float = 343.0) -> float:
+    """1/dt in double as the filter design sees it (simulator.cpp:940-952)."""
+    dt = float(np.float32(courant)) * float(np.float32(h)) / (c * np.sqrt(3.0))
+    return 1.0 / dt
+
+
+def design_first_order_np(fs: float, reflection: float, fc: float) -> np.ndarray:
+    from . import capi
+    return capi.design_first_order(fs, reflection, fc)
+
+
+def design_octave_cascade_np(fs: float, alpha) -> np.ndarray:
+    from . import capi
+    return capi.design_octave_cascade(fs, alpha)
+
+
+def voxel_index(pos, bbox_min, h, shape) -> np.ndarray:
+    """World position -> reference voxel index (Simulator::getGridIdxFromVecPos,
+    simulator.h:32-35: toVoxel then truncation)."""
+    nx, ny, nz = shape
+    p = np.atleast_2d(np.asarray(pos, np.float32))
+    v = (p - np.asarray(bbox_min, np.float32)) / np.float32(h)
+    ix = v.astype(np.int64)
+    ix = np.clip(ix, 1, np.array([nx - 2, ny - 2, nz - 2]))
+    return (ix[:, 2] * ny + ix[:, 1]) * nx + ix[:, 0]
+
+
+def boundary_form(sc: Scene) -> int:
+    """The reference's explicit boundary correction for the reference
+    Courant number (0.5/sqrt 3); the centered form at the 3D limit, where a
+    thick explicit damping layer diverges."""
+    return 0 if sc.courant <= 0.5 else 1
+
+
+def build_simulation(sc: Scene, *, storage: int = 0, device: int = 0, boundary_k: float = 0.0,
+                     form: int | None = None, storage_scale: float = 0.0, steps: int | None = None):
+    """Create, voxelise, classify and configure a Simulation for a scene and
+    start it from rest.  Returns (sim, info dict)."""
+    from . import capi
+    p = capi.default_params(device=device, courant=sc.courant, cell_size=sc.cell_size, bbox_nudge=sc.nudge,
+                            sponge_width=sc.sponge_width, storage=storage, storage_scale=storage_scale,
+                            boundary_k=boundary_k,
+                            boundary_form=boundary_form(sc) if form is None else form)
+    sim = capi.Simulation(p)
+    sim.set_material_roles(sc.roles)
+    sim.set_mesh(sc.verts, sc.tris, sc.tri_mat)
+    sim.classify()
+    g = sim.info()
+    shape = (int(g.nx), int(g.ny), int(g.nz))
+    bmin = np.array(list(g.bbox_min), np.float32)
+    if sc.coef64 is not None:
+        sim.set_filters(sc.coef64.astype(np.float32), n_sections=sc.n_sections)
+    if sc.hard is not None:
+        sim.set_hard_source(sc.hard)
+    src = voxel_index(sc.src_pos, bmin, g.cell_size, shape) if len(sc.src_pos) else np.zeros(0, np.uint64)
+    rcv = voxel_index(sc.rcv_pos, bmin, g.cell_size, shape) if len(sc.rcv_pos) else np.zeros(0, np.uint64)
+    if src.size:
+        sim.set_sources(src, sc.src_sig)
+    sim.set_receivers(rcv)
+    sim.start(sc.steps if steps is None else steps)
+    return sim, dict(shape=shape, bmin=bmin, src=src, rcv=rcv, info=g)
