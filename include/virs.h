@@ -224,9 +224,17 @@ virs_status virs_energy(virs_sim *sim, double *out);
 virs_status virs_set_timing(virs_sim *sim, int enable);
 virs_status virs_get_timing(virs_sim *sim, virs_timing *out);
 
-/* Kernel variant: tile height (4, 8 or 16 rows) and planes per block;
- * 0 = the library's choice. */
-virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block);
+/* Kernel variant: tile height (4, 8 or 16 rows; 0 = 8), planes per block
+ * (0 = the library's choice) and pipeline depth: 0 = the register-streaming
+ * kernel, 1..3 = the TMA kernel with that many planes in flight, -1 = the
+ * default (TMA, 2).  All variants give bit-identical results. */
+virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block, int pipeline_depth);
+
+/* Failure-path self test (no reference counterpart): launches a kernel that
+ * waits, `limit` times (1..2^20), on an mbarrier that nothing completes, the
+ * way the step kernel's bounded waits give up; returns VIRS_E_TIMEOUT when
+ * the timeout was reported, and the handle stays usable. */
+virs_status virs_check_bounded_wait(virs_sim *sim, uint32_t limit);
 
 #ifdef __cplusplus
 }

@@ -489,8 +489,9 @@ static void boundary_f32(const vo_run_args *a, const float *pc, const float *pp,
             const float *k = a->coef32 + (uint64_t)a->bmat[b] * S * 5;
             float *s = st + (uint64_t)b * S * 4;
             for (uint32_t q = 0; q < S; ++q, k += 5, s += 4) {
-                float y = k[0] * in;
-                y = fmaf(k[1], s[0], y);
+                /* nvcc fuses the first two products as fma(b0, in, b1*s0):
+                 * found against the reference build's own kernels */
+                float y = fmaf(k[0], in, k[1] * s[0]);
                 y = fmaf(k[2], s[1], y);
                 y = fmaf(-k[3], s[2], y);
                 y = fmaf(-k[4], s[3], y);

@@ -1,13 +1,12 @@
 """Golden vectors produced by the reference's own CUDA kernels
-(tests/golden/make_golden.py): the oracle must reproduce them on the CPU,
-and the CUDA path through the C ABI on the GPU."""
+(tests/golden/make_golden.py): the oracle must reproduce them bit for bit
+on the CPU, and the CUDA path through the C ABI on the GPU."""
 from pathlib import Path
 
 import numpy as np
 import pytest
 
 import oracle
-from helpers import rel_l2
 
 GOLD = Path(__file__).resolve().parent / "golden"
 CASES = sorted(p.stem for p in GOLD.glob("ref_*.npz"))
@@ -48,9 +47,8 @@ def test_oracle_step_matches_reference_gpu(name):
     d = _load(name)
     ir, p = _oracle_run(d)
     assert np.abs(d["ir"]).max() > 0
-    assert rel_l2(ir, d["ir"]) <= 1e-6
-    assert rel_l2(p, d["p_final"]) <= 1e-6
-    print(name, "bit-identical samples:", float(np.mean(ir.view(np.uint32) == d["ir"].view(np.uint32))))
+    assert np.array_equal(ir.view(np.uint32), d["ir"].view(np.uint32))
+    assert np.array_equal(p.view(np.uint32), d["p_final"].view(np.uint32))
 
 
 @pytest.mark.gpu
@@ -71,6 +69,6 @@ def test_cuda_path_matches_reference_gpu(name):
     sim.start(steps)
     sim.run(steps)
     got = sim.ir()
-    assert rel_l2(got, d["ir"]) <= 1e-6
-    assert rel_l2(sim.pressure(), d["p_final"]) <= 1e-6
+    assert np.array_equal(got.view(np.uint32), d["ir"].view(np.uint32))
+    assert np.array_equal(sim.pressure().view(np.uint32), d["p_final"].view(np.uint32))
     sim.close()

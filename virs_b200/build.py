@@ -32,7 +32,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fvi
               "-Xptxas", "-warn-spills", *INC]
 # per-file extra flags: the step kernels flush subnormals like the reference
 # build (--use_fast_math implies -ftz=true) and keep every rounding explicit
-PER_FILE = {"kernels_step.cu": ["-ftz=true"], "kernels_misc.cu": ["-ftz=true"]}
+PER_FILE = {"kernels_step.cu": ["-ftz=true"], "kernels_step_tma.cu": ["-ftz=true"], "kernels_misc.cu": ["-ftz=true"]}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-Wall",
              f"-I{CUDA_HOME / 'include'}", *INC]
 
@@ -64,7 +64,7 @@ def _compile(src: Path) -> Path:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
-    deps = list(CSRC.glob("*.hpp")) + list((ROOT / "include").glob("*.h"))
+    deps = list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
     srcs = sources()
     todo = [s for s in srcs if force or _needs(s, OBJ / (s.name + ".o"), deps)]
     if todo:

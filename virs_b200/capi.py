@@ -85,7 +85,8 @@ _SIGS = {
     "virs_energy": ([_P, _P], C.c_int),
     "virs_set_timing": ([_P, C.c_int], C.c_int),
     "virs_get_timing": ([_P, _P], C.c_int),
-    "virs_set_tiling": ([_P, C.c_int, C.c_int], C.c_int),
+    "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)
@@ -335,5 +336,9 @@ class Simulation:
         check(lib().virs_get_timing(self._h, C.byref(t)))
         return t
 
-    def set_tiling(self, rows: int = 0, planes: int = 0):
-        check(lib().virs_set_tiling(self._h, rows, planes))
+    def check_bounded_wait(self, limit: int = 1000) -> int:
+        """Status of the bounded-wait self test (VIRS_E_TIMEOUT expected)."""
+        return int(lib().virs_check_bounded_wait(self._h, limit))
+
+    def set_tiling(self, rows: int = 0, planes: int = 0, depth: int = -1):
+        check(lib().virs_set_tiling(self._h, rows, planes, depth))

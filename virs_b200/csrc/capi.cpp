@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "internal.hpp"
 
 #define VIRS_EXPORT extern "C" __attribute__((visibility("default")))
@@ -112,8 +114,12 @@ struct virs_sim {
     double fs = 0;
     float scale = 1.f, inv_scale = 1.f;
 
-    // kernel variant
-    int tile_rows = 8, zc = 0;
+    // kernel variant: depth 0 = register-streaming kernel, 1..3 = TMA
+    // kernel with that many planes in flight
+    int tile_rows = 8, zc = 0, depth = 2;
+    CUtensorMap tmP[2], tmQ[2], tmC;
+    int maps_rows = 0;             // tile rows the maps were built for (0 = none)
+    DevBuf err;                    // device error flag of bounded waits
 
     // CUDA graphs for GRAPH_STEPS steps, one per parity of `cur`
     static constexpr int GRAPH_STEPS = 32;
@@ -279,6 +285,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->cur = 0;
     s->nb = 0;
     s->steps_done = 0;
+    s->maps_rows = 0;
     // sources and receivers refer to voxel indices of the previous grid
     s->nsrc = s->nrcv = 0;
     s->src_ref.clear();
@@ -326,6 +333,66 @@ virs_status ensure_ir(virs_sim *s, uint64_t need)
     return VIRS_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+virs_status encode(CUtensorMap *m, CUtensorMapDataType dt, size_t elem, void *base, const virs_sim *s, uint32_t bx,
+                   uint32_t by)
+{
+    auto fn = encode_fn();
+    if (!fn) return fail(VIRS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {s->px, s->ny, s->nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)s->px * elem, (cuuint64_t)s->px * s->ny * elem};
+    const cuuint32_t box[3] = {bx, by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VIRS_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return VIRS_OK;
+}
+
+// tensor maps of the two field buffers (halo box and tile box) and of the
+// cell codes, for the current tile height
+virs_status build_maps(virs_sim *s)
+{
+    const int rows = s->tile_rows;
+    const CUtensorMapDataType dt = s->prm.storage == VIRS_STORAGE_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : s->prm.storage == VIRS_STORAGE_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                                        : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const size_t el = s->storage_bytes();
+    for (int b = 0; b < 2; ++b) {
+        VIRS_TRY(encode(&s->tmP[b], dt, el, s->field[b].ptr, s, (uint32_t)tma_box_width(s->prm.storage), rows + 2));
+        VIRS_TRY(encode(&s->tmQ[b], dt, el, s->field[b].ptr, s, (uint32_t)tma_tile_x(), rows));
+    }
+    VIRS_TRY(encode(&s->tmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), rows));
+    if (!s->err.ptr) VIRS_TRY(s->err.alloc(sizeof(int), "error flag"));
+    s->maps_rows = rows;
+    return VIRS_OK;
+}
+
+// read and clear the device error flag of the bounded waits
+virs_status check_err(virs_sim *s)
+{
+    if (!s->err.ptr) return VIRS_OK;
+    int e = 0;
+    VIRS_CUDA(cudaMemcpy(&e, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        VIRS_CUDA(cudaMemset(s->err.ptr, 0, sizeof(int)));
+        return fail(VIRS_E_TIMEOUT, "a stencil block gave up waiting for its staged planes (bounded wait expired)");
+    }
+    return VIRS_OK;
+}
+
 virs_status ready_to_run(virs_sim *s)
 {
     if (!s->has_grid) return fail(VIRS_E_STATE, "no grid: call virs_load_obj, virs_set_mesh or virs_set_grid");
@@ -336,6 +403,7 @@ virs_status ready_to_run(virs_sim *s)
                                     std::to_string(s->nmat) + " materials set)");
     if (!s->state.ptr) VIRS_TRY(alloc_states(s));
     if (!s->ctr.ptr) VIRS_TRY(s->ctr.alloc(sizeof(uint32_t), "step counter"));
+    if (s->depth > 0 && s->maps_rows != s->tile_rows) VIRS_TRY(build_maps(s));
     return VIRS_OK;
 }
 
@@ -388,9 +456,16 @@ PostArgs post_args(const virs_sim *s, int parity)
     return a;
 }
 
+cudaError_t launch_stencil(const virs_sim *s, int parity, cudaStream_t st)
+{
+    if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
+    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
+    return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, step_args(s, parity), m, s->err.as<int>(), st);
+}
+
 cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
 {
-    cudaError_t e = launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
+    cudaError_t e = launch_stencil(s, parity, st);
     if (e != cudaSuccess) return e;
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
@@ -428,7 +503,7 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
         for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
             const int par = s->cur ^ (int)(i & 1);
             cudaEventRecord(ev[2 * i], st);
-            err = launch_step(s->prm.storage, s->tile_rows, step_args(s, par), st);
+            err = launch_stencil(s, par, st);
             cudaEventRecord(ev[2 * i + 1], st);
             if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
         }
@@ -686,6 +761,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
     }
     s->state.release();
     if (s->filters_set) VIRS_TRY(alloc_states(s));
+    s->maps_rows = 0;
     s->classified = true;
     VIRS_CUDA(cudaEventRecord(s->done, st));
     return VIRS_OK;
@@ -914,7 +990,8 @@ VIRS_EXPORT virs_status virs_synchronize(virs_sim *s)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_synchronize: null");
     VIRS_TRY(use_device(s));
-    return wait_done(s);
+    VIRS_TRY(wait_done(s));
+    return check_err(s);
 }
 
 VIRS_EXPORT virs_status virs_run_host(virs_sim *s, uint64_t steps, const float *signal, float *ir_out, void *stream)
@@ -945,7 +1022,7 @@ VIRS_EXPORT virs_status virs_run_host(virs_sim *s, uint64_t steps, const float *
         VIRS_CUDA(cudaMemcpy2DAsync(ir_out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
                                     cudaMemcpyDeviceToHost, st));
     VIRS_CUDA(cudaStreamSynchronize(st));
-    return VIRS_OK;
+    return check_err(s);
 }
 
 VIRS_EXPORT virs_status virs_step(virs_sim *s, uint32_t step, int *keep_going, float *sample)
@@ -967,6 +1044,7 @@ VIRS_EXPORT virs_status virs_step(virs_sim *s, uint32_t step, int *keep_going, f
     if (s->nrcv) VIRS_CUDA(cudaMemcpyAsync(&v, s->ir.as<float>() + step, 4, cudaMemcpyDeviceToHost, st));
     VIRS_CUDA(cudaStreamSynchronize(st));
     VIRS_CUDA(cudaEventRecord(s->done, st));
+    VIRS_TRY(check_err(s));
     if (sample) *sample = v;
     if (!std::isfinite(v)) return fail(VIRS_E_UNSTABLE, "receiver sample is not finite at step " + std::to_string(step));
     if (s->out0.size() <= step) s->out0.resize((size_t)step + 1, 0.f);
@@ -999,6 +1077,7 @@ VIRS_EXPORT virs_status virs_get_ir(const virs_sim *s, uint64_t first, uint64_t 
     if (!s->nrcv || !steps) return VIRS_OK;
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
+    VIRS_TRY(check_err(const_cast<virs_sim *>(s)));
     VIRS_CUDA(cudaMemcpy2D(out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
                            cudaMemcpyDeviceToHost));
     return VIRS_OK;
@@ -1113,14 +1192,29 @@ VIRS_EXPORT virs_status virs_get_timing(virs_sim *s, virs_timing *o)
     return VIRS_OK;
 }
 
-VIRS_EXPORT virs_status virs_set_tiling(virs_sim *s, int rows, int planes)
+VIRS_EXPORT virs_status virs_set_tiling(virs_sim *s, int rows, int planes, int depth)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_set_tiling: null");
     if (rows != 0 && rows != 4 && rows != 8 && rows != 16) return fail(VIRS_E_ARG, "tile rows must be 4, 8 or 16");
     if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
+    if (depth < -1 || depth > 3) return fail(VIRS_E_ARG, "pipeline depth must be -1 (default), 0 (no TMA) or 1..3");
     VIRS_TRY(wait_done(s));
     s->tile_rows = rows ? rows : 8;
     s->zc = planes;
+    s->depth = depth < 0 ? 2 : depth;
+    s->maps_rows = 0;
     s->drop_graphs();
     return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_check_bounded_wait(virs_sim *s, uint32_t limit)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_check_bounded_wait: null");
+    if (limit == 0 || limit > (1u << 20)) return fail(VIRS_E_ARG, "limit must be 1..2^20");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    if (!s->err.ptr) VIRS_TRY(s->err.alloc(sizeof(int), "error flag"));
+    VIRS_CUDA(launch_wait_probe(s->err.as<int>(), limit, s->stream));
+    VIRS_CUDA(cudaStreamSynchronize(s->stream));
+    return check_err(s);
 }

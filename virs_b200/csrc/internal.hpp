@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "virs.h"
@@ -103,6 +104,19 @@ struct PostArgs {
 cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
 int default_planes(uint32_t nz);
+
+// TMA-staged step (kernels_step_tma.cu)
+struct TmaMaps {
+    const CUtensorMap *p;   // p^n with halo box
+    const CUtensorMap *q;   // p^{n-1}, tile box
+    const CUtensorMap *c;   // cell codes, tile box
+};
+cudaError_t launch_step_tma(int storage, int tile_rows, int depth, const StepArgs &a, const TmaMaps &m, int *err,
+                            cudaStream_t s);
+int tma_box_width(int storage);   // x extent of the halo box (elements)
+int tma_pad(int storage);         // x halo on each side (elements)
+int tma_tile_x();                 // x extent of a tile
+cudaError_t launch_wait_probe(int *err, uint32_t limit, cudaStream_t s);
 
 // classification launchers (kernels_classify.cu)
 struct ClassifyArgs {

@@ -1,0 +1,175 @@
+// Device helpers shared by the stencil kernels: storage types, the
+// leapfrog update and the boundary correction, with the arithmetic order of
+// the reference build written out (see kernels_step.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "internal.hpp"
+
+namespace virs {
+namespace step {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- storage types ------------------------------------------------------------
+
+template <typename T> struct Io;
+
+template <> struct Io<float> {
+    static constexpr int VEC = 4;
+    __device__ static void ld(const float *p, float (&r)[VEC])
+    {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+    }
+    __device__ static void ld_stream(const float *p, float (&r)[VEC])
+    {
+        const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+        r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+    }
+    __device__ static void st(float *p, const float (&r)[VEC])
+    {
+        __stcs(reinterpret_cast<float4 *>(p), make_float4(r[0], r[1], r[2], r[3]));
+    }
+    __device__ static float ld1(const float *p) { return *p; }
+    __device__ static float get(float v) { return v; }
+    __device__ static float put(float v) { return v; }
+};
+
+template <> struct Io<__half> {
+    static constexpr int VEC = 8;
+    __device__ static void unpack(const uint4 v, float (&r)[VEC])
+    {
+        const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(h[i]);
+            r[2 * i] = f.x;
+            r[2 * i + 1] = f.y;
+        }
+    }
+    __device__ static void ld(const __half *p, float (&r)[VEC]) { unpack(*reinterpret_cast<const uint4 *>(p), r); }
+    __device__ static void ld_stream(const __half *p, float (&r)[VEC]) { unpack(__ldcs(reinterpret_cast<const uint4 *>(p)), r); }
+    __device__ static void st(__half *p, const float (&r)[VEC])
+    {
+        uint4 v;
+        __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2half2_rn(r[2 * i], r[2 * i + 1]);
+        __stcs(reinterpret_cast<uint4 *>(p), v);
+    }
+    __device__ static float ld1(const __half *p) { return __half2float(*p); }
+    __device__ static float get(__half v) { return __half2float(v); }
+    __device__ static __half put(float v) { return __float2half_rn(v); }
+};
+
+template <> struct Io<__nv_bfloat16> {
+    static constexpr int VEC = 8;
+    __device__ static void unpack(const uint4 v, float (&r)[VEC])
+    {
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            r[2 * i] = f.x;
+            r[2 * i + 1] = f.y;
+        }
+    }
+    __device__ static void ld(const __nv_bfloat16 *p, float (&r)[VEC]) { unpack(*reinterpret_cast<const uint4 *>(p), r); }
+    __device__ static void ld_stream(const __nv_bfloat16 *p, float (&r)[VEC])
+    {
+        unpack(__ldcs(reinterpret_cast<const uint4 *>(p)), r);
+    }
+    __device__ static void st(__nv_bfloat16 *p, const float (&r)[VEC])
+    {
+        uint4 v;
+        __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(r[2 * i], r[2 * i + 1]);
+        __stcs(reinterpret_cast<uint4 *>(p), v);
+    }
+    __device__ static float ld1(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    __device__ static float get(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
+};
+
+template <int VEC> __device__ inline void ld_code(const uint8_t *p, uint8_t (&c)[VEC]);
+template <> __device__ inline void ld_code<4>(const uint8_t *p, uint8_t (&c)[4])
+{
+    const uchar4 v = __ldcs(reinterpret_cast<const uchar4 *>(p));
+    c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+}
+template <> __device__ inline void ld_code<8>(const uint8_t *p, uint8_t (&c)[8])
+{
+    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        c[i] = (v.x >> (8 * i)) & 0xff;
+        c[4 + i] = (v.y >> (8 * i)) & 0xff;
+    }
+}
+
+__device__ __forceinline__ float pick(uint8_t code, uint8_t bit, float centre, float nb)
+{
+    return (code & bit) ? centre : nb;
+}
+
+// simulator_gpu.cu:70-88 with the contractions of the reference build.
+__device__ __forceinline__ float leapfrog(uint8_t c, float ce, float xp, float xm, float yp, float ym, float zp,
+                                          float zm, float qv, float c2dt2, float inv_h2)
+{
+    float s = pick(c, W_XP, ce, xp);
+    s = __fadd_rn(s, pick(c, W_XM, ce, xm));
+    s = __fadd_rn(s, pick(c, W_YP, ce, yp));
+    s = __fadd_rn(s, pick(c, W_YM, ce, ym));
+    s = __fadd_rn(s, pick(c, W_ZP, ce, zp));
+    s = __fadd_rn(s, pick(c, W_ZM, ce, zm));
+    const float lap = __fmul_rn(__fmaf_rn(-6.0f, ce, s), inv_h2);
+    const float t = __fsub_rn(__fmul_rn(2.0f, ce), qv);
+    return __fmaf_rn(c2dt2, lap, t);
+}
+
+// simulator_gpu.cu:126-148: biquad sections in series on d = p - p^{n-1}
+// (b0*in + b1*s0 contracted to fma(b0, in, b1*s0) as the reference build
+// does),
+// then p+ -= K*(0.1*y + 0.9*d)*0.4 (times the sponge weight) in double, or
+// the centered form of the same correction.
+__device__ __noinline__ float boundary(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+{
+    const float d = __fsub_rn(ce, qv);
+    float in = d;
+    const uint64_t nb = a.nb;
+    const float *kc = a.coef + (uint64_t)__ldg(a.bmat + slot) * a.nsec * 5;
+    float *st = a.state + slot;
+    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5, st += 4 * nb) {
+        const float s0 = st[0], s1 = st[nb], s2 = st[2 * nb], s3 = st[3 * nb];
+        float y = __fmaf_rn(__ldg(kc), in, __fmul_rn(__ldg(kc + 1), s0));
+        y = __fmaf_rn(__ldg(kc + 2), s1, y);
+        y = __fmaf_rn(-__ldg(kc + 3), s2, y);
+        y = __fmaf_rn(-__ldg(kc + 4), s3, y);
+        st[0] = in;
+        st[nb] = s0;
+        st[2 * nb] = y;
+        st[3 * nb] = s2;
+        in = y;
+    }
+    const double w = (double)__ldg(a.bw + slot);
+    if (a.form == VIRS_BOUNDARY_REFERENCE) {
+        const double t = __fma_rn((double)in, a.mix_y, __dmul_rn((double)d, a.mix_d));
+        const double u = __dmul_rn(__dmul_rn(__dmul_rn(a.K, t), a.gain), w);
+        return __double2float_rn(__dsub_rn((double)r, u));
+    }
+    // centered: the direct damping term at (p+ - p-)/2, solved for p+
+    const double kgw = __dmul_rn(__dmul_rn(a.K, a.gain), w);
+    const double ac = __dmul_rn(__dmul_rn(kgw, a.mix_d), 0.5);
+    const double num = __dadd_rn(__dsub_rn((double)r, __dmul_rn(kgw, __dmul_rn((double)in, a.mix_y))),
+                                 __dmul_rn(ac, (double)qv));
+    return __double2float_rn(__ddiv_rn(num, __dadd_rn(1.0, ac)));
+}
+
+} // namespace
+} // namespace step
+} // namespace virs

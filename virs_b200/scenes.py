@@ -101,9 +101,10 @@ class Scene:
 
 
 def _interior_points(rng, lo, hi, n, margin):
-    lo = np.asarray(lo, np.float64) + margin
-    hi = np.asarray(hi, np.float64) - margin
-    return rng.uniform(lo, hi, (n, 3))
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    m = np.minimum(margin, 0.25 * (hi - lo))       # thin crops keep a quarter on each side
+    return rng.uniform(lo + m, hi - m, (n, 3))
 
 
 def plain_small(seed: int = 1, steps: int = 2000) -> Scene:
