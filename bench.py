@@ -175,6 +175,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         t = sim.timing()
         sim.set_timing(False)
         out["kernel_ms"] = t.step_kernel_ms / max(t.step_launches, 1)
+        out["boundary_ms"] = t.boundary_kernel_ms / max(t.step_launches, 1)
     if want_e2e:
         nsrc, nrcv = len(sc.src_pos), len(sc.rcv_pos)
         first = int(sim.info().steps_done)
@@ -300,9 +301,10 @@ def run_virs(args):
             "frac": round(achieved / peak, 4) if achieved else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
             "traffic": None,
-            "kernel": "k_step<float,8> (stencil + fused boundary filters)",
+            "kernel": "k_step_tma<float> (stencil; boundary voxels in a separate list pass)",
             "kernel_ms": kernel_ms,
             "bytes_per_voxel": BYTES_F32,
+            "boundary_pass_ms": r32.get("boundary_ms"),
         },
         "e2e": {
             "value": round(nvox * args.steps / (r32["e2e_ms"] * 1e-3) / 1e9 * world, 3),
@@ -312,7 +314,7 @@ def run_virs(args):
             "api": "virs_run_host (pinned host buffers)",
             "wall_ms": r32["e2e_wall_ms"],
         },
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 3 * args.steps,
         "clocks": r32["clocks"],
         "variants": variants,
     }

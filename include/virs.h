@@ -82,6 +82,7 @@ typedef struct virs_grid_info {
 
 typedef struct virs_timing {
     double step_kernel_ms;   /* summed CUDA-event time of the stencil kernel         */
+    double boundary_kernel_ms; /* summed CUDA-event time of the boundary-list kernel */
     uint64_t step_launches;  /* stencil launches timed                                */
     uint64_t kernel_launches;/* all kernels this library launched while timing        */
 } virs_timing;
@@ -220,7 +221,8 @@ virs_status virs_energy(virs_sim *sim, double *out);
 /* ---- measurement ------------------------------------------------------------- */
 
 /* While enabled, virs_run launches without a graph and brackets every
- * stencil launch with CUDA events; virs_get_timing sums them. */
+ * stencil launch and every boundary-list launch with CUDA events;
+ * virs_get_timing sums them. */
 virs_status virs_set_timing(virs_sim *sim, int enable);
 virs_status virs_get_timing(virs_sim *sim, virs_timing *out);
 
@@ -229,6 +231,21 @@ virs_status virs_get_timing(virs_sim *sim, virs_timing *out);
  * kernel, 1..3 = the TMA kernel with that many planes in flight, -1 = the
  * default (TMA, 2).  All variants give bit-identical results. */
 virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block, int pipeline_depth);
+
+typedef struct virs_tiling {
+    int32_t tile_rows;        /* 4, 8 or 16                                        */
+    int32_t planes_per_block; /* z planes streamed by one block                    */
+    int32_t pipeline_depth;   /* 0 = register kernel, 1..3 = TMA planes in flight  */
+    float ms_per_step;        /* measured by virs_autotune (0 otherwise)           */
+} virs_tiling;
+
+/* Autotuner (no reference counterpart): right after virs_start_simulation,
+ * times `trial_steps` steps of each TMA variant (tile rows 4/8/16, depth
+ * 1..3, 8..64 planes per block) on this handle's own grid and keeps the
+ * fastest; the simulation is then back at rest.  Results are cached per
+ * device, storage and grid shape for the life of the process. */
+virs_status virs_autotune(virs_sim *sim, uint32_t trial_steps, virs_tiling *best);
+virs_status virs_get_tiling(const virs_sim *sim, virs_tiling *out);
 
 /* Failure-path self test (no reference counterpart): launches a kernel that
  * waits, `limit` times (1..2^20), on an mbarrier that nothing completes, the

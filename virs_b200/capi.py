@@ -45,8 +45,14 @@ class GridInfo(C.Structure):
     ]
 
 
+class Tiling(C.Structure):
+    _fields_ = [("tile_rows", C.c_int32), ("planes_per_block", C.c_int32), ("pipeline_depth", C.c_int32),
+                ("ms_per_step", C.c_float)]
+
+
 class Timing(C.Structure):
-    _fields_ = [("step_kernel_ms", C.c_double), ("step_launches", C.c_uint64), ("kernel_launches", C.c_uint64)]
+    _fields_ = [("step_kernel_ms", C.c_double), ("boundary_kernel_ms", C.c_double), ("step_launches", C.c_uint64),
+                ("kernel_launches", C.c_uint64)]
 
 
 _P = C.c_void_p
@@ -87,6 +93,8 @@ _SIGS = {
     "virs_get_timing": ([_P, _P], C.c_int),
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
+    "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_get_tiling": ([_P, _P], C.c_int),
 }
 
 EXPORTED = tuple(_SIGS)
@@ -339,6 +347,16 @@ class Simulation:
     def check_bounded_wait(self, limit: int = 1000) -> int:
         """Status of the bounded-wait self test (VIRS_E_TIMEOUT expected)."""
         return int(lib().virs_check_bounded_wait(self._h, limit))
+
+    def autotune(self, trial_steps: int = 10) -> Tiling:
+        t = Tiling()
+        check(lib().virs_autotune(self._h, trial_steps, C.byref(t)))
+        return t
+
+    def tiling(self) -> Tiling:
+        t = Tiling()
+        check(lib().virs_get_tiling(self._h, C.byref(t)))
+        return t
 
     def set_tiling(self, rows: int = 0, planes: int = 0, depth: int = -1):
         check(lib().virs_set_tiling(self._h, rows, planes, depth))

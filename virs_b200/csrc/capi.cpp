@@ -10,7 +10,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
@@ -128,7 +131,7 @@ struct virs_sim {
 
     // timing
     bool timing = false;
-    double t_ms = 0;
+    double t_ms = 0, t_bms = 0;
     uint64_t t_steps = 0, t_launch = 0;
 
     // virs_step's RMS rule (simulator_gpu.cu:303-330)
@@ -467,6 +470,8 @@ cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
 {
     cudaError_t e = launch_stencil(s, parity, st);
     if (e != cudaSuccess) return e;
+    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), st);
+    if (e != cudaSuccess) return e;
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
 
@@ -500,25 +505,32 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
         std::vector<cudaEvent_t> ev(2 * n);
         for (auto &e : ev) VIRS_CUDA(cudaEventCreate(&e));
         cudaError_t err = cudaSuccess;
+        ev.resize(3 * n);
+        for (size_t k = 2 * n; k < ev.size(); ++k) VIRS_CUDA(cudaEventCreate(&ev[k]));
         for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
             const int par = s->cur ^ (int)(i & 1);
             cudaEventRecord(ev[2 * i], st);
             err = launch_stencil(s, par, st);
             cudaEventRecord(ev[2 * i + 1], st);
+            if (err == cudaSuccess) err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), st);
+            cudaEventRecord(ev[2 * n + i], st);
             if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
         }
-        if (err == cudaSuccess) err = cudaEventSynchronize(ev.back());
-        double ms = 0;
+        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+        double ms = 0, bms = 0;
         for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
-            float t = 0;
+            float t = 0, tb = 0;
             err = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&tb, ev[2 * i + 1], ev[2 * n + i]);
             ms += t;
+            bms += tb;
         }
+        s->t_bms += bms;
         for (auto &e : ev) cudaEventDestroy(e);
         if (err != cudaSuccess) return cuda_fail(err, "timed step loop");
         s->t_ms += ms;
         s->t_steps += n;
-        s->t_launch += 2 * n;
+        s->t_launch += (s->nb ? 3 : 2) * n;
     } else {
         uint64_t i = 0;
         if (n >= (uint64_t)virs_sim::GRAPH_STEPS) {
@@ -1178,7 +1190,7 @@ VIRS_EXPORT virs_status virs_set_timing(virs_sim *s, int enable)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_set_timing: null");
     s->timing = enable != 0;
-    s->t_ms = 0;
+    s->t_ms = s->t_bms = 0;
     s->t_steps = s->t_launch = 0;
     return VIRS_OK;
 }
@@ -1187,6 +1199,7 @@ VIRS_EXPORT virs_status virs_get_timing(virs_sim *s, virs_timing *o)
 {
     if (!s || !o) return fail(VIRS_E_ARG, "virs_get_timing: null argument");
     o->step_kernel_ms = s->t_ms;
+    o->boundary_kernel_ms = s->t_bms;
     o->step_launches = s->t_steps;
     o->kernel_launches = s->t_launch;
     return VIRS_OK;
@@ -1217,4 +1230,122 @@ VIRS_EXPORT virs_status virs_check_bounded_wait(virs_sim *s, uint32_t limit)
     VIRS_CUDA(launch_wait_probe(s->err.as<int>(), limit, s->stream));
     VIRS_CUDA(cudaStreamSynchronize(s->stream));
     return check_err(s);
+}
+
+namespace {
+
+// best tiling per (device, storage, nx, ny, nz), filled by virs_autotune
+struct TuneKey {
+    int dev, storage;
+    uint32_t nx, ny, nz;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(dev, storage, nx, ny, nz) < std::tie(o.dev, o.storage, o.nx, o.ny, o.nz);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, virs_tiling> g_tune;
+
+virs_status reset_state(virs_sim *s)
+{
+    VIRS_CUDA(cudaMemsetAsync(s->field[0].ptr, 0, s->field[0].bytes, s->stream));
+    VIRS_CUDA(cudaMemsetAsync(s->field[1].ptr, 0, s->field[1].bytes, s->stream));
+    VIRS_CUDA(cudaMemsetAsync(s->state.ptr, 0, s->state.bytes, s->stream));
+    VIRS_CUDA(cudaMemsetAsync(s->ctr.ptr, 0, 4, s->stream));
+    if (s->ir.ptr) VIRS_CUDA(cudaMemsetAsync(s->ir.ptr, 0, s->ir.bytes, s->stream));
+    VIRS_CUDA(cudaStreamSynchronize(s->stream));
+    s->cur = 0;
+    s->steps_done = 0;
+    s->out0.clear();
+    s->rms_state = 0.f;
+    return VIRS_OK;
+}
+
+} // namespace
+
+VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_tiling *best)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_autotune: null");
+    if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
+    if (s->steps_done != 0) return fail(VIRS_E_STATE, "virs_autotune must run before the first step");
+    if (trial_steps == 0 || trial_steps > 1000) return fail(VIRS_E_ARG, "trial_steps must be 1..1000");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    const TuneKey key{s->prm.device, s->prm.storage, s->nx, s->ny, s->nz};
+    virs_tiling pick{};
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            pick = it->second;
+            cached = true;
+        }
+    }
+    if (!cached) {
+        VIRS_TRY(ensure_ir(s, 2ull * trial_steps + 2));
+        cudaEvent_t e0, e1;
+        VIRS_CUDA(cudaEventCreate(&e0));
+        VIRS_CUDA(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        const int rows_c[] = {4, 8, 16}, depth_c[] = {1, 2, 3}, planes_c[] = {8, 16, 32, 64};
+        virs_status st = VIRS_OK;
+        for (int d : depth_c)
+            for (int r : rows_c)
+                for (int pl : planes_c) {
+                    if (st != VIRS_OK) break;
+                    s->tile_rows = r;
+                    s->depth = d;
+                    s->zc = pl;
+                    s->maps_rows = 0;
+                    if ((st = ready_to_run(s)) != VIRS_OK) break;
+                    // one untimed step, then trial_steps timed ones
+                    cudaError_t e = enqueue_step(s, s->cur, s->stream);
+                    s->cur ^= 1;
+                    cudaEventRecord(e0, s->stream);
+                    for (uint32_t k = 0; k < trial_steps && e == cudaSuccess; ++k) {
+                        e = enqueue_step(s, s->cur, s->stream);
+                        s->cur ^= 1;
+                    }
+                    cudaEventRecord(e1, s->stream);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float ms = 0;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                    if (e != cudaSuccess) {
+                        st = cuda_fail(e, "autotune trial");
+                        break;
+                    }
+                    if ((st = check_err(s)) != VIRS_OK) break;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        pick = {r, pl, d, ms / trial_steps};
+                    }
+                    if ((st = reset_state(s)) != VIRS_OK) break;
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st != VIRS_OK) return st;
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune[key] = pick;
+    }
+    s->tile_rows = pick.tile_rows;
+    s->zc = pick.planes_per_block;
+    s->depth = pick.pipeline_depth;
+    s->maps_rows = 0;
+    s->drop_graphs();
+    VIRS_TRY(ready_to_run(s));
+    VIRS_TRY(reset_state(s));
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    if (best) *best = pick;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_tiling(const virs_sim *s, virs_tiling *out)
+{
+    if (!s || !out) return fail(VIRS_E_ARG, "virs_get_tiling: null argument");
+    out->tile_rows = s->tile_rows;
+    out->planes_per_block = s->zc;
+    out->pipeline_depth = s->depth;
+    out->ms_per_step = 0.f;
+    return VIRS_OK;
 }

@@ -103,6 +103,7 @@ struct PostArgs {
 // kernel launchers (kernels_step.cu)
 cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, cudaStream_t s);
 int default_planes(uint32_t nz);
 
 // TMA-staged step (kernels_step_tma.cu)

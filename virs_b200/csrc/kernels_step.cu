@@ -3,7 +3,7 @@
 // Semantics follow the reference step (src/simulator/simulator_gpu.cu):
 //   interior leapfrog with the wall mirror rule       :38-103
 //   boundary biquad correction, evaluated in double   :105-150
-// fused into one pass.  Layout and mapping:
+// in two passes.  Layout and mapping:
 //   * fields are [nz][ny][px] with px = nx rounded up to 32 (rows start on
 //     128-byte lines); two buffers, p^{n+1} overwrites p^{n-1} in place
 //     (each output depends on p^{n-1} at its own voxel only);
@@ -15,12 +15,11 @@
 //     ahead of its use;
 //   * one byte per voxel (the cell code) replaces the flags and the six
 //     neighbour flags of the reference;
-//   * boundary voxels are found without any index list: a warp covers
-//     consecutive voxels of one row, so a warp-wide exclusive scan of its
-//     boundary counts plus the per-128-voxel prefix `bseg` gives each
-//     boundary voxel its slot in the compacted (ascending index) order; the
-//     filter states are stored [section][4][slot] so the slots of one warp
-//     touch consecutive words.
+//   * boundary voxels (flag 2) are skipped -- their p^{n-1} stays in place --
+//     and updated by k_boundary, one thread per entry of the compacted,
+//     ascending boundary list: the leapfrog and the biquad correction
+//     together, with no divergence in the stencil kernel; the filter states
+//     are stored [section][4][slot] so a warp touches consecutive words.
 //
 // Arithmetic order is fixed with _rn intrinsics so that the result is
 // bit-identical to the CPU oracle: the reference CUDA build contracts
@@ -96,7 +95,6 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
     }
     __syncthreads();
 
-    const uint64_t seg0 = (uint64_t)x0 / SEG;
     for (int z = z0; z < z1; ++z) {
         const int b = (z - z0) & 1;
         const size_t zc = (size_t)z * plane, zn = zc + plane;
@@ -118,7 +116,6 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
         if (lane == 31) right = hr;
 
         float r[VEC];
-        unsigned bmask = 0;
 #pragma unroll
         for (int k = 0; k < VEC; ++k) {
             const uint8_t c = cd[k];
@@ -133,25 +130,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
                     const uint32_t sn = __ldg(a.ctr);
                     r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
                 }
+            } else if (c & CODE_BND) {
+                r[k] = qv[k]; // the boundary pass updates it
             } else {
                 r[k] = leapfrog(c, cc[k], xp, xm, yp, ym, cp[k], cm[k], qv[k], a.c2dt2, a.inv_h2);
-                if (c & CODE_BND) bmask |= 1u << k;
-            }
-        }
-
-        const int cnt = __popc(bmask);
-        if (__any_sync(FULL, cnt != 0)) {
-            int inc = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(FULL, inc, o);
-                if (lane >= o) inc += t;
-            }
-            if (cnt) {
-                uint64_t slot = (uint64_t)__ldg(a.bseg + ((uint64_t)z * ny + y) * a.spr + seg0) + (inc - cnt);
-#pragma unroll
-                for (int k = 0; k < VEC; ++k)
-                    if (bmask & (1u << k)) r[k] = boundary(a, r[k], cc[k], qv[k], slot++);
             }
         }
 
@@ -175,6 +157,29 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
         hl = hln;
         hr = hrn;
     }
+}
+
+// The compacted boundary pass (simulator_gpu.cu:105-150): one thread per
+// boundary voxel in list order; the leapfrog update (the stencil kernel
+// left these voxels untouched) and the filter correction.
+template <typename T> __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a,
+                                                                        const uint32_t *__restrict bidx)
+{
+    using IO = Io<T>;
+    const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= a.nb) return;
+    const uint32_t ref = __ldg(bidx + slot);
+    const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
+    const size_t sy = a.px, sz = (size_t)a.px * a.ny;
+    const size_t i = (size_t)z * sz + (size_t)y * sy + x;
+    const T *P = static_cast<const T *>(a.p);
+    T *Q = static_cast<T *>(a.q);
+    const uint8_t c = __ldg(a.code + i);
+    const float ce = IO::get(P[i]), qv = IO::get(Q[i]);
+    float r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
+                       IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
+    r = boundary(a, r, ce, qv, slot);
+    Q[i] = IO::put(r);
 }
 
 // Additive sources, then receivers, then the step counter
@@ -230,6 +235,18 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
     case VIRS_STORAGE_BF16: return launch_step_t<__nv_bfloat16>(tile_rows, a, s);
     default: return launch_step_t<float>(tile_rows, a, s);
     }
+}
+
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, cudaStream_t s)
+{
+    if (a.nb == 0) return cudaSuccess;
+    const unsigned g = (unsigned)((a.nb + 255) / 256);
+    switch (storage) {
+    case VIRS_STORAGE_F16: k_boundary<__half><<<g, 256, 0, s>>>(a, bidx); break;
+    case VIRS_STORAGE_BF16: k_boundary<__nv_bfloat16><<<g, 256, 0, s>>>(a, bidx); break;
+    default: k_boundary<float><<<g, 256, 0, s>>>(a, bidx); break;
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s)

@@ -18,6 +18,10 @@
 // streaming 16-byte stores.  No multicast: every copy reads this GPU's own
 // memory into this block's shared memory.
 //
+// Boundary voxels (flag 2) are left unchanged here -- their p^{n-1} stays in
+// place -- and are updated afterwards by the compacted boundary pass
+// (k_boundary), so this kernel has no divergent filter work.
+//
 // Every wait on an mbarrier is bounded; a wait that gives up sets *err and
 // the block returns (the host turns that into VIRS_E_TIMEOUT).
 #include <cuda.h>
@@ -176,13 +180,15 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
     if (tid == 0)
         for (int j = 0; j < D && j <= jmax; ++j) issue(j);
 
-    const uint64_t seg0 = (uint64_t)x0 / SEG;
     for (int i = 0, z = z0; z < z1; ++i, ++z) {
-        bool bad = !wait_stage(bars, i + 2, D, err);
-        if (i == 0) bad = bad || !wait_stage(bars, 0, D, err) || !wait_stage(bars, 1, D, err);
-        // one barrier per plane: the stage is ready for everyone, and every
-        // thread is done with plane z-1, so the stage that held P(z-2) can
-        // be refilled
+        // thread 0 waits for the stage (bounded); the barrier then tells every
+        // thread that the stage is ready and that everyone is done with plane
+        // z-1, so the stage that held P(z-2) can be refilled
+        bool bad = false;
+        if (tid == 0) {
+            bad = !wait_stage(bars, i + 2, D, err);
+            if (i == 0) bad = bad || !wait_stage(bars, 0, D, err) || !wait_stage(bars, 1, D, err);
+        }
         if (__syncthreads_or(bad)) return;
         if (tid == 0 && i >= 1 && i + L + 2 <= jmax) issue(i + L + 2);
 
@@ -207,7 +213,6 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
         if (lane == 31) right = Io<T>::get(Pc[c0 + 4]);
 
         float r[4];
-        unsigned bmask = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const uint8_t c = (uint8_t)(code4 >> (8 * k));
@@ -220,24 +225,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
                     const uint32_t sn = __ldg(a.ctr);
                     r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
                 }
+            } else if (c & CODE_BND) {
+                r[k] = qv[k]; // updated by the boundary pass, which needs p^{n-1}
             } else {
                 r[k] = leapfrog(c, cc[k], xp, xm, yp[k], ym[k], zp[k], zm[k], qv[k], a.c2dt2, a.inv_h2);
-                if (c & CODE_BND) bmask |= 1u << k;
-            }
-        }
-        const int cnt = act ? __popc(bmask) : 0;
-        if (__any_sync(FULL, cnt != 0)) {
-            int inc = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(FULL, inc, o);
-                if (lane >= o) inc += t;
-            }
-            if (cnt) {
-                uint64_t slot = (uint64_t)__ldg(a.bseg + ((uint64_t)z * ny + y) * a.spr + seg0) + (inc - cnt);
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (bmask & (1u << k)) r[k] = boundary(a, r[k], cc[k], qv[k], slot++);
             }
         }
         if (act) st4(Q + (size_t)z * plane + (size_t)y * a.px + x, r);
