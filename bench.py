@@ -155,6 +155,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     from virs_b200 import scenes
     total = args.warmup + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
     sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
+    tiling = sim.autotune(args.tune_steps) if args.tune_steps else sim.tiling()
     sim.run(args.warmup, stream.cuda_stream)
     torch.cuda.synchronize()
     if dist:
@@ -166,7 +167,9 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
         ms = float(t.item())
-    out = {"ms": ms, "clocks": clk.summary(), "meta": meta}
+    out = {"ms": ms, "clocks": clk.summary(), "meta": meta,
+           "tiling": {"tile_rows": tiling.tile_rows, "planes_per_block": tiling.planes_per_block,
+                      "pipeline_depth": tiling.pipeline_depth}}
     # per-kernel events over K' steps (no graph; events around each stencil launch)
     if args.kernel_steps:
         sim.set_timing(True)
@@ -292,6 +295,7 @@ def run_virs(args):
             "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * 4 / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
             "timing": "CUDA events on the launching stream around virs_run (CUDA graph), max over ranks",
+            "tiling": r32["tiling"],
         },
         "roofline": {
             "bound": "hbm",
@@ -401,6 +405,7 @@ def main():
     ap.add_argument("--impl", choices=["virs", "reference"], default="virs")
     ap.add_argument("--size", type=int, nargs=3, default=[1024, 768, 512])
     ap.add_argument("--kernel-steps", type=int, default=100, help="steps of the per-kernel CUDA-event pass")
+    ap.add_argument("--tune-steps", type=int, default=4, help="steps per candidate of virs_autotune (0 = no tuning)")
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

@@ -218,6 +218,7 @@ virs_status virs_init_pressure_sphere(virs_sim *sim, uint64_t x, uint64_t y, uin
 /* FP64 discrete energy of the current state (the physics health monitor). */
 virs_status virs_energy(virs_sim *sim, double *out);
 
+
 /* ---- measurement ------------------------------------------------------------- */
 
 /* While enabled, virs_run launches without a graph and brackets every
@@ -246,6 +247,25 @@ typedef struct virs_tiling {
  * device, storage and grid shape for the life of the process. */
 virs_status virs_autotune(virs_sim *sim, uint32_t trial_steps, virs_tiling *best);
 virs_status virs_get_tiling(const virs_sim *sim, virs_tiling *out);
+
+/* ---- batched runs ------------------------------------------------------------ */
+
+/* Many simulations advanced together (no reference counterpart: the
+ * reference runs one room with one source at a time).  Members are handles
+ * that are classified, configured and started, on one device, with one
+ * storage type, at the same step; they keep their buffers and results (read
+ * them with virs_get_ir on each member).  Every step is three launches for
+ * the whole batch -- one persistent TMA stencil kernel over the tiles of all
+ * members, one boundary-list kernel, one source/receiver kernel -- and
+ * virs_batch_run replays them as CUDA graphs.  Changing a member after
+ * virs_batch_create makes virs_batch_run fail with VIRS_E_STATE. */
+typedef struct virs_batch virs_batch;
+virs_status virs_batch_create(virs_sim *const *members, uint32_t n, virs_batch **out);
+virs_status virs_batch_run(virs_batch *batch, uint64_t steps, void *stream);
+virs_status virs_batch_synchronize(virs_batch *batch);
+virs_status virs_batch_set_tiling(virs_batch *batch, int tile_rows, int planes_per_block, int pipeline_depth);
+virs_status virs_batch_autotune(virs_batch *batch, uint32_t trial_steps, virs_tiling *best);
+virs_status virs_batch_destroy(virs_batch *batch);
 
 /* Failure-path self test (no reference counterpart): launches a kernel that
  * waits, `limit` times (1..2^20), on an mbarrier that nothing completes, the

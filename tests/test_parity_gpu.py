@@ -344,3 +344,55 @@ def test_bounded_wait_reports_timeout_and_context_survives():
     sim.synchronize()
     assert np.isfinite(sim.ir()).all()
     sim.close()
+
+
+def test_autotune_keeps_results_bit_identical():
+    sc = scenes.plain_small(steps=120)
+    sim, _ = scenes.build_simulation(sc)
+    sim.run(sc.steps)
+    base = sim.ir()
+    sim.start(sc.steps)
+    t = sim.autotune(3)
+    assert t.tile_rows in (4, 8, 16) and 1 <= t.pipeline_depth <= 3 and t.ms_per_step > 0
+    assert sim.info().steps_done == 0
+    sim.run(sc.steps)
+    assert np.array_equal(sim.ir().view(np.uint32), base.view(np.uint32))
+    got = sim.tiling()
+    assert (got.tile_rows, got.planes_per_block, got.pipeline_depth) == (t.tile_rows, t.planes_per_block,
+                                                                         t.pipeline_depth)
+    sim.close()
+
+
+@pytest.mark.parametrize("storage", [capi.STORAGE_F32, capi.STORAGE_BF16])
+def test_batch_matches_members_run_alone(storage):
+    """Three source positions in one room and three rooms of other sizes and
+    materials, advanced together; every member's IR equals its own run."""
+    scs = scenes.batched(steps=140, n_sources=3, n_rooms=3, room=64, size_range=(40, 90))
+    alone = []
+    for sc in scs:
+        sim, _ = scenes.build_simulation(sc, storage=storage)
+        sim.run(sc.steps)
+        alone.append(sim.ir())
+        sim.close()
+    sims = [scenes.build_simulation(sc, storage=storage)[0] for sc in scs]
+    with capi.Batch(sims) as b:
+        b.run(100)              # graph chunks + remainder
+        b.run(40)
+        b.synchronize()
+        for sim, want in zip(sims, alone):
+            assert np.array_equal(sim.ir().view(np.uint32), want.view(np.uint32))
+    for s in sims:
+        s.close()
+
+
+def test_batch_rejects_changed_members():
+    scs = scenes.batched(steps=20, n_sources=2, n_rooms=0, room=48)
+    sims = [scenes.build_simulation(sc)[0] for sc in scs]
+    b = capi.Batch(sims)
+    sims[1].set_receivers([int(sims[1].boundary_indices()[0])])
+    with pytest.raises(capi.VirsError) as e:
+        b.run(4)
+    assert e.value.status == capi.E_STATE
+    b.close()
+    for s in sims:
+        s.close()

@@ -94,6 +94,12 @@ _SIGS = {
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_batch_create": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_batch_run": ([_P, C.c_uint64, _P], C.c_int),
+    "virs_batch_synchronize": ([_P], C.c_int),
+    "virs_batch_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "virs_batch_autotune": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_batch_destroy": ([_P], C.c_int),
     "virs_get_tiling": ([_P, _P], C.c_int),
 }
 
@@ -360,3 +366,44 @@ class Simulation:
 
     def set_tiling(self, rows: int = 0, planes: int = 0, depth: int = -1):
         check(lib().virs_set_tiling(self._h, rows, planes, depth))
+
+
+class Batch:
+    """One virs_batch: many Simulations advanced together (3 launches per step)."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)                       # keep the members alive
+        arr = (C.c_void_p * len(self.sims))(*[s.handle.value for s in self.sims])
+        self._h = C.c_void_p()
+        check(lib().virs_batch_create(arr, len(self.sims), C.byref(self._h)))
+
+    def run(self, steps: int, stream: int | None = None):
+        check(lib().virs_batch_run(self._h, steps, stream))
+
+    def synchronize(self):
+        check(lib().virs_batch_synchronize(self._h))
+
+    def set_tiling(self, rows: int = 0, planes: int = 0, depth: int = -1):
+        check(lib().virs_batch_set_tiling(self._h, rows, planes, depth))
+
+    def autotune(self, trial_steps: int = 4) -> Tiling:
+        t = Tiling()
+        check(lib().virs_batch_autotune(self._h, trial_steps, C.byref(t)))
+        return t
+
+    def close(self):
+        if self._h:
+            lib().virs_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

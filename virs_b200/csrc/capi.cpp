@@ -128,6 +128,7 @@ struct virs_sim {
     static constexpr int GRAPH_STEPS = 32;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_dirty = true;
+    uint64_t gen = 0;              // bumped on every change of buffers or parameters
 
     // timing
     bool timing = false;
@@ -155,6 +156,7 @@ struct virs_sim {
                 g = nullptr;
             }
         graph_dirty = true;
+        ++gen;
     }
 
     size_t storage_bytes() const { return prm.storage == VIRS_STORAGE_F32 ? 4 : 2; }
@@ -190,6 +192,7 @@ virs_status upload_hard(virs_sim *s)
     if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->hard.ptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
     s->nhard = (uint32_t)v.size();
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 
@@ -211,6 +214,7 @@ virs_status alloc_states(virs_sim *s)
 {
     VIRS_TRY(s->state.alloc(std::max<uint64_t>(s->nb, 1) * s->nsec * 4 * sizeof(float), "filter states"));
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 
@@ -333,6 +337,7 @@ virs_status ensure_ir(virs_sim *s, uint64_t need)
     std::swap(s->ir.bytes, nb.bytes);
     s->ircap = cap;
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 
@@ -836,6 +841,7 @@ VIRS_EXPORT virs_status virs_set_filters(virs_sim *s, uint32_t nm, uint32_t ns, 
     s->nsec = ns;
     s->filters_set = true;
     s->graph_dirty = true;
+    ++s->gen;
     if (s->classified) VIRS_TRY(alloc_states(s));
     return VIRS_OK;
 }
@@ -919,6 +925,7 @@ VIRS_EXPORT virs_status virs_set_sources(virs_sim *s, uint32_t n, const uint64_t
     s->src_ref.assign(idx, idx + n);
     s->sig.release();
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 
@@ -940,6 +947,7 @@ VIRS_EXPORT virs_status virs_set_receivers(virs_sim *s, uint32_t n, const uint64
     s->ir.release();
     s->ircap = 0;
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 
@@ -951,6 +959,7 @@ virs_status upload_signals(virs_sim *s)
     VIRS_TRY(s->sig.alloc(std::max<size_t>(v.size(), 1) * 4, "source signals"));
     if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->sig.ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
     s->graph_dirty = true;
+    ++s->gen;
     return VIRS_OK;
 }
 } // namespace
@@ -1347,5 +1356,289 @@ VIRS_EXPORT virs_status virs_get_tiling(const virs_sim *s, virs_tiling *out)
     out->planes_per_block = s->zc;
     out->pipeline_depth = s->depth;
     out->ms_per_step = 0.f;
+    return VIRS_OK;
+}
+
+// ============================================================================
+// batched runs: many simulations advanced together, three launches per step
+// ============================================================================
+
+struct virs_batch {
+    std::vector<virs_sim *> mem;
+    std::vector<uint64_t> gen;
+    int dev = 0, storage = 0, rows = 8, depth = 2, planes = 0;
+    uint64_t ntiles = 0, nbnd = 0;
+    DevBuf desc, err;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    static constexpr int GRAPH_STEPS = 32;
+
+    ~virs_batch()
+    {
+        drop_graphs();
+        if (done) cudaEventDestroy(done);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void drop_graphs()
+    {
+        for (auto &g : graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    }
+};
+
+namespace {
+
+virs_status batch_check(const virs_batch *b)
+{
+    for (size_t i = 0; i < b->mem.size(); ++i) {
+        const virs_sim *s = b->mem[i];
+        if (s->gen != b->gen[i])
+            return fail(VIRS_E_STATE, "batch member " + std::to_string(i) + " changed after the batch was built");
+        if (s->cur != b->mem[0]->cur || s->steps_done != b->mem[0]->steps_done)
+            return fail(VIRS_E_STATE, "batch members must be at the same step");
+    }
+    return VIRS_OK;
+}
+
+// descriptors of every member for the batch's tiling
+virs_status batch_build(virs_batch *b)
+{
+    b->drop_graphs();
+    std::vector<BatchMember> h(b->mem.size());
+    uint64_t tiles = 0, bnd = 0;
+    const CUtensorMapDataType dt = b->storage == VIRS_STORAGE_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : b->storage == VIRS_STORAGE_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                                    : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    for (size_t i = 0; i < b->mem.size(); ++i) {
+        virs_sim *s = b->mem[i];
+        VIRS_TRY(ready_to_run(s));
+        BatchMember &m = h[i];
+        std::memset(&m, 0, sizeof(m));
+        const size_t el = s->storage_bytes();
+        for (int k = 0; k < 2; ++k) {
+            VIRS_TRY(encode(&m.mapP[k], dt, el, s->field[k].ptr, s, (uint32_t)tma_box_width(b->storage), b->rows + 2));
+            VIRS_TRY(encode(&m.mapQ[k], dt, el, s->field[k].ptr, s, (uint32_t)tma_tile_x(), b->rows));
+        }
+        VIRS_TRY(encode(&m.mapC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), b->rows));
+        const int zc = b->planes > 0 ? b->planes : (s->zc > 0 ? s->zc : default_planes(s->nz));
+        for (int par = 0; par < 2; ++par) {
+            m.step[par] = step_args(s, par);
+            m.step[par].zc = zc;
+            m.post[par] = post_args(s, par);
+        }
+        m.bidx = s->bidx.as<uint32_t>();
+        m.gx = (s->px + tma_tile_x() - 1) / tma_tile_x();
+        m.gy = (s->ny + b->rows - 1) / b->rows;
+        m.gz = (s->nz - 2 + zc - 1) / zc;
+        m.first_tile = tiles;
+        m.first_bnd = bnd;
+        tiles += (uint64_t)m.gx * m.gy * m.gz;
+        bnd += s->nb;
+        b->gen[i] = s->gen;
+    }
+    VIRS_TRY(b->desc.alloc(h.size() * sizeof(BatchMember), "batch descriptors"));
+    VIRS_CUDA(cudaMemcpy(b->desc.ptr, h.data(), h.size() * sizeof(BatchMember), cudaMemcpyHostToDevice));
+    b->ntiles = tiles;
+    b->nbnd = bnd;
+    return VIRS_OK;
+}
+
+cudaError_t batch_enqueue(const virs_batch *b, int parity, cudaStream_t st)
+{
+    const BatchMember *d = b->desc.as<BatchMember>();
+    const uint32_t n = (uint32_t)b->mem.size();
+    cudaError_t e = launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->err.as<int>(), st);
+    if (e != cudaSuccess) return e;
+    e = launch_boundary_batch(b->storage, d, n, b->nbnd, parity, st);
+    if (e != cudaSuccess) return e;
+    return launch_post_batch(b->storage, d, n, parity, st);
+}
+
+virs_status batch_graphs(virs_batch *b, cudaStream_t st)
+{
+    b->drop_graphs();
+    for (int par = 0; par < 2; ++par) {
+        cudaGraph_t g = nullptr;
+        VIRS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < virs_batch::GRAPH_STEPS && e == cudaSuccess; ++i) e = batch_enqueue(b, par ^ (i & 1), st);
+        const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(e, "capturing the batched step loop");
+        }
+        if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    return VIRS_OK;
+}
+
+virs_status batch_steps(virs_batch *b, uint64_t n, cudaStream_t st, bool use_graph)
+{
+    virs_sim *m0 = b->mem[0];
+    for (virs_sim *s : b->mem)
+        if (s->steps_done + n > s->ircap)
+            return fail(VIRS_E_ARG, "a batch member has receiver storage for fewer steps: reserve them with "
+                                    "virs_start_simulation");
+    for (virs_sim *s : b->mem) {
+        VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+        VIRS_CUDA(cudaStreamWaitEvent(st, s->done, 0));
+    }
+    const int cur = m0->cur;
+    uint64_t i = 0;
+    if (use_graph && n >= (uint64_t)virs_batch::GRAPH_STEPS) {
+        if (!b->graph[0]) VIRS_TRY(batch_graphs(b, st));
+        for (; i + virs_batch::GRAPH_STEPS <= n; i += virs_batch::GRAPH_STEPS)
+            VIRS_CUDA(cudaGraphLaunch(b->graph[cur ^ (int)(i & 1)], st));
+    }
+    for (; i < n; ++i) {
+        const cudaError_t e = batch_enqueue(b, cur ^ (int)(i & 1), st);
+        if (e != cudaSuccess) return cuda_fail(e, "batched step launch");
+    }
+    for (virs_sim *s : b->mem) {
+        s->cur ^= (int)(n & 1);
+        s->steps_done += n;
+        VIRS_CUDA(cudaEventRecord(s->done, st));
+    }
+    VIRS_CUDA(cudaEventRecord(b->done, st));
+    return VIRS_OK;
+}
+
+} // namespace
+
+VIRS_EXPORT virs_status virs_batch_create(virs_sim *const *sims, uint32_t n, virs_batch **out)
+{
+    if (!out || !sims || n == 0) return fail(VIRS_E_ARG, "virs_batch_create: null or empty argument");
+    *out = nullptr;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!sims[i]) return fail(VIRS_E_ARG, "virs_batch_create: null member");
+        if (!started(sims[i])) return fail(VIRS_E_STATE, "batch members must be started (virs_start_simulation)");
+        if (sims[i]->prm.device != sims[0]->prm.device || sims[i]->prm.storage != sims[0]->prm.storage)
+            return fail(VIRS_E_ARG, "batch members must share the device and the storage type");
+        for (uint32_t j = 0; j < i; ++j)
+            if (sims[j] == sims[i]) return fail(VIRS_E_ARG, "a simulation appears twice in the batch");
+    }
+    std::unique_ptr<virs_batch> b(new (std::nothrow) virs_batch());
+    if (!b) return fail(VIRS_E_OOM, "virs_batch_create: host allocation failed");
+    b->mem.assign(sims, sims + n);
+    b->gen.assign(n, 0);
+    b->dev = sims[0]->prm.device;
+    b->storage = sims[0]->prm.storage;
+    VIRS_TRY(use_device(sims[0]));
+    for (virs_sim *s : b->mem) VIRS_TRY(wait_done(s));
+    VIRS_CUDA(cudaStreamCreate(&b->stream));
+    VIRS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+    VIRS_TRY(b->err.alloc(sizeof(int), "batch error flag"));
+    VIRS_TRY(batch_build(b.get()));
+    VIRS_TRY(batch_check(b.get()));
+    VIRS_CUDA(cudaEventRecord(b->done, b->stream));
+    *out = b.release();
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_batch_destroy(virs_batch *b)
+{
+    if (!b) return VIRS_OK;
+    cudaSetDevice(b->dev);
+    cudaStreamSynchronize(b->stream);
+    delete b;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_batch_run(virs_batch *b, uint64_t steps, void *stream)
+{
+    if (!b) return fail(VIRS_E_ARG, "virs_batch_run: null");
+    VIRS_CUDA(cudaSetDevice(b->dev));
+    VIRS_TRY(batch_check(b));
+    if (steps == 0) return VIRS_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+    return batch_steps(b, steps, st, true);
+}
+
+VIRS_EXPORT virs_status virs_batch_synchronize(virs_batch *b)
+{
+    if (!b) return fail(VIRS_E_ARG, "virs_batch_synchronize: null");
+    VIRS_CUDA(cudaSetDevice(b->dev));
+    VIRS_CUDA(cudaEventSynchronize(b->done));
+    int e = 0;
+    VIRS_CUDA(cudaMemcpy(&e, b->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        VIRS_CUDA(cudaMemset(b->err.ptr, 0, sizeof(int)));
+        return fail(VIRS_E_TIMEOUT, "a batched stencil block gave up waiting for its staged planes");
+    }
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_batch_set_tiling(virs_batch *b, int rows, int planes, int depth)
+{
+    if (!b) return fail(VIRS_E_ARG, "virs_batch_set_tiling: null");
+    if (rows != 0 && rows != 4 && rows != 8 && rows != 16) return fail(VIRS_E_ARG, "tile rows must be 4, 8 or 16");
+    if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
+    if (depth < -1 || depth == 0 || depth > 3) return fail(VIRS_E_ARG, "batched runs use the TMA kernel: depth -1 or 1..3");
+    VIRS_CUDA(cudaSetDevice(b->dev));
+    VIRS_CUDA(cudaEventSynchronize(b->done));
+    b->rows = rows ? rows : 8;
+    b->planes = planes;
+    b->depth = depth < 0 ? 2 : depth;
+    return batch_build(b);
+}
+
+VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps, virs_tiling *best)
+{
+    if (!b) return fail(VIRS_E_ARG, "virs_batch_autotune: null");
+    if (trial_steps == 0 || trial_steps > 1000) return fail(VIRS_E_ARG, "trial_steps must be 1..1000");
+    VIRS_CUDA(cudaSetDevice(b->dev));
+    VIRS_TRY(batch_check(b));
+    for (virs_sim *s : b->mem) {
+        if (s->steps_done != 0) return fail(VIRS_E_STATE, "virs_batch_autotune must run before the first step");
+        if (s->ircap < 2ull * trial_steps + 2) return fail(VIRS_E_ARG, "reserve at least 2*trial_steps+2 steps");
+    }
+    cudaEvent_t e0, e1;
+    VIRS_CUDA(cudaEventCreate(&e0));
+    VIRS_CUDA(cudaEventCreate(&e1));
+    virs_tiling pick{8, 0, 2, 0.f};
+    float best_ms = 1e30f;
+    virs_status st = VIRS_OK;
+    for (int d : {1, 2, 3})
+        for (int r : {4, 8, 16})
+            for (int pl : {8, 16, 32, 64}) {
+                if (st != VIRS_OK) break;
+                b->rows = r;
+                b->depth = d;
+                b->planes = pl;
+                if ((st = batch_build(b)) != VIRS_OK) break;
+                if ((st = batch_steps(b, 1, b->stream, false)) != VIRS_OK) break;
+                cudaEventRecord(e0, b->stream);
+                if ((st = batch_steps(b, trial_steps, b->stream, false)) != VIRS_OK) break;
+                cudaEventRecord(e1, b->stream);
+                cudaError_t e = cudaEventSynchronize(e1);
+                float ms = 0;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e != cudaSuccess) {
+                    st = cuda_fail(e, "batch autotune trial");
+                    break;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    pick = {r, pl, d, ms / trial_steps};
+                }
+                for (virs_sim *s : b->mem)
+                    if ((st = reset_state(s)) != VIRS_OK) break;
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != VIRS_OK) return st;
+    b->rows = pick.tile_rows;
+    b->depth = pick.pipeline_depth;
+    b->planes = pick.planes_per_block;
+    VIRS_TRY(batch_build(b));
+    VIRS_TRY(virs_batch_synchronize(b));
+    if (best) *best = pick;
     return VIRS_OK;
 }

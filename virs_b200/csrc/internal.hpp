@@ -100,6 +100,24 @@ struct PostArgs {
     float inv_scale;
 };
 
+// one member of a batched run (device-resident descriptor)
+struct alignas(64) BatchMember {
+    CUtensorMap mapP[2];    // halo box over field[0] / field[1]
+    CUtensorMap mapQ[2];    // tile box over field[0] / field[1]
+    CUtensorMap mapC;       // cell codes
+    StepArgs step[2];       // per parity: p = field[parity], q = field[parity ^ 1]
+    PostArgs post[2];
+    const uint32_t *bidx;
+    uint64_t first_tile;    // index of this member's first tile in the batch
+    uint64_t first_bnd;     // index of this member's first boundary voxel
+    uint32_t gx, gy, gz;    // tile grid
+};
+cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
+                                  uint64_t ntiles, int parity, int *err, cudaStream_t s);
+cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
+                                  cudaStream_t s);
+cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem, int parity, cudaStream_t s);
+
 // kernel launchers (kernels_step.cu)
 cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);

@@ -162,12 +162,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
 // The compacted boundary pass (simulator_gpu.cu:105-150): one thread per
 // boundary voxel in list order; the leapfrog update (the stencil kernel
 // left these voxels untouched) and the filter correction.
-template <typename T> __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a,
-                                                                        const uint32_t *__restrict bidx)
+template <typename T>
+__device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
 {
     using IO = Io<T>;
-    const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= a.nb) return;
     const uint32_t ref = __ldg(bidx + slot);
     const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
     const size_t sy = a.px, sz = (size_t)a.px * a.ny;
@@ -182,9 +180,34 @@ template <typename T> __global__ void __launch_bounds__(256) k_boundary(const __
     Q[i] = IO::put(r);
 }
 
+template <typename T> __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a,
+                                                                        const uint32_t *__restrict bidx)
+{
+    const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot < a.nb) boundary_voxel<T>(a, bidx, slot);
+}
+
+// batched: thread g belongs to the last member whose first boundary index
+// is <= g (members without boundary voxels are skipped by that rule)
+template <typename T>
+__global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__restrict mem, uint32_t nmem,
+                                                        uint64_t ntotal, int parity)
+{
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ntotal) return;
+    uint32_t lo = 0, hi = nmem - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) / 2;
+        if (mem[mid].first_bnd <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchMember &b = mem[lo];
+    boundary_voxel<T>(b.step[parity], b.bidx, g - b.first_bnd);
+}
+
 // Additive sources, then receivers, then the step counter
 // (simulator_gpu.cu:292-300: the receiver reads the new field).
-template <typename T> __global__ void k_post(const PostArgs a)
+template <typename T> __device__ __forceinline__ void post_body(const PostArgs &a)
 {
     using IO = Io<T>;
     T *Q = static_cast<T *>(a.q);
@@ -200,6 +223,13 @@ template <typename T> __global__ void k_post(const PostArgs a)
             a.ir[(uint64_t)r * a.cap + sn] = __fmul_rn(IO::get(Q[a.rcv[r]]), a.inv_scale);
     __syncthreads();
     if (threadIdx.x == 0) *a.ctr = sn + 1;
+}
+
+template <typename T> __global__ void k_post(const __grid_constant__ PostArgs a) { post_body<T>(a); }
+
+template <typename T> __global__ void k_post_batch(const BatchMember *__restrict mem, int parity)
+{
+    post_body<T>(mem[blockIdx.x].post[parity]);
 }
 
 template <typename T>
@@ -245,6 +275,29 @@ cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx
     case VIRS_STORAGE_F16: k_boundary<__half><<<g, 256, 0, s>>>(a, bidx); break;
     case VIRS_STORAGE_BF16: k_boundary<__nv_bfloat16><<<g, 256, 0, s>>>(a, bidx); break;
     default: k_boundary<float><<<g, 256, 0, s>>>(a, bidx); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
+                                  cudaStream_t s)
+{
+    if (nbnd == 0) return cudaSuccess;
+    const unsigned g = (unsigned)((nbnd + 255) / 256);
+    switch (storage) {
+    case VIRS_STORAGE_F16: k_boundary_batch<__half><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
+    case VIRS_STORAGE_BF16: k_boundary_batch<__nv_bfloat16><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
+    default: k_boundary_batch<float><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem, int parity, cudaStream_t s)
+{
+    switch (storage) {
+    case VIRS_STORAGE_F16: k_post_batch<__half><<<nmem, 256, 0, s>>>(mem, parity); break;
+    case VIRS_STORAGE_BF16: k_post_batch<__nv_bfloat16><<<nmem, 256, 0, s>>>(mem, parity); break;
+    default: k_post_batch<float><<<nmem, 256, 0, s>>>(mem, parity); break;
     }
     return cudaGetLastError();
 }

@@ -26,6 +26,8 @@
 // the block returns (the host turns that into VIRS_E_TIMEOUT).
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "step_common.cuh"
 
 namespace virs {
@@ -134,47 +136,46 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bars, int j, int D, int *er
     return false;
 }
 
+// One tile (bx, by, bz) of one simulation.  `jg` is the block's running
+// count of issued stages; it continues across tiles so that the ring slot
+// and mbarrier phase of every stage stay consistent when a block processes
+// several tiles (the batched kernel).  Returns false when a bounded wait
+// gave up.
 template <typename T, int TY, int L>
-__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __grid_constant__ StepArgs a, const __grid_constant__ CUtensorMap mP,
-                                                     const __grid_constant__ CUtensorMap mQ,
-                                                     const __grid_constant__ CUtensorMap mC, int *err)
+__device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
+                                          const CUtensorMap *mC, int bx, int by, int bz, int *err,
+                                          unsigned char *smem, uint64_t *bars, uint32_t &jg)
 {
     using S = Stage<T, TY>;
     constexpr int PAD = Geo<T>::PAD, PW = Geo<T>::PW;
     constexpr int D = L + 3;
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * S::SB);
 
     const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
-    const int x0 = blockIdx.x * TX;
+    const int x0 = bx * TX;
     const int x = x0 + lane * 4;
-    const int y0 = blockIdx.y * TY;
+    const int y0 = by * TY;
     const int y = y0 + ty;
-    const int z0 = 1 + blockIdx.z * a.zc;
+    const int z0 = 1 + bz * a.zc;
     const int z1 = min(z0 + a.zc, (int)a.nz - 1);
-    if (z0 >= z1) return;
+    if (z0 >= z1) return true;
     const int jmax = z1 - z0 + 1; // last stage ordinal (plane z1 - 1)
     const int ny = (int)a.ny;
     const bool act = x < (int)a.px && y < ny;
     const size_t plane = (size_t)a.px * ny;
     T *Q = static_cast<T *>(a.q);
-
-    if (tid == 0) {
-        for (int s = 0; s < D; ++s) mbar_init(&bars[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
+    const uint32_t j0 = jg;
 
     auto issue = [&](int j) {
         const int k = z0 - 2 + j;
-        unsigned char *st = smem + (j % D) * S::SB;
-        uint64_t *b = bars + (j % D);
+        const uint32_t g = j0 + (uint32_t)j;
+        unsigned char *st = smem + (g % D) * S::SB;
+        uint64_t *b = bars + (g % D);
         const bool full = j >= 2;
         mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB : 0u));
-        tma_load_3d(st, &mP, b, x0 - PAD, y0 - 1, k + 1);
+        tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k + 1);
         if (full) {
-            tma_load_3d(st + S::PBa, &mQ, b, x0, y0, k);
-            tma_load_3d(st + S::PBa + S::QBa, &mC, b, x0, y0, k);
+            tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
+            tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
         }
     };
     if (tid == 0)
@@ -186,16 +187,16 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
         // z-1, so the stage that held P(z-2) can be refilled
         bool bad = false;
         if (tid == 0) {
-            bad = !wait_stage(bars, i + 2, D, err);
-            if (i == 0) bad = bad || !wait_stage(bars, 0, D, err) || !wait_stage(bars, 1, D, err);
+            bad = !wait_stage(bars, j0 + i + 2, D, err);
+            if (i == 0) bad = bad || !wait_stage(bars, j0, D, err) || !wait_stage(bars, j0 + 1, D, err);
         }
-        if (__syncthreads_or(bad)) return;
+        if (__syncthreads_or(bad)) return false;
         if (tid == 0 && i >= 1 && i + L + 2 <= jmax) issue(i + L + 2);
 
-        const T *Pm = reinterpret_cast<const T *>(smem + (i % D) * S::SB);       // P(z-1)
-        const T *Pc = reinterpret_cast<const T *>(smem + ((i + 1) % D) * S::SB); // P(z)
-        const unsigned char *s2 = smem + ((i + 2) % D) * S::SB;
-        const T *Pp = reinterpret_cast<const T *>(s2);                             // P(z+1)
+        const T *Pm = reinterpret_cast<const T *>(smem + ((j0 + i) % D) * S::SB);       // P(z-1)
+        const T *Pc = reinterpret_cast<const T *>(smem + ((j0 + i + 1) % D) * S::SB);   // P(z)
+        const unsigned char *s2 = smem + ((j0 + i + 2) % D) * S::SB;
+        const T *Pp = reinterpret_cast<const T *>(s2);                                   // P(z+1)
         const T *Qs = reinterpret_cast<const T *>(s2 + S::PBa);
         const uint32_t code4 = *reinterpret_cast<const uint32_t *>(s2 + S::PBa + S::QBa + ty * TX + lane * 4);
 
@@ -232,6 +233,57 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
             }
         }
         if (act) st4(Q + (size_t)z * plane + (size_t)y * a.px + x, r);
+    }
+    jg = j0 + (uint32_t)jmax + 1;
+    return true;
+}
+
+template <int D> __device__ __forceinline__ void init_bars(uint64_t *bars)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        for (int s = 0; s < D; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+template <typename T, int TY, int L>
+__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __grid_constant__ StepArgs a,
+                                                                        const __grid_constant__ CUtensorMap mP,
+                                                                        const __grid_constant__ CUtensorMap mQ,
+                                                                        const __grid_constant__ CUtensorMap mC, int *err)
+{
+    constexpr int D = L + 3;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
+    init_bars<D>(bars);
+    uint32_t jg = 0;
+    step_tile<T, TY, L>(a, &mP, &mQ, &mC, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
+}
+
+// Many simulations in one launch: a persistent grid walks the concatenated
+// tile lists of all members (tiles of a member are consecutive, so
+// neighbouring tiles run at the same time and share the halo rows in L2).
+template <typename T, int TY, int L>
+__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma_batch(const BatchMember *__restrict mem,
+                                                                              uint32_t nmem, uint64_t ntiles,
+                                                                              int parity, int *err)
+{
+    constexpr int D = L + 3;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
+    init_bars<D>(bars);
+    uint32_t jg = 0;
+    uint32_t m = 0;
+    for (uint64_t w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        while (m + 1 < nmem && mem[m + 1].first_tile <= w) ++m;   // tiles are visited in increasing order
+        const BatchMember &b = mem[m];
+        const uint64_t local = w - b.first_tile;
+        const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / ((uint64_t)b.gx * b.gy));
+        __syncthreads(); // every thread is done with the previous tile's stages
+        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, bx, by, bz, err,
+                                 smem, bars, jg))
+            return;
     }
 }
 
@@ -288,7 +340,56 @@ __global__ void k_wait_probe(int *err, uint32_t limit)
     if (threadIdx.x == 0) atomicExch(err, 1);
 }
 
+template <typename T, int TY, int L>
+cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, int *err, cudaStream_t s)
+{
+    auto kern = k_step_tma_batch<T, TY, L>;
+    constexpr size_t sm = smem_bytes<T, TY, L>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * TY, sm)) != cudaSuccess) return e;
+    const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)nsm * (uint64_t)std::max(per, 1));
+    kern<<<(unsigned)grid, dim3(32, TY), sm, s>>>(mem, nmem, ntiles, parity, err);
+    return cudaGetLastError();
+}
+
+template <typename T, int TY>
+cudaError_t launch_batch2(int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, int *err,
+                          cudaStream_t s)
+{
+    switch (depth) {
+    case 1: return launch_batch3<T, TY, 1>(mem, nmem, ntiles, parity, err, s);
+    case 3: return launch_batch3<T, TY, 3>(mem, nmem, ntiles, parity, err, s);
+    default: return launch_batch3<T, TY, 2>(mem, nmem, ntiles, parity, err, s);
+    }
+}
+
+template <typename T>
+cudaError_t launch_batch1(int rows, int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity,
+                          int *err, cudaStream_t s)
+{
+    switch (rows) {
+    case 4: return launch_batch2<T, 4>(depth, mem, nmem, ntiles, parity, err, s);
+    case 16: return launch_batch2<T, 16>(depth, mem, nmem, ntiles, parity, err, s);
+    default: return launch_batch2<T, 8>(depth, mem, nmem, ntiles, parity, err, s);
+    }
+}
+
 } // namespace
+
+cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
+                                  uint64_t ntiles, int parity, int *err, cudaStream_t s)
+{
+    if (ntiles == 0) return cudaSuccess;
+    switch (storage) {
+    case VIRS_STORAGE_F16: return launch_batch1<__half>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
+    case VIRS_STORAGE_BF16: return launch_batch1<__nv_bfloat16>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
+    default: return launch_batch1<float>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
+    }
+}
 
 int tma_box_width(int storage) { return storage == VIRS_STORAGE_F32 ? TX + 8 : TX + 16; }
 int tma_pad(int storage) { return storage == VIRS_STORAGE_F32 ? 4 : 8; }

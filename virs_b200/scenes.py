@@ -161,6 +161,43 @@ def large_hall(seed: int = 3, steps: int = 4000, size=(1024, 768, 512), h: float
                  src, sig, rcv, seed=seed)
 
 
+def batched(seed: int = 5, steps: int = 3000, n_sources: int = 64, n_rooms: int = 16, room: int = 256,
+            size_range=(96, 320), h: float = 1.0 / 64.0) -> list[Scene]:
+    """The batched workload: n_sources seeded source positions in one room of
+    room^3 voxels (one simulation per source) plus n_rooms rooms whose voxel
+    counts lie between size_range[0]^3 and size_range[1]^3 with seeded aspect
+    ratios and 1-4 materials (3-section cascades), each with one source and
+    one receiver."""
+    rng = np.random.default_rng(seed)
+    fs = fs_of(h, 1.0)
+    out = []
+    L = np.full(3, room * h)
+    v, t, m = box((0, 0, 0), L, [0, 0, 0, 0, 1, 1])
+    alpha = rng.uniform(0.05, 0.8, (2, 3))
+    coef = np.stack([design_octave_cascade_np(fs, a) for a in alpha])
+    rcv = _interior_points(rng, (0, 0, 0), L, 1, 0.5)
+    srcs = _interior_points(rng, (0, 0, 0), L, n_sources, 0.5)
+    sig = diff_gaussian(steps, 8.0)[None, :]
+    for k in range(n_sources):
+        out.append(Scene(f"batch_src{k}", v, t, m, np.array([0, 1], np.uint8), h, 0.0, 1.0, 1, steps, 2, 3, coef,
+                         srcs[k:k + 1], sig, rcv, seed=seed))
+    for k in range(n_rooms):
+        side = rng.uniform(size_range[0], size_range[1])
+        aspect = rng.uniform(0.6, 1.6, 3)
+        aspect /= np.cbrt(aspect.prod())
+        dims = np.clip(np.round(side * aspect / 8) * 8, 32, 512)
+        L = dims * h
+        nm = int(rng.integers(1, 5))
+        v, t, m = box((0, 0, 0), L, rng.integers(0, nm, 6))
+        alpha = rng.uniform(0.05, 0.8, (nm, 3))
+        coef = np.stack([design_octave_cascade_np(fs, a) for a in alpha])
+        src = _interior_points(rng, (0, 0, 0), L, 1, 0.3)
+        rc = _interior_points(rng, (0, 0, 0), L, 1, 0.3)
+        out.append(Scene(f"batch_room{k}", v, t, m, np.arange(nm, dtype=np.uint8), h, 0.0, 1.0, 1, steps, nm, 3,
+                         coef, src, sig, rc, seed=seed))
+    return out
+
+
 def reference_room(seed: int = 4, steps: int = 300, size=(48, 40, 32), h: float = 0.05) -> Scene:
     """The reference's configuration on a small grid: material 0 walls,
     material 1 a speaker box (hard source), default filter and constants."""
