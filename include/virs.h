@@ -218,6 +218,21 @@ virs_status virs_init_pressure_sphere(virs_sim *sim, uint64_t x, uint64_t y, uin
 /* FP64 discrete energy of the current state (the physics health monitor). */
 virs_status virs_energy(virs_sim *sim, double *out);
 
+/* The same energy for callers that cannot allocate device memory (no
+ * counterpart in the reference): real-time threads, where cudaMalloc and
+ * cudaFree may synchronise the device and block, or hosts that own all
+ * device memory through their own pool.  virs_energy allocates its
+ * reduction buffer on first use; this variant keeps one partial sum per z
+ * plane in a static device array of VIRS_ENERGY_MAX_PLANES doubles (64 KiB,
+ * held by every GPU that loads the library until exit) and calls no
+ * allocator.  Grids with more planes get VIRS_E_ARG.  The result is written
+ * to the caller's device double `d_out`, in order on `stream` (NULL = the
+ * handle's stream); nothing waits for it.  The first call on a device looks
+ * up the array's address (cudaGetSymbolAddress): make it before any stream
+ * capture.  All calls share the array, so calls whose work overlaps on the
+ * GPU race. */
+#define VIRS_ENERGY_MAX_PLANES 8192
+virs_status virs_energy_noalloc(virs_sim *sim, double *d_out, void *stream);
 
 /* ---- measurement ------------------------------------------------------------- */
 

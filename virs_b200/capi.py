@@ -89,6 +89,7 @@ _SIGS = {
     "virs_set_pressure": ([_P, _P, _P, C.c_size_t], C.c_int),
     "virs_init_pressure_sphere": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_int], C.c_int),
     "virs_energy": ([_P, _P], C.c_int),
+    "virs_energy_noalloc": ([_P, _P, _P], C.c_int),
     "virs_set_timing": ([_P, C.c_int], C.c_int),
     "virs_get_timing": ([_P, _P], C.c_int),
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -341,6 +342,10 @@ class Simulation:
         e = C.c_double()
         check(lib().virs_energy(self._h, C.byref(e)))
         return float(e.value)
+
+    def energy_noalloc(self, d_out_ptr: int, stream: int | None = None) -> None:
+        """Enqueue the allocation-free energy into the device double at d_out_ptr."""
+        check(lib().virs_energy_noalloc(self._h, d_out_ptr, stream))
 
     def set_timing(self, enable: bool):
         check(lib().virs_set_timing(self._h, int(enable)))

@@ -1359,6 +1359,35 @@ VIRS_EXPORT virs_status virs_get_tiling(const virs_sim *s, virs_tiling *out)
     return VIRS_OK;
 }
 
+namespace virs {
+
+// inputs of the allocation-free energy monitor; orders `stream` after the
+// handle's queued work with an event (no allocation)
+virs_status energy_inputs(virs_sim *s, void *stream, EnergyInputs *in)
+{
+    if (!s->classified) return fail(VIRS_E_STATE, "grid not classified");
+    VIRS_TRY(use_device(s));
+    in->p = s->field[s->cur].ptr;
+    in->q = s->field[s->cur ^ 1].ptr;
+    in->code = s->code.as<uint8_t>();
+    in->nx = s->nx;
+    in->ny = s->ny;
+    in->nz = s->nz;
+    in->px = s->px;
+    in->storage = s->prm.storage;
+    in->device = s->prm.device;
+    in->lambda2 = (double)s->c2dt2 * (double)s->inv_h2;
+    in->scale2 = (double)s->inv_scale * (double)s->inv_scale;
+    in->stream = stream ? (cudaStream_t)stream : s->stream;
+    if (in->stream != s->stream) {
+        VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+        VIRS_CUDA(cudaStreamWaitEvent(in->stream, s->done, 0));
+    }
+    return VIRS_OK;
+}
+
+} // namespace virs
+
 // ============================================================================
 // batched runs: many simulations advanced together, three launches per step
 // ============================================================================

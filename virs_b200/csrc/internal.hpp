@@ -186,6 +186,17 @@ cudaError_t launch_pack(int storage, const void *field, float *out, uint32_t nx,
 cudaError_t launch_unpack(int storage, const float *in, void *field, uint32_t nx, uint32_t ny, uint32_t nz,
                           uint32_t px, float scale, cudaStream_t s);
 
+// what virs_energy_noalloc needs from a handle (capi.cpp)
+struct EnergyInputs {
+    const void *p, *q;
+    const uint8_t *code;
+    uint32_t nx, ny, nz, px;
+    int storage, device;
+    double lambda2, scale2;
+    cudaStream_t stream;
+};
+virs_status energy_inputs(virs_sim *sim, void *stream, EnergyInputs *out);
+
 // ---- host-side geometry (voxelize.cpp, design.cpp) ---------------------------
 
 struct Mesh {
