@@ -23,7 +23,9 @@ The JSON line carries:
               bandwidth of MEASURED_PEAKS.json
   cpu_baseline  the CPU oracle's FP32 step (OpenMP, all host threads) on a
               crop of the hall
-  variants    the BF16-storage form of the same hall
+  variants    the BF16-storage form of the same hall, and the batched
+              workload (64 source positions in a 256^3 room + 16 rooms of
+              96^3..320^3, 1.29 G voxels per step) in FP32 and BF16 storage
 
 --impl reference times the reference's CPU implementation of this path.
 The reference's own CPU build cannot be compiled here (oneTBB, Embree,
@@ -210,6 +212,36 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     return out
 
 
+def bench_batch(storage, args, stream, dev):
+    """The batched workload: 64 source positions in a 256^3 room plus 16 rooms
+    of 96^3..320^3, advanced by three launches per step (virs_batch)."""
+    import torch
+    from virs_b200 import capi, scenes
+    steps, warm = args.batch_steps, 5
+    scs = scenes.batched(steps=steps + warm + 2 * 3 + 4)
+    sims = [scenes.build_simulation(sc, storage=storage, device=dev)[0] for sc in scs]
+    nvox = sum(int(np.prod(s.shape)) for s in sims)
+    b = capi.Batch(sims)
+    t = b.autotune(2)
+    b.run(warm, stream.cuda_stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.run(steps, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    b.synchronize()
+    ok = all(bool(np.isfinite(s.ir()).all()) for s in sims)
+    b.close()
+    for s in sims:
+        s.close()
+    return {"value": nvox * steps / (ms * 1e-3) / 1e9, "ms_per_step": ms / steps, "members": len(scs),
+            "voxels_per_step": nvox, "steps": steps, "tiling": [t.tile_rows, t.planes_per_block, t.pipeline_depth],
+            "ir_finite": ok, "launches_per_step": 3}
+
+
 def cpu_sample(shape, steps_budget_s, threads):
     """The oracle's FP32 step on a crop of the hall (same x, y extent, fewer
     planes), timed on the host; returns (Gvox/s, description)."""
@@ -266,6 +298,12 @@ def run_virs(args):
             "roofline_frac": (nvox * BYTES_16 / (rb["kernel_ms"] * 1e-3) / 1e9) / peak if rb.get("kernel_ms") else None,
             "bytes_per_voxel": BYTES_16,
         }
+    if args.batch_steps:
+        for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):
+            rb = bench_batch(st, args, stream, dev)
+            rb["value"] *= world
+            variants[name] = rb
+        variants["bf16_batched_vs_f32_plain"] = None   # filled below
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -322,6 +360,8 @@ def run_virs(args):
         "clocks": r32["clocks"],
         "variants": variants,
     }
+    if "batched_bf16" in variants:
+        variants["bf16_batched_vs_f32_plain"] = round(variants["batched_bf16"]["value"] / value, 3)
     if args.traffic_json and Path(args.traffic_json).exists():
         line["roofline"]["traffic"] = json.loads(Path(args.traffic_json).read_text()).get("bytes_per_launch")
     if world == 1 and not args.no_cpu:
@@ -408,6 +448,7 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=4, help="steps per candidate of virs_autotune (0 = no tuning)")
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=60, help="timed steps of the batched workload (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--traffic-json", default=str(ROOT / "profiles" / "step_traffic.json"))
     args = ap.parse_args()

@@ -263,6 +263,21 @@ typedef struct virs_tiling {
 virs_status virs_autotune(virs_sim *sim, uint32_t trial_steps, virs_tiling *best);
 virs_status virs_get_tiling(const virs_sim *sim, virs_tiling *out);
 
+/* ---- adjoint ----------------------------------------------------------------- */
+
+/* Gradients of a receiver loss (no reference counterpart; used for inverse
+ * design of boundary materials).  virs_forward_checkpointed starts from rest
+ * and runs `steps` FP32 steps, keeping the state every `every` steps.
+ * virs_adjoint then takes dL/dIR (dl_dir [n_rcv][steps], host) and returns
+ * dL/dcoeff (grad_coef [n_materials][n_sections][5] = {b0 b1 b2 a1 a2},
+ * FP64) and dL/dsignal (grad_signal [n_src][steps]); either output may be
+ * NULL.  Each checkpoint segment is recomputed once; the reverse pass runs
+ * the step backwards in time (the interior update is self-adjoint, the
+ * filters run transposed).  The receiver samples of the forward run stay
+ * readable; the fields do not, so start again before running. */
+virs_status virs_forward_checkpointed(virs_sim *sim, uint64_t steps, uint32_t every, void *stream);
+virs_status virs_adjoint(virs_sim *sim, const float *dl_dir, double *grad_coef, float *grad_signal);
+
 /* ---- batched runs ------------------------------------------------------------ */
 
 /* Many simulations advanced together (no reference counterpart: the

@@ -78,6 +78,8 @@ def lib():
         L.vo_run_f32.argtypes = [C.c_void_p]
         L.vo_run_f64.restype = C.c_int
         L.vo_run_f64.argtypes = [C.c_void_p]
+        L.vo_adjoint_f64.restype = C.c_int
+        L.vo_adjoint_f64.argtypes = [C.c_void_p]
         L.vo_energy_f32.restype = C.c_double
         L.vo_energy_f32.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _u8p, _f32p, _f32p, C.c_double]
         L.vo_set_threads.argtypes = [C.c_int]
@@ -225,7 +227,13 @@ class _RunArgs(C.Structure):
         ("n_rcv", C.c_uint32), ("rcv_idx", C.c_void_p),
         ("steps", C.c_uint64), ("step0", C.c_uint64), ("ir_stride", C.c_uint64),
         ("ir", C.c_void_p), ("p", C.c_void_p), ("pprev", C.c_void_p), ("state", C.c_void_p),
+        ("ir64", C.c_void_p),
     ]
+
+
+class _AdjArgs(C.Structure):
+    _fields_ = [("run", C.c_void_p), ("dl_dir", C.c_void_p), ("every", C.c_uint32), ("grad_coef", C.c_void_p),
+                ("grad_sig", C.c_void_p)]
 
 
 def _ptr(a):
@@ -279,6 +287,34 @@ class Scene:
         a.steps, a.step0, a.ir_stride = steps, step0, steps
         a.ir, a.p, a.pprev, a.state = _ptr(ir), _ptr(p), _ptr(pp), _ptr(st)
         return a
+
+    def run64(self, steps):
+        """FP64 run returning the receiver samples in double [R, steps]."""
+        ir = np.zeros((max(self.rcv_idx.size, 1), steps), np.float32)
+        ir64 = np.zeros((max(self.rcv_idx.size, 1), steps), np.float64)
+        a = self._args(steps, 0, ir, None, None, None, True)
+        a.ir64 = ir64.ctypes.data
+        if lib().vo_run_f64(C.byref(a)) != 0:
+            raise MemoryError("oracle run: allocation failed")
+        return ir64[: self.rcv_idx.size]
+
+    def adjoint64(self, steps, dl_dir, every=64):
+        """Gradients of a receiver loss through the FP64 model: returns
+        (dL/dcoef [M][S][5], dL/dsignal [n_src][steps])."""
+        dl = np.ascontiguousarray(dl_dir, np.float64).reshape(self.rcv_idx.size, steps)
+        gc = np.zeros(self.n_materials * self.n_sections * 5, np.float64)
+        gs = np.zeros((max(self.src_idx.size, 1), steps), np.float64)
+        ir = np.zeros((max(self.rcv_idx.size, 1), steps), np.float32)
+        a = self._args(steps, 0, ir, None, None, None, True)
+        aa = _AdjArgs()
+        aa.run = C.addressof(a)
+        aa.dl_dir = dl.ctypes.data
+        aa.every = int(every)
+        aa.grad_coef = gc.ctypes.data
+        aa.grad_sig = gs.ctypes.data
+        if lib().vo_adjoint_f64(C.byref(aa)) != 0:
+            raise MemoryError("oracle adjoint: allocation failed")
+        return gc.reshape(self.n_materials, self.n_sections, 5), gs[: self.src_idx.size]
 
     def run(self, steps, *, f64=False, step0=0, state=None):
         """Run ``steps`` steps.  ``state`` = (p, pprev, biquad_states) to

@@ -428,6 +428,7 @@ typedef struct vo_run_args {
     void *p;                       /* in/out p^n      (float or double)    */
     void *pprev;                   /* in/out p^{n-1}                       */
     void *state;                   /* in/out [nb][S][4]                    */
+    double *ir64;                  /* FP64 run: IR in double (may be NULL) */
 } vo_run_args;
 
 static inline float vsel(const uint8_t *fl, const float *p, uint64_t n, float c)
@@ -561,11 +562,56 @@ VO_API int vo_run_f32(const vo_run_args *a)
     return 0;
 }
 
+/* One step of the model in double precision (interior, boundary, sources). */
+static void f64_step(const vo_run_args *a, const double *pc, const double *pp, double *pn, double *st, uint64_t sn)
+{
+    const uint64_t nx = a->nx, ny = a->ny, nz = a->nz, sy = nx, sz = nx * ny;
+    const uint8_t *fl = a->flags;
+    const uint32_t S = a->n_sections;
+    const double hard = sn < a->n_hard ? (double)a->hard[sn] : 0.0;
+    const double c2dt2 = a->c2dt2_d, inv_h2 = a->inv_h2_d;
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+    for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+        for (uint64_t y = 1; y + 1 < ny; ++y)
+            for (uint64_t x = 1; x + 1 < nx; ++x) {
+                const uint64_t i = (uint64_t)z * sz + y * sy + x;
+                const uint8_t f = fl[i];
+                if (f == 1) { pn[i] = 0.0; continue; }
+                if (f == 3) { pn[i] = hard; continue; }
+                if (f != 0 && f != 2) continue;
+                const double c = pc[i];
+                double s = (fl[i + 1] == 1 ? c : pc[i + 1]) + (fl[i - 1] == 1 ? c : pc[i - 1]) +
+                           (fl[i + sy] == 1 ? c : pc[i + sy]) + (fl[i - sy] == 1 ? c : pc[i - sy]) +
+                           (fl[i + sz] == 1 ? c : pc[i + sz]) + (fl[i - sz] == 1 ? c : pc[i - sz]);
+                pn[i] = 2.0 * c - pp[i] + c2dt2 * ((s - 6.0 * c) * inv_h2);
+            }
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+    for (int64_t b = 0; b < (int64_t)a->nb; ++b) {
+        const uint64_t i = a->bidx[b];
+        const double d = pc[i] - pp[i];
+        double in = d;
+        const double *k = a->coef64 + (uint64_t)a->bmat[b] * S * 5;
+        double *s = st + (uint64_t)b * S * 4;
+        for (uint32_t q = 0; q < S; ++q, k += 5, s += 4) {
+            double y = k[0] * in + k[1] * s[0] + k[2] * s[1] - k[3] * s[2] - k[4] * s[3];
+            s[1] = s[0]; s[0] = in; s[3] = s[2]; s[2] = y; in = y;
+        }
+        const double w = a->bw ? (double)a->bw[b] : 1.0;
+        if (a->form == 0) {
+            pn[i] -= a->K_d * (in * a->mix_y + d * a->mix_d) * a->gain * w;
+        } else {
+            const double kgw = a->K_d * a->gain * w, ac = kgw * a->mix_d * 0.5;
+            pn[i] = (pn[i] - kgw * in * a->mix_y + ac * pp[i]) / (1.0 + ac);
+        }
+    }
+    for (uint32_t s = 0; s < a->n_src; ++s) pn[a->src_idx[s]] += (double)sig_at(a, s, sn);
+}
+
 /* The same model in double precision: the truth the reduced-precision forms
  * are measured against.  Coefficients come from a->coef64. */
 VO_API int vo_run_f64(const vo_run_args *a)
 {
-    const uint64_t N = a->nx * a->ny * a->nz, nx = a->nx, ny = a->ny, nz = a->nz, sy = nx, sz = nx * ny;
+    const uint64_t N = a->nx * a->ny * a->nz;
     double *b0 = calloc(N, sizeof(double)), *b1 = calloc(N, sizeof(double)), *b2 = calloc(N, sizeof(double));
     const uint64_t nst = a->nb * a->n_sections * 4;
     double *st = calloc(nst ? nst : 1, sizeof(double));
@@ -574,56 +620,187 @@ VO_API int vo_run_f64(const vo_run_args *a)
     if (a->pprev) memcpy(b1, a->pprev, N * sizeof(double));
     if (a->state) memcpy(st, a->state, nst * sizeof(double));
     double *pc = b0, *pp = b1, *pn = b2;
-    const uint8_t *fl = a->flags;
-    const uint32_t S = a->n_sections;
     for (uint64_t n = 0; n < a->steps; ++n) {
-        const uint64_t sn = a->step0 + n;
-        const double hard = sn < a->n_hard ? (double)a->hard[sn] : 0.0;
-        const double c2dt2 = a->c2dt2_d, inv_h2 = a->inv_h2_d;
-#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
-        for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
-            for (uint64_t y = 1; y + 1 < ny; ++y)
-                for (uint64_t x = 1; x + 1 < nx; ++x) {
-                    const uint64_t i = (uint64_t)z * sz + y * sy + x;
-                    const uint8_t f = fl[i];
-                    if (f == 1) { pn[i] = 0.0; continue; }
-                    if (f == 3) { pn[i] = hard; continue; }
-                    if (f != 0 && f != 2) continue;
-                    const double c = pc[i];
-                    double s = (fl[i + 1] == 1 ? c : pc[i + 1]) + (fl[i - 1] == 1 ? c : pc[i - 1]) +
-                               (fl[i + sy] == 1 ? c : pc[i + sy]) + (fl[i - sy] == 1 ? c : pc[i - sy]) +
-                               (fl[i + sz] == 1 ? c : pc[i + sz]) + (fl[i - sz] == 1 ? c : pc[i - sz]);
-                    pn[i] = 2.0 * c - pp[i] + c2dt2 * ((s - 6.0 * c) * inv_h2);
-                }
-#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
-        for (int64_t b = 0; b < (int64_t)a->nb; ++b) {
-            const uint64_t i = a->bidx[b];
-            const double d = pc[i] - pp[i];
-            double in = d;
-            const double *k = a->coef64 + (uint64_t)a->bmat[b] * S * 5;
-            double *s = st + (uint64_t)b * S * 4;
-            for (uint32_t q = 0; q < S; ++q, k += 5, s += 4) {
-                double y = k[0] * in + k[1] * s[0] + k[2] * s[1] - k[3] * s[2] - k[4] * s[3];
-                s[1] = s[0]; s[0] = in; s[3] = s[2]; s[2] = y; in = y;
-            }
-            const double w = a->bw ? (double)a->bw[b] : 1.0;
-            if (a->form == 0) {
-                pn[i] -= a->K_d * (in * a->mix_y + d * a->mix_d) * a->gain * w;
-            } else {
-                const double kgw = a->K_d * a->gain * w, ac = kgw * a->mix_d * 0.5;
-                pn[i] = (pn[i] - kgw * in * a->mix_y + ac * pp[i]) / (1.0 + ac);
-            }
-        }
-        for (uint32_t s = 0; s < a->n_src; ++s) pn[a->src_idx[s]] += (double)sig_at(a, s, sn);
+        f64_step(a, pc, pp, pn, st, a->step0 + n);
         double *t = pp; pp = pc; pc = pn; pn = t;
-        for (uint32_t r = 0; r < a->n_rcv; ++r)
+        for (uint32_t r = 0; r < a->n_rcv; ++r) {
             a->ir[(uint64_t)r * a->ir_stride + n] = (float)pc[a->rcv_idx[r]];
+            if (a->ir64) a->ir64[(uint64_t)r * a->ir_stride + n] = pc[a->rcv_idx[r]];
+        }
     }
     if (a->p) memcpy(a->p, pc, N * sizeof(double));
     if (a->pprev) memcpy(a->pprev, pp, N * sizeof(double));
     if (a->state) memcpy(a->state, st, nst * sizeof(double));
     free(b0); free(b1); free(b2); free(st);
     return 0;
+}
+
+/* Reverse-mode gradient of a receiver loss through the FP64 model.
+ *
+ * Given dL/dIR (dl_dir, [n_rcv][steps]) the adjoint runs the steps backwards.
+ * With T the adjoint of p^{n+1} and RR the negated adjoint carried through
+ * the q-role of p^n, one reverse step n is:
+ *   T[rcv] += dL/dIR_n;  dL/dsig_n = T[src];
+ *   F = T, except at boundary voxels where the correction's adjoint acts
+ *   (reference form: F = T, ybar = -K g w mix_y T, dbar = -K g w mix_d T;
+ *   centered form: F = T/(1+a), ybar = -K g w mix_y T/(1+a), cq = a T/(1+a));
+ *   the biquad cascade runs transposed (sections last to first), giving the
+ *   coefficient gradients, the state adjoints and dbar += xbar_0;
+ *   T' = A F - RR (+ dbar at boundary voxels)   -- the forward leapfrog
+ *   RR' = F (+ dbar - cq at boundary voxels).
+ * A is symmetric on the updated voxels (walls mirrored, fixed voxels 0), so
+ * the interior adjoint is the leapfrog itself.  Forward states are rebuilt
+ * from checkpoints taken every `every` steps. */
+typedef struct vo_adj_args {
+    const vo_run_args *run;       /* forward set-up (FP64 fields used) */
+    const double *dl_dir;         /* [n_rcv][steps]                    */
+    uint32_t every;               /* checkpoint interval (>= 1)        */
+    double *grad_coef;            /* [M][S][5], accumulated            */
+    double *grad_sig;             /* [n_src][steps] or NULL            */
+} vo_adj_args;
+
+VO_API int vo_adjoint_f64(const vo_adj_args *aa)
+{
+    const vo_run_args *a = aa->run;
+    const uint64_t N = a->nx * a->ny * a->nz, nx = a->nx, ny = a->ny, nz = a->nz, sy = nx, sz = nx * ny;
+    const uint64_t steps = a->steps, every = aa->every ? aa->every : 64;
+    const uint32_t S = a->n_sections;
+    const uint64_t nb = a->nb, nst = nb * S * 4;
+    const uint64_t nck = (steps + every - 1) / every;
+    const uint8_t *fl = a->flags;
+    double *ckp = calloc(nck * N, sizeof(double)), *ckq = calloc(nck * N, sizeof(double));
+    double *cks = calloc(nck * (nst ? nst : 1), sizeof(double));
+    double *b0 = calloc(N, sizeof(double)), *b1 = calloc(N, sizeof(double)), *b2 = calloc(N, sizeof(double));
+    double *st = calloc(nst ? nst : 1, sizeof(double));
+    double *segD = calloc(every * (nb ? nb : 1), sizeof(double));
+    double *segS = calloc(every * (nst ? nst : 1), sizeof(double));
+    double *T = calloc(N, sizeof(double)), *RR = calloc(N, sizeof(double)), *AS = calloc(nst ? nst : 1, sizeof(double));
+    double *dbar = calloc(nb ? nb : 1, sizeof(double)), *cqv = calloc(nb ? nb : 1, sizeof(double));
+    uint8_t *active = calloc(N, 1);
+    int rc = 0;
+    if (!ckp || !ckq || !cks || !b0 || !b1 || !b2 || !st || !segD || !segS || !T || !RR || !AS || !dbar || !cqv ||
+        !active) { rc = -1; goto done; }
+    for (uint64_t z = 1; z + 1 < nz; ++z)
+        for (uint64_t y = 1; y + 1 < ny; ++y)
+            for (uint64_t x = 1; x + 1 < nx; ++x) {
+                const uint64_t i = z * sz + y * sy + x;
+                active[i] = fl[i] == 0 || fl[i] == 2;
+            }
+    {
+        /* forward with checkpoints */
+        double *pc = b0, *pp = b1, *pn = b2;
+        for (uint64_t n = 0; n < steps; ++n) {
+            if (n % every == 0) {
+                const uint64_t c = n / every;
+                memcpy(ckp + c * N, pc, N * sizeof(double));
+                memcpy(ckq + c * N, pp, N * sizeof(double));
+                if (nst) memcpy(cks + c * nst, st, nst * sizeof(double));
+            }
+            f64_step(a, pc, pp, pn, st, a->step0 + n);
+            double *t = pp; pp = pc; pc = pn; pn = t;
+        }
+    }
+    const double lam2 = a->c2dt2_d * a->inv_h2_d;
+    for (int64_t c = (int64_t)nck - 1; c >= 0; --c) {
+        const uint64_t n0 = (uint64_t)c * every, n1 = n0 + every < steps ? n0 + every : steps;
+        /* rebuild the segment's forward boundary data */
+        double *pc = b0, *pp = b1, *pn = b2;
+        memcpy(pc, ckp + c * N, N * sizeof(double));
+        memcpy(pp, ckq + c * N, N * sizeof(double));
+        if (nst) memcpy(st, cks + c * nst, nst * sizeof(double));
+        for (uint64_t n = n0; n < n1; ++n) {
+            const uint64_t k = n - n0;
+            for (uint64_t b = 0; b < nb; ++b) segD[k * nb + b] = pc[a->bidx[b]] - pp[a->bidx[b]];
+            if (nst) memcpy(segS + k * nst, st, nst * sizeof(double));
+            f64_step(a, pc, pp, pn, st, a->step0 + n);
+            double *t = pp; pp = pc; pc = pn; pn = t;
+        }
+        for (int64_t n = (int64_t)n1 - 1; n >= (int64_t)n0; --n) {
+            const uint64_t k = (uint64_t)n - n0;
+            for (uint32_t r = 0; r < a->n_rcv; ++r) {
+                const uint64_t i = a->rcv_idx[r];
+                if (active[i]) T[i] += aa->dl_dir[(uint64_t)r * steps + (uint64_t)n];
+            }
+            if (aa->grad_sig)
+                for (uint32_t s = 0; s < a->n_src; ++s) aa->grad_sig[(uint64_t)s * steps + (uint64_t)n] = T[a->src_idx[s]];
+            /* boundary voxels: correction and cascade, transposed */
+            for (uint64_t b = 0; b < nb; ++b) {
+                const uint64_t i = a->bidx[b];
+                const double f = T[i], w = a->bw ? (double)a->bw[b] : 1.0;
+                const double kgw = a->K_d * a->gain * w;
+                double ybar, db, fr, cq = 0.0;
+                if (a->form == 0) {
+                    fr = f;
+                    ybar = -kgw * a->mix_y * f;
+                    db = -kgw * a->mix_d * f;
+                } else {
+                    const double ac = kgw * a->mix_d * 0.5;
+                    fr = f / (1.0 + ac);
+                    ybar = -kgw * a->mix_y * fr;
+                    db = 0.0;
+                    cq = ac * fr;
+                }
+                /* forward values of the sections at step n */
+                const double *k5 = a->coef64 + (uint64_t)a->bmat[b] * S * 5;
+                const double *s0 = segS + k * nst + b * S * 4;
+                double xin[16];
+                double in = segD[k * nb + b];
+                for (uint32_t q = 0; q < S; ++q) {
+                    const double *kk = k5 + 5 * q, *ss = s0 + 4 * q;
+                    xin[q] = in;
+                    in = kk[0] * in + kk[1] * ss[0] + kk[2] * ss[1] - kk[3] * ss[2] - kk[4] * ss[3];
+                }
+                double *as = AS + b * S * 4;
+                double *g = aa->grad_coef + (uint64_t)a->bmat[b] * S * 5;
+                double yb = ybar;
+                for (int32_t q = (int32_t)S - 1; q >= 0; --q) {
+                    const double *kk = k5 + 5 * q, *ss = s0 + 4 * q;
+                    double *aq = as + 4 * q;
+                    const double yt = yb + aq[2];              /* Y1+ = y */
+                    g[5 * q + 0] += yt * xin[q];
+                    g[5 * q + 1] += yt * ss[0];
+                    g[5 * q + 2] += yt * ss[1];
+                    g[5 * q + 3] -= yt * ss[2];
+                    g[5 * q + 4] -= yt * ss[3];
+                    const double xbar = kk[0] * yt + aq[0];    /* X1+ = x */
+                    const double x1 = kk[1] * yt + aq[1];      /* X2+ = X1 */
+                    const double x2 = kk[2] * yt;
+                    const double y1 = -kk[3] * yt + aq[3];     /* Y2+ = Y1 */
+                    const double y2 = -kk[4] * yt;
+                    aq[0] = x1; aq[1] = x2; aq[2] = y1; aq[3] = y2;
+                    yb = xbar;
+                }
+                db += yb;
+                T[i] = fr;
+                dbar[b] = db;
+                cqv[b] = cq;
+            }
+            /* T' = A F - RR into RR's buffer; RR' = F (T's buffer) */
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+            for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
+                for (uint64_t y = 1; y + 1 < ny; ++y)
+                    for (uint64_t x = 1; x + 1 < nx; ++x) {
+                        const uint64_t i = (uint64_t)z * sz + y * sy + x;
+                        if (!active[i]) { RR[i] = 0.0; continue; }
+                        const double c0 = T[i];
+                        double acc = 0.0;
+                        const uint64_t nbr[6] = {i + 1, i - 1, i + sy, i - sy, i + sz, i - sz};
+                        for (int d = 0; d < 6; ++d)
+                            if (fl[nbr[d]] != 1) acc += T[nbr[d]] - c0;
+                        RR[i] = 2.0 * c0 - RR[i] + lam2 * acc;
+                    }
+            for (uint64_t b = 0; b < nb; ++b) {
+                const uint64_t i = a->bidx[b];
+                RR[i] += dbar[b];
+                T[i] += dbar[b] - cqv[b];
+            }
+            double *t = T; T = RR; RR = t;
+        }
+    }
+done:
+    free(ckp); free(ckq); free(cks); free(b0); free(b1); free(b2); free(st); free(segD); free(segS);
+    free(T); free(RR); free(AS); free(dbar); free(cqv); free(active);
+    return rc;
 }
 
 /* Discrete energy of the lossless interior scheme (FP64):

@@ -219,3 +219,57 @@ def test_fp32_close_to_fp64_reference_room():
     b = osc.run(sc.steps, f64=True)
     assert np.isfinite(a).all()
     assert rel_l2(a, b) < 1e-5
+
+
+@pytest.mark.parametrize("form,courant", [(0, 0.5), (1, 1.0)])
+def test_fp64_adjoint_matches_finite_differences(form, courant):
+    """Gradients of an IR loss w.r.t. filter coefficients and source samples
+    from the FP64 adjoint (checkpoints every 16 steps) against central
+    differences with h = 1e-3, Richardson-extrapolated (h and h/2) to remove
+    the O(h^2) truncation of the strongly non-linear denominator terms."""
+    import dataclasses
+    sc, _ = scenes.inverse_design(steps=120, size=(20, 18, 14), h=0.05, n_materials=3)
+    sc = dataclasses.replace(sc, courant=courant)
+    if form == 0:
+        sc = dataclasses.replace(sc, coef64=sc.coef64)
+    g = oracle_grid(sc)
+    osc = oracle_scene(sc, g)
+    osc.form = form
+    target = osc.run64(sc.steps) * 0.9 + 0.01
+
+    def loss():
+        ir = osc.run64(sc.steps)
+        return np.sum((ir - target) ** 2) / ir.size, ir
+
+    _, ir = loss()
+    gc, gs = osc.adjoint64(sc.steps, 2 * (ir - target) / ir.size, every=16)
+
+    def fd(setv, base, h):
+        setv(base + h); lp, _ = loss()
+        setv(base - h); lm, _ = loss()
+        setv(base)
+        return (lp - lm) / (2 * h)
+
+    for (m, s, j) in [(0, 0, 0), (1, 1, 3), (2, 0, 4), (0, 1, 1), (2, 1, 2)]:
+        k = (m * osc.n_sections + s) * 5 + j
+        base = osc.coef64[k]
+
+        def setv(v, k=k):
+            osc.coef64[k] = v
+
+        d1, d2 = fd(setv, base, 1e-3), fd(setv, base, 5e-4)
+        rich = (4 * d2 - d1) / 3
+        assert abs(rich - gc[m, s, j]) <= 1e-4 * abs(gc[m, s, j]) + 1e-14, (m, s, j, rich, gc[m, s, j])
+    for (s, n) in [(0, 10), (0, 60)]:
+        base = float(osc.src_sig[s, n])
+        h = np.float32(1e-3)
+
+        def setv(v, s=s, n=n):
+            osc.src_sig[s, n] = v
+
+        setv(np.float32(base) + h); lp, _ = loss()
+        up = float(osc.src_sig[s, n])
+        setv(np.float32(base) - h); lm, _ = loss()
+        dn = float(osc.src_sig[s, n])
+        setv(np.float32(base))
+        assert abs((lp - lm) / (up - dn) - gs[s, n]) <= 1e-6 * abs(gs[s, n])

@@ -95,6 +95,8 @@ _SIGS = {
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
+    "virs_forward_checkpointed": ([_P, C.c_uint64, C.c_uint32, _P], C.c_int),
+    "virs_adjoint": ([_P, _P, _P, _P], C.c_int),
     "virs_batch_create": ([_P, C.c_uint32, _P], C.c_int),
     "virs_batch_run": ([_P, C.c_uint64, _P], C.c_int),
     "virs_batch_synchronize": ([_P], C.c_int),
@@ -287,6 +289,7 @@ class Simulation:
         i = _c(np.atleast_1d(idx), np.uint64)
         s = _c(signal, np.float32).reshape(i.size, -1)
         check(lib().virs_set_sources(self._h, i.size, _ptr(i), _ptr(s), s.shape[1]))
+        self._nsrc = i.size
 
     def set_receivers(self, idx):
         i = _c(np.atleast_1d(idx), np.uint64)
@@ -358,6 +361,20 @@ class Simulation:
     def check_bounded_wait(self, limit: int = 1000) -> int:
         """Status of the bounded-wait self test (VIRS_E_TIMEOUT expected)."""
         return int(lib().virs_check_bounded_wait(self._h, limit))
+
+    def forward_checkpointed(self, steps: int, every: int = 64, stream: int | None = None):
+        check(lib().virs_forward_checkpointed(self._h, steps, every, stream))
+        self._adj_steps = steps
+
+    def adjoint(self, dl_dir, n_materials: int, n_sections: int):
+        """(dL/dcoef [M][S][5] float64, dL/dsignal [n_src][steps] float32)."""
+        steps = self._adj_steps
+        dl = _c(dl_dir, np.float32).reshape(-1, steps)
+        gc = np.zeros((n_materials, n_sections, 5), np.float64)
+        nsrc = getattr(self, "_nsrc", 0)
+        gs = np.zeros((max(nsrc, 1), steps), np.float32)
+        check(lib().virs_adjoint(self._h, _ptr(dl), _ptr(gc), _ptr(gs)))
+        return gc, gs[:nsrc]
 
     def autotune(self, trial_steps: int = 10) -> Tiling:
         t = Tiling()

@@ -120,7 +120,8 @@ struct virs_sim {
     // kernel variant: depth 0 = register-streaming kernel, 1..3 = TMA
     // kernel with that many planes in flight
     int tile_rows = 8, zc = 0, depth = 2;
-    CUtensorMap tmP[2], tmQ[2], tmC;
+    CUtensorMap tmP[2], tmQ[2], tmC, tmB;
+    DevBuf side;                   // {free, p, p^{n-1}} per boundary slot (TMA kernel -> boundary pass)
     int maps_rows = 0;             // tile rows the maps were built for (0 = none)
     DevBuf err;                    // device error flag of bounded waits
 
@@ -140,6 +141,16 @@ struct virs_sim {
     float rms_state = 0.f;
 
     DevBuf energy_partial;
+
+    // adjoint: checkpoints of a forward run and the reverse-pass buffers
+    struct {
+        uint64_t steps = 0, nck = 0, gen = 0;
+        uint32_t every = 0;
+        bool ready = false;
+        DevBuf ckp, ckq, cks, segrec, segst, buf[2], ast, dbar, cq, grad, dl, gsig;
+        CUtensorMap mapP[2], mapQ[2];
+    } adj;
+    bool fields_valid = true;      // false after virs_adjoint until the next start
 
     ~virs_sim()
     {
@@ -272,7 +283,9 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->ny = (uint32_t)ny;
     s->nz = (uint32_t)nz;
     s->px = (uint32_t)((nx + 31) / 32 * 32);
-    s->spr = (s->px + SEG - 1) / SEG;
+    // segments per row, padded to a multiple of 4 so that rows of the prefix
+    // array are 16-byte aligned for the TMA
+    s->spr = ((s->px + SEG - 1) / SEG + 3) / 4 * 4;
     s->nvox = (size_t)s->px * ny * nz;
     s->nref = n;
     s->h = h;
@@ -280,7 +293,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bmat, &s->bw, &s->state})
+                      &s->field[1], &s->bidx, &s->bmat, &s->bw, &s->state, &s->side})
         b->release();
     VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
     VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
@@ -354,19 +367,32 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-virs_status encode(CUtensorMap *m, CUtensorMapDataType dt, size_t elem, void *base, const virs_sim *s, uint32_t bx,
-                   uint32_t by)
+virs_status encode_dims(CUtensorMap *m, CUtensorMapDataType dt, size_t elem, void *base, uint64_t d0, uint64_t d1,
+                        uint64_t d2, uint32_t bx, uint32_t by)
 {
     auto fn = encode_fn();
     if (!fn) return fail(VIRS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    const cuuint64_t dims[3] = {s->px, s->ny, s->nz};
-    const cuuint64_t strides[2] = {(cuuint64_t)s->px * elem, (cuuint64_t)s->px * s->ny * elem};
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {(cuuint64_t)d0 * elem, (cuuint64_t)d0 * d1 * elem};
     const cuuint32_t box[3] = {bx, by, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(VIRS_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return VIRS_OK;
+}
+
+// a [nz][ny][px] array of the grid
+virs_status encode(CUtensorMap *m, CUtensorMapDataType dt, size_t elem, void *base, const virs_sim *s, uint32_t bx,
+                   uint32_t by)
+{
+    return encode_dims(m, dt, elem, base, s->px, s->ny, s->nz, bx, by);
+}
+
+// the boundary prefix, [nz][ny][spr] (spr is a multiple of 4)
+virs_status encode_prefix(CUtensorMap *m, const virs_sim *s, uint32_t rows)
+{
+    return encode_dims(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, s->bseg.ptr, s->spr, s->ny, s->nz, 4, rows);
 }
 
 // tensor maps of the two field buffers (halo box and tile box) and of the
@@ -383,6 +409,7 @@ virs_status build_maps(virs_sim *s)
         VIRS_TRY(encode(&s->tmQ[b], dt, el, s->field[b].ptr, s, (uint32_t)tma_tile_x(), rows));
     }
     VIRS_TRY(encode(&s->tmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), rows));
+    VIRS_TRY(encode_prefix(&s->tmB, s, rows));
     if (!s->err.ptr) VIRS_TRY(s->err.alloc(sizeof(int), "error flag"));
     s->maps_rows = rows;
     return VIRS_OK;
@@ -418,6 +445,7 @@ virs_status ready_to_run(virs_sim *s)
 StepArgs step_args(const virs_sim *s, int parity)
 {
     StepArgs a{};
+    a.side = s->side.as<float4>();
     a.p = s->field[parity].ptr;
     a.q = s->field[parity ^ 1].ptr;
     a.code = s->code.as<uint8_t>();
@@ -467,7 +495,7 @@ PostArgs post_args(const virs_sim *s, int parity)
 cudaError_t launch_stencil(const virs_sim *s, int parity, cudaStream_t st)
 {
     if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
-    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
+    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC, &s->tmB};
     return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, step_args(s, parity), m, s->err.as<int>(), st);
 }
 
@@ -475,7 +503,7 @@ cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
 {
     cudaError_t e = launch_stencil(s, parity, st);
     if (e != cudaSuccess) return e;
-    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), st);
+    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), s->depth > 0, st);
     if (e != cudaSuccess) return e;
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
@@ -504,6 +532,7 @@ virs_status build_graphs(virs_sim *s, cudaStream_t st)
 
 virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
 {
+    if (!s->fields_valid) return fail(VIRS_E_STATE, "the fields were consumed by virs_adjoint: start the simulation again");
     VIRS_TRY(ready_to_run(s));
     VIRS_TRY(ensure_ir(s, s->steps_done + n));
     if (s->timing) {
@@ -517,7 +546,8 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
             cudaEventRecord(ev[2 * i], st);
             err = launch_stencil(s, par, st);
             cudaEventRecord(ev[2 * i + 1], st);
-            if (err == cudaSuccess) err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), st);
+            if (err == cudaSuccess)
+                err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), s->depth > 0, st);
             cudaEventRecord(ev[2 * n + i], st);
             if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
         }
@@ -759,6 +789,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(s->bidx.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary indices"));
         VIRS_TRY(s->bmat.alloc(std::max<uint64_t>(nb, 1), "boundary materials"));
         VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
+        VIRS_TRY(s->side.alloc(std::max<uint64_t>(nb, 1) * sizeof(float4), "boundary records"));
         CompactArgs cp{};
         cp.flags = s->flags.as<uint8_t>();
         cp.bseg = s->bseg.as<uint32_t>();
@@ -984,6 +1015,7 @@ VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
     s->steps_done = 0;
     s->out0.clear();
     s->rms_state = 0.f;
+    s->fields_valid = true;
     s->drop_graphs();
     VIRS_CUDA(cudaDeviceSynchronize());
     VIRS_CUDA(cudaEventRecord(s->done, s->stream));
@@ -1397,6 +1429,7 @@ struct virs_batch {
     std::vector<uint64_t> gen;
     int dev = 0, storage = 0, rows = 8, depth = 2, planes = 0;
     uint64_t ntiles = 0, nbnd = 0;
+    uint32_t max_sections = 0;
     DevBuf desc, err;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -1439,6 +1472,7 @@ virs_status batch_build(virs_batch *b)
     b->drop_graphs();
     std::vector<BatchMember> h(b->mem.size());
     uint64_t tiles = 0, bnd = 0;
+    b->max_sections = 0;
     const CUtensorMapDataType dt = b->storage == VIRS_STORAGE_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                    : b->storage == VIRS_STORAGE_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                                     : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
@@ -1453,6 +1487,7 @@ virs_status batch_build(virs_batch *b)
             VIRS_TRY(encode(&m.mapQ[k], dt, el, s->field[k].ptr, s, (uint32_t)tma_tile_x(), b->rows));
         }
         VIRS_TRY(encode(&m.mapC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), b->rows));
+        VIRS_TRY(encode_prefix(&m.mapB, s, b->rows));
         const int zc = b->planes > 0 ? b->planes : (s->zc > 0 ? s->zc : default_planes(s->nz));
         for (int par = 0; par < 2; ++par) {
             m.step[par] = step_args(s, par);
@@ -1467,6 +1502,7 @@ virs_status batch_build(virs_batch *b)
         m.first_bnd = bnd;
         tiles += (uint64_t)m.gx * m.gy * m.gz;
         bnd += s->nb;
+        b->max_sections = std::max(b->max_sections, s->nsec);
         b->gen[i] = s->gen;
     }
     VIRS_TRY(b->desc.alloc(h.size() * sizeof(BatchMember), "batch descriptors"));
@@ -1482,7 +1518,7 @@ cudaError_t batch_enqueue(const virs_batch *b, int parity, cudaStream_t st)
     const uint32_t n = (uint32_t)b->mem.size();
     cudaError_t e = launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->err.as<int>(), st);
     if (e != cudaSuccess) return e;
-    e = launch_boundary_batch(b->storage, d, n, b->nbnd, parity, st);
+    e = launch_boundary_batch(b->storage, d, n, b->nbnd, parity, b->max_sections, st);
     if (e != cudaSuccess) return e;
     return launch_post_batch(b->storage, d, n, parity, st);
 }
@@ -1669,5 +1705,129 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
     VIRS_TRY(batch_build(b));
     VIRS_TRY(virs_batch_synchronize(b));
     if (best) *best = pick;
+    return VIRS_OK;
+}
+
+// ============================================================================
+// adjoint
+// ============================================================================
+
+VIRS_EXPORT virs_status virs_forward_checkpointed(virs_sim *s, uint64_t steps, uint32_t every, void *stream)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_forward_checkpointed: null");
+    if (steps == 0 || every == 0 || every > 4096) return fail(VIRS_E_ARG, "need steps > 0 and 1 <= every <= 4096");
+    if (s->prm.storage != VIRS_STORAGE_F32) return fail(VIRS_E_ARG, "the adjoint runs with FP32 storage");
+    if (s->depth == 0) return fail(VIRS_E_STATE, "the adjoint needs the TMA kernel (pipeline depth 1..3)");
+    VIRS_TRY(virs_start_simulation(s, steps));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    auto &A = s->adj;
+    A.ready = false;
+    A.steps = steps;
+    A.every = every;
+    A.nck = (steps + every - 1) / every;
+    const size_t fb = s->nvox * 4, sb = std::max<uint64_t>(s->nb, 1) * s->nsec * 4 * 4;
+    VIRS_TRY(A.ckp.alloc(A.nck * fb, "checkpoints"));
+    VIRS_TRY(A.ckq.alloc(A.nck * fb, "checkpoints"));
+    VIRS_TRY(A.cks.alloc(A.nck * sb, "checkpoints"));
+    VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+    VIRS_CUDA(cudaStreamWaitEvent(st, s->done, 0));
+    for (uint64_t c = 0; c < A.nck; ++c) {
+        VIRS_CUDA(cudaMemcpyAsync(A.ckp.as<char>() + c * fb, s->field[s->cur].ptr, fb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(A.ckq.as<char>() + c * fb, s->field[s->cur ^ 1].ptr, fb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(A.cks.as<char>() + c * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
+        VIRS_TRY(run_steps(s, std::min<uint64_t>(every, steps - c * every), st));
+    }
+    A.gen = s->gen;
+    A.ready = true;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *grad_coef, float *grad_signal)
+{
+    if (!s || !dl_dir) return fail(VIRS_E_ARG, "virs_adjoint: null argument");
+    auto &A = s->adj;
+    if (!A.ready || A.gen != s->gen || s->steps_done != A.steps || !s->fields_valid)
+        return fail(VIRS_E_STATE, "call virs_forward_checkpointed first (and change nothing in between)");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    cudaStream_t st = s->stream;
+    const uint64_t steps = A.steps, every = A.every, nb = s->nb;
+    const size_t fb = s->nvox * 4, sb = std::max<uint64_t>(nb, 1) * s->nsec * 4 * 4;
+    const uint32_t ncoef = s->nmat * s->nsec * 5;
+    VIRS_TRY(A.segrec.alloc(every * std::max<uint64_t>(nb, 1) * sizeof(float4), "adjoint segment records"));
+    VIRS_TRY(A.segst.alloc(every * sb, "adjoint segment states"));
+    for (int k = 0; k < 2; ++k) VIRS_TRY(A.buf[k].alloc(fb, "adjoint field"));
+    VIRS_TRY(A.ast.alloc(sb, "adjoint filter states"));
+    VIRS_TRY(A.dbar.alloc(std::max<uint64_t>(nb, 1) * 4, "adjoint boundary terms"));
+    VIRS_TRY(A.cq.alloc(std::max<uint64_t>(nb, 1) * 4, "adjoint boundary terms"));
+    VIRS_TRY(A.grad.alloc(ncoef * sizeof(double), "coefficient gradients"));
+    VIRS_TRY(A.dl.alloc(std::max<uint32_t>(s->nrcv, 1) * steps * 4, "loss gradient"));
+    VIRS_TRY(A.gsig.alloc(std::max<uint32_t>(s->nsrc, 1) * steps * 4, "signal gradients"));
+    if (s->nrcv) VIRS_CUDA(cudaMemcpy(A.dl.ptr, dl_dir, (size_t)s->nrcv * steps * 4, cudaMemcpyHostToDevice));
+    const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    for (int k = 0; k < 2; ++k) {
+        VIRS_TRY(encode(&A.mapP[k], dt, 4, A.buf[k].ptr, s, (uint32_t)tma_box_width(VIRS_STORAGE_F32), s->tile_rows + 2));
+        VIRS_TRY(encode(&A.mapQ[k], dt, 4, A.buf[k].ptr, s, (uint32_t)tma_tile_x(), s->tile_rows));
+    }
+    VIRS_TRY(ready_to_run(s));
+    int t = 0; // A.buf[t] holds T, A.buf[t ^ 1] holds RR
+    for (int64_t c = (int64_t)A.nck - 1; c >= 0; --c) {
+        const uint64_t n0 = (uint64_t)c * every, n1 = std::min<uint64_t>(n0 + every, steps);
+        // rebuild the segment: restore the checkpoint and run forward, keeping
+        // the states before every step and the stencil's boundary records
+        s->cur = 0;
+        VIRS_CUDA(cudaMemcpyAsync(s->field[0].ptr, A.ckp.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(s->field[1].ptr, A.ckq.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(s->state.ptr, A.cks.as<char>() + c * sb, sb, cudaMemcpyDeviceToDevice, st));
+        const uint32_t c0 = (uint32_t)n0;
+        VIRS_CUDA(cudaMemcpyAsync(s->ctr.ptr, &c0, 4, cudaMemcpyHostToDevice, st));
+        VIRS_CUDA(cudaStreamSynchronize(st));
+        for (uint64_t n = n0; n < n1; ++n) {
+            const uint64_t k = n - n0;
+            VIRS_CUDA(cudaMemcpyAsync(A.segst.as<char>() + k * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
+            cudaError_t e = launch_stencil(s, s->cur, st);
+            if (e == cudaSuccess) e = launch_keep_records(s->side.as<float4>(), A.segrec.as<float4>() + k * nb, nb, st);
+            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), s->bidx.as<uint32_t>(), true, st);
+            if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, s->cur), st);
+            if (e != cudaSuccess) return cuda_fail(e, "adjoint recomputation");
+            s->cur ^= 1;
+        }
+        // reverse steps of the segment
+        for (int64_t n = (int64_t)n1 - 1; n >= (int64_t)n0; --n) {
+            const uint64_t k = (uint64_t)n - n0;
+            float *T = A.buf[t].as<float>(), *RR = A.buf[t ^ 1].as<float>();
+            cudaError_t e = launch_adj_inject(T, s->code.as<uint8_t>(), s->rcv.as<uint64_t>(), s->nrcv, A.dl.as<float>(),
+                                              steps, (uint64_t)n, s->src.as<uint64_t>(), s->nsrc, A.gsig.as<float>(),
+                                              steps, st);
+            if (e == cudaSuccess)
+                e = launch_adj_boundary(T, s->bidx.as<uint32_t>(), s->bmat.as<uint8_t>(), s->bw.as<float>(),
+                                        s->coef.as<float>(), A.segrec.as<float4>() + k * nb,
+                                        reinterpret_cast<const float *>(A.segst.as<char>() + k * sb), A.ast.as<float>(),
+                                        A.dbar.as<float>(), A.cq.as<float>(), A.grad.as<double>(), nb, s->nx, s->ny,
+                                        s->px, s->nsec, s->nmat, s->prm.boundary_form, (double)s->K,
+                                        s->prm.mix_filtered, s->prm.mix_direct, (double)s->prm.boundary_gain, st);
+            if (e == cudaSuccess) {
+                StepArgs a = step_args(s, 0);
+                a.p = T;
+                a.q = RR;
+                a.nhard = 0;
+                const TmaMaps m{&A.mapP[t], &A.mapQ[t ^ 1], &s->tmC, &s->tmB};
+                e = launch_step_tma(VIRS_STORAGE_F32, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
+            }
+            if (e == cudaSuccess)
+                e = launch_adj_fix(RR, T, s->bidx.as<uint32_t>(), s->side.as<float4>(), A.dbar.as<float>(),
+                                   A.cq.as<float>(), nb, s->nx, s->ny, s->px, st);
+            if (e != cudaSuccess) return cuda_fail(e, "adjoint step");
+            t ^= 1;
+        }
+    }
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    VIRS_TRY(check_err(s));
+    if (grad_coef) VIRS_CUDA(cudaMemcpy(grad_coef, A.grad.ptr, ncoef * sizeof(double), cudaMemcpyDeviceToHost));
+    if (grad_signal && s->nsrc)
+        VIRS_CUDA(cudaMemcpy(grad_signal, A.gsig.ptr, (size_t)s->nsrc * steps * 4, cudaMemcpyDeviceToHost));
+    // the fields now hold an intermediate forward state
+    s->fields_valid = false;
+    VIRS_CUDA(cudaEventRecord(s->done, st));
     return VIRS_OK;
 }

@@ -68,6 +68,7 @@ constexpr int SEG = 128;              // voxels per boundary-prefix segment
 // ---- kernel argument blocks -------------------------------------------------
 
 struct StepArgs {
+    float4 *side;           // per boundary slot {free, p, p^{n-1}, 0}, written by the TMA stencil kernel
     const void *p;          // p^n (storage type)
     void *q;                // in p^{n-1}, out p^{n+1}
     const uint8_t *code;
@@ -105,6 +106,7 @@ struct alignas(64) BatchMember {
     CUtensorMap mapP[2];    // halo box over field[0] / field[1]
     CUtensorMap mapQ[2];    // tile box over field[0] / field[1]
     CUtensorMap mapC;       // cell codes
+    CUtensorMap mapB;       // boundary prefix
     StepArgs step[2];       // per parity: p = field[parity], q = field[parity ^ 1]
     PostArgs post[2];
     const uint32_t *bidx;
@@ -115,13 +117,15 @@ struct alignas(64) BatchMember {
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
                                   uint64_t ntiles, int parity, int *err, cudaStream_t s);
 cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
-                                  cudaStream_t s);
+                                  uint32_t max_sections, cudaStream_t s);
 cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem, int parity, cudaStream_t s);
 
 // kernel launchers (kernels_step.cu)
 cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, cudaStream_t s);
+// side == true: finish the records the TMA stencil kernel wrote; false:
+// gather the neighbours and do the whole update (after the register kernel)
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, bool side, cudaStream_t s);
 int default_planes(uint32_t nz);
 
 // TMA-staged step (kernels_step_tma.cu)
@@ -129,6 +133,7 @@ struct TmaMaps {
     const CUtensorMap *p;   // p^n with halo box
     const CUtensorMap *q;   // p^{n-1}, tile box
     const CUtensorMap *c;   // cell codes, tile box
+    const CUtensorMap *b;   // boundary prefix, 4 segments x tile rows
 };
 cudaError_t launch_step_tma(int storage, int tile_rows, int depth, const StepArgs &a, const TmaMaps &m, int *err,
                             cudaStream_t s);
@@ -174,6 +179,18 @@ struct CompactArgs {
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);
+
+// adjoint kernels (kernels_adjoint.cu)
+cudaError_t launch_adj_inject(float *T, const uint8_t *code, const uint64_t *rcv, uint32_t nrcv, const float *dl,
+                              uint64_t dl_stride, uint64_t n, const uint64_t *src, uint32_t nsrc, float *gsig,
+                              uint64_t gs_stride, cudaStream_t s);
+cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *bmat, const float *bw, const float *coef,
+                                const float4 *rec, const float *fst, float *ast, float *dbar, float *cq, double *grad,
+                                uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, uint32_t nsec, uint32_t nmat,
+                                int form, double K, double mix_y, double mix_d, double gain, cudaStream_t s);
+cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const float4 *rec, const float *dbar,
+                           const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s);
+cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s);
 
 // misc kernels (kernels_misc.cu)
 cudaError_t launch_energy(int storage, const void *p, const void *q, const uint8_t *code, uint32_t nx, uint32_t ny,

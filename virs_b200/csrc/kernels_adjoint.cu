@@ -1,0 +1,197 @@
+// Reverse-mode (adjoint) kernels: gradients of a receiver loss with respect
+// to the boundary filter coefficients and the source signals.
+//
+// One forward step maps (p, q, S) -> (p+, p, S+), linear in the fields and
+// the filter states.  With T the adjoint of p^{n+1} and RR the negated
+// adjoint carried by p^n through its role as q of the next step, one
+// reverse step n is
+//   k_adj_inject     T[rcv] += dL/dIR_n ; dL/dsig_n = T[src]
+//   k_adj_boundary   at boundary voxels the correction and the biquad cascade
+//                    run transposed: F = T (reference form) or T/(1+a)
+//                    (centered form), the cascade's state adjoints and the
+//                    coefficient gradients (FP64), dbar = d(loss)/d(p - q)
+//   stencil          T' = A F - RR into RR's buffer: the forward stencil
+//                    kernel itself, since A (2 + lambda^2 * Laplacian with
+//                    mirrored walls and zero fixed voxels) is symmetric on
+//                    the updated voxels; hard-source voxels are given 0
+//   k_adj_fix        boundary voxels: T'_b = A F_b - RR_b + dbar_b (from the
+//                    stencil's record) and RR'_b = F_b + dbar_b - cq_b
+// and the buffers swap.  The forward values the cascade needs (p - q and
+// the states before step n) come from a recomputation of the segment from
+// the last checkpoint.
+#include "step_common.cuh"
+
+namespace virs {
+namespace {
+
+using namespace step;
+
+__global__ void k_adj_inject(float *T, const uint8_t *__restrict code, const uint64_t *__restrict rcv, uint32_t nrcv,
+                             const float *__restrict dl, uint64_t dl_stride, uint64_t n, const uint64_t *__restrict src,
+                             uint32_t nsrc, float *__restrict gsig, uint64_t gs_stride)
+{
+    for (uint32_t r = threadIdx.x; r < nrcv; r += blockDim.x) {
+        // receivers read the new field; a receiver on a voxel that is not
+        // updated (wall, hard source, border) reads a constant
+        const uint64_t i = rcv[r];
+        if (code[i] < CODE_HARD) atomicAdd(T + i, dl[(uint64_t)r * dl_stride + n]);
+    }
+    __syncthreads();
+    for (uint32_t s = threadIdx.x; s < nsrc; s += blockDim.x) gsig[(uint64_t)s * gs_stride + n] = T[src[s]];
+}
+
+struct AdjArgs {
+    float *T;                  // adjoint field (p role)
+    const uint32_t *bidx;
+    const uint8_t *bmat;
+    const float *bw;
+    const float *coef;         // [M][S][5]
+    const float4 *rec;         // forward records of this step {free, p, q, 0}
+    const float *fst;          // forward states before this step [S][4][nb]
+    float *ast;                // state adjoints [S][4][nb]
+    float *dbar, *cq;          // per slot
+    double *grad;              // [M][S][5]
+    uint64_t nb;
+    uint32_t nx, ny, px, nsec, ncoef;
+    int form;
+    double K, mix_y, mix_d, gain;
+};
+
+constexpr int AB = 256;
+
+__global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
+{
+    extern __shared__ double gsm[]; // block partial sums of the coefficient gradients
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB) gsm[k] = 0.0;
+    __syncthreads();
+    const uint64_t b = (uint64_t)blockIdx.x * AB + threadIdx.x;
+    if (b < a.nb) {
+        const uint32_t ref = a.bidx[b];
+        const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
+        const size_t i = ((size_t)z * a.ny + y) * a.px + x;
+        const float f = a.T[i];
+        const double w = (double)a.bw[b];
+        const double kgw = a.K * a.gain * w;
+        double fr, ybar, db = 0.0, cqv = 0.0;
+        if (a.form == VIRS_BOUNDARY_REFERENCE) {
+            fr = f;
+            ybar = -kgw * a.mix_y * f;
+            db = -kgw * a.mix_d * f;
+        } else {
+            const double ac = kgw * a.mix_d * 0.5;
+            fr = f / (1.0 + ac);
+            ybar = -kgw * a.mix_y * fr;
+            cqv = ac * fr;
+        }
+        // forward inputs of every section at this step
+        const uint32_t S = a.nsec, m = a.bmat[b];
+        const float *kc = a.coef + (uint64_t)m * S * 5;
+        const float4 rec = a.rec[b];
+        float xin[16];
+        float in = __fsub_rn(rec.y, rec.z);
+        for (uint32_t q = 0; q < S; ++q) {
+            const float *kq = kc + 5 * q;
+            const float s0 = a.fst[(uint64_t)(4 * q + 0) * a.nb + b], s1 = a.fst[(uint64_t)(4 * q + 1) * a.nb + b];
+            const float s2 = a.fst[(uint64_t)(4 * q + 2) * a.nb + b], s3 = a.fst[(uint64_t)(4 * q + 3) * a.nb + b];
+            xin[q] = in;
+            float yv = __fmaf_rn(kq[0], in, __fmul_rn(kq[1], s0));
+            yv = __fmaf_rn(kq[2], s1, yv);
+            yv = __fmaf_rn(-kq[3], s2, yv);
+            in = __fmaf_rn(-kq[4], s3, yv);
+        }
+        double yb = ybar;
+        for (int q = (int)S - 1; q >= 0; --q) {
+            const float *kq = kc + 5 * q;
+            float *aq = a.ast + b;
+            const uint64_t o0 = (uint64_t)(4 * q + 0) * a.nb, o1 = (uint64_t)(4 * q + 1) * a.nb;
+            const uint64_t o2 = (uint64_t)(4 * q + 2) * a.nb, o3 = (uint64_t)(4 * q + 3) * a.nb;
+            const double yt = yb + (double)aq[o2];
+            const double s0 = a.fst[o0 + b], s1 = a.fst[o1 + b], s2 = a.fst[o2 + b], s3 = a.fst[o3 + b];
+            double *g = gsm + (uint64_t)(m * S + q) * 5;
+            atomicAdd(g + 0, yt * (double)xin[q]);
+            atomicAdd(g + 1, yt * s0);
+            atomicAdd(g + 2, yt * s1);
+            atomicAdd(g + 3, -yt * s2);
+            atomicAdd(g + 4, -yt * s3);
+            const double xbar = (double)kq[0] * yt + (double)aq[o0];
+            const double x1 = (double)kq[1] * yt + (double)aq[o1];
+            const double x2 = (double)kq[2] * yt;
+            const double y1 = -(double)kq[3] * yt + (double)aq[o3];
+            const double y2 = -(double)kq[4] * yt;
+            aq[o0] = (float)x1;
+            aq[o1] = (float)x2;
+            aq[o2] = (float)y1;
+            aq[o3] = (float)y2;
+            yb = xbar;
+        }
+        db += yb;
+        a.T[i] = (float)fr;
+        a.dbar[b] = (float)db;
+        a.cq[b] = (float)cqv;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB)
+        if (gsm[k] != 0.0) atomicAdd(a.grad + k, gsm[k]);
+}
+
+// boundary voxels after the stencil: T' (in RR's buffer) and the next RR
+// (in T's buffer)
+__global__ void k_adj_fix(float *Tn, float *Tb, const uint32_t *__restrict bidx, const float4 *__restrict rec,
+                          const float *__restrict dbar, const float *__restrict cq, uint64_t nb, uint32_t nx,
+                          uint32_t ny, uint32_t px)
+{
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const uint32_t ref = bidx[b];
+    const uint32_t x = ref % nx, t = ref / nx, y = t % ny, z = t / ny;
+    const size_t i = ((size_t)z * ny + y) * px + x;
+    Tn[i] = rec[b].x + dbar[b];
+    Tb[i] = Tb[i] + dbar[b] - cq[b];
+}
+
+// the boundary data the reverse pass needs from one forward step
+__global__ void k_keep_records(const float4 *__restrict side, float4 *__restrict out, uint64_t nb)
+{
+    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb) out[b] = side[b];
+}
+
+} // namespace
+
+cudaError_t launch_adj_inject(float *T, const uint8_t *code, const uint64_t *rcv, uint32_t nrcv, const float *dl,
+                              uint64_t dl_stride, uint64_t n, const uint64_t *src, uint32_t nsrc, float *gsig,
+                              uint64_t gs_stride, cudaStream_t s)
+{
+    k_adj_inject<<<1, 256, 0, s>>>(T, code, rcv, nrcv, dl, dl_stride, n, src, nsrc, gsig, gs_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *bmat, const float *bw, const float *coef,
+                                const float4 *rec, const float *fst, float *ast, float *dbar, float *cq, double *grad,
+                                uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, uint32_t nsec, uint32_t nmat,
+                                int form, double K, double mix_y, double mix_d, double gain, cudaStream_t s)
+{
+    if (nb == 0) return cudaSuccess;
+    AdjArgs a{T, bidx, bmat, bw, coef, rec, fst, ast, dbar, cq, grad, nb, nx, ny, px, nsec, nmat * nsec * 5, form,
+              K, mix_y, mix_d, gain};
+    const size_t sm = (size_t)a.ncoef * sizeof(double);
+    k_adj_boundary<<<(unsigned)((nb + AB - 1) / AB), AB, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const float4 *rec, const float *dbar,
+                           const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s)
+{
+    if (nb == 0) return cudaSuccess;
+    k_adj_fix<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(Tn, Tb, bidx, rec, dbar, cq, nb, nx, ny, px);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s)
+{
+    if (nb == 0) return cudaSuccess;
+    k_keep_records<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(side, out, nb);
+    return cudaGetLastError();
+}
+
+} // namespace virs

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
 // The compacted boundary pass (simulator_gpu.cu:105-150): one thread per
 // boundary voxel in list order; the leapfrog update (the stencil kernel
 // left these voxels untouched) and the filter correction.
-template <typename T>
+template <typename T, int MAXS>
 __device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
 {
     using IO = Io<T>;
@@ -176,20 +176,34 @@ __device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t
     const float ce = IO::get(P[i]), qv = IO::get(Q[i]);
     float r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
                        IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
-    r = boundary(a, r, ce, qv, slot);
+    r = boundary<MAXS>(a, r, ce, qv, slot);
     Q[i] = IO::put(r);
 }
 
-template <typename T> __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a,
-                                                                        const uint32_t *__restrict bidx)
+// finishes the record the TMA stencil kernel left for this slot
+template <typename T, int MAXS>
+__device__ __forceinline__ void boundary_record(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
+{
+    const float4 rec = __ldcs(a.side + slot);
+    const uint32_t ref = __ldg(bidx + slot);
+    const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
+    const size_t i = ((size_t)z * a.ny + y) * a.px + x;
+    T *Q = static_cast<T *>(a.q);
+    Q[i] = Io<T>::put(boundary<MAXS>(a, rec.x, rec.y, rec.z, slot));
+}
+
+template <typename T, bool SIDE, int MAXS>
+__global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a, const uint32_t *__restrict bidx)
 {
     const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot < a.nb) boundary_voxel<T>(a, bidx, slot);
+    if (slot >= a.nb) return;
+    if (SIDE) boundary_record<T, MAXS>(a, bidx, slot);
+    else boundary_voxel<T, MAXS>(a, bidx, slot);
 }
 
 // batched: thread g belongs to the last member whose first boundary index
 // is <= g (members without boundary voxels are skipped by that rule)
-template <typename T>
+template <typename T, int MAXS>
 __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__restrict mem, uint32_t nmem,
                                                         uint64_t ntotal, int parity)
 {
@@ -202,7 +216,7 @@ __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__res
         else hi = mid - 1;
     }
     const BatchMember &b = mem[lo];
-    boundary_voxel<T>(b.step[parity], b.bidx, g - b.first_bnd);
+    boundary_record<T, MAXS>(b.step[parity], b.bidx, g - b.first_bnd);
 }
 
 // Additive sources, then receivers, then the step counter
@@ -267,27 +281,59 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
     }
 }
 
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, cudaStream_t s)
+namespace {
+
+template <typename T, bool SIDE>
+void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, const uint32_t *bidx, cudaStream_t s)
+{
+    if (ns <= 1) k_boundary<T, SIDE, 1><<<g, 256, 0, s>>>(a, bidx);
+    else if (ns == 2) k_boundary<T, SIDE, 2><<<g, 256, 0, s>>>(a, bidx);
+    else if (ns <= 4) k_boundary<T, SIDE, 4><<<g, 256, 0, s>>>(a, bidx);
+    else k_boundary<T, SIDE, 0><<<g, 256, 0, s>>>(a, bidx);
+}
+
+template <typename T>
+void boundary_batch_by_sections(uint32_t maxs, unsigned g, const BatchMember *mem, uint32_t nmem, uint64_t nbnd,
+                                int parity, cudaStream_t s)
+{
+    if (maxs <= 4) k_boundary_batch<T, 4><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity);
+    else k_boundary_batch<T, 0><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity);
+}
+
+} // namespace
+
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, bool side, cudaStream_t s)
 {
     if (a.nb == 0) return cudaSuccess;
     const unsigned g = (unsigned)((a.nb + 255) / 256);
     switch (storage) {
-    case VIRS_STORAGE_F16: k_boundary<__half><<<g, 256, 0, s>>>(a, bidx); break;
-    case VIRS_STORAGE_BF16: k_boundary<__nv_bfloat16><<<g, 256, 0, s>>>(a, bidx); break;
-    default: k_boundary<float><<<g, 256, 0, s>>>(a, bidx); break;
+    case VIRS_STORAGE_F16:
+        if (side) boundary_by_sections<__half, true>(a.nsec, g, a, bidx, s);
+        else boundary_by_sections<__half, false>(a.nsec, g, a, bidx, s);
+        break;
+    case VIRS_STORAGE_BF16:
+        if (side) boundary_by_sections<__nv_bfloat16, true>(a.nsec, g, a, bidx, s);
+        else boundary_by_sections<__nv_bfloat16, false>(a.nsec, g, a, bidx, s);
+        break;
+    default:
+        if (side) boundary_by_sections<float, true>(a.nsec, g, a, bidx, s);
+        else boundary_by_sections<float, false>(a.nsec, g, a, bidx, s);
+        break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
-                                  cudaStream_t s)
+                                  uint32_t max_sections, cudaStream_t s)
 {
     if (nbnd == 0) return cudaSuccess;
     const unsigned g = (unsigned)((nbnd + 255) / 256);
     switch (storage) {
-    case VIRS_STORAGE_F16: k_boundary_batch<__half><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
-    case VIRS_STORAGE_BF16: k_boundary_batch<__nv_bfloat16><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
-    default: k_boundary_batch<float><<<g, 256, 0, s>>>(mem, nmem, nbnd, parity); break;
+    case VIRS_STORAGE_F16: boundary_batch_by_sections<__half>(max_sections, g, mem, nmem, nbnd, parity, s); break;
+    case VIRS_STORAGE_BF16:
+        boundary_batch_by_sections<__nv_bfloat16>(max_sections, g, mem, nmem, nbnd, parity, s);
+        break;
+    default: boundary_batch_by_sections<float>(max_sections, g, mem, nmem, nbnd, parity, s); break;
     }
     return cudaGetLastError();
 }

@@ -18,9 +18,12 @@
 // streaming 16-byte stores.  No multicast: every copy reads this GPU's own
 // memory into this block's shared memory.
 //
-// Boundary voxels (flag 2) are left unchanged here -- their p^{n-1} stays in
-// place -- and are updated afterwards by the compacted boundary pass
-// (k_boundary), so this kernel has no divergent filter work.
+// Boundary voxels (flag 2): their leapfrog value is computed here with the
+// staged neighbours and written, with p and p^{n-1}, to the voxel's slot of
+// the compacted boundary list; p^{n-1} stays in place.  The boundary pass
+// (k_boundary) then applies the filters to those records, coalesced, so the
+// only divergent work here is one warp scan and one 16-byte store per
+// boundary voxel.
 //
 // Every wait on an mbarrier is bounded; a wait that gives up sets *err and
 // the block returns (the host turns that into VIRS_E_TIMEOUT).
@@ -79,10 +82,12 @@ template <typename T, int TY> struct Stage {
     static constexpr uint32_t PB = Geo<T>::PW * (TY + 2) * sizeof(T);
     static constexpr uint32_t QB = TX * TY * sizeof(T);
     static constexpr uint32_t CB = TX * TY;
+    static constexpr uint32_t BB = 4 * TY * sizeof(uint32_t); // 4 prefix segments per tile row
     static constexpr uint32_t PBa = (PB + 127u) & ~127u;
     static constexpr uint32_t QBa = (QB + 127u) & ~127u;
     static constexpr uint32_t CBa = (CB + 127u) & ~127u;
-    static constexpr uint32_t SB = PBa + QBa + CBa;
+    static constexpr uint32_t BBa = (BB + 127u) & ~127u;
+    static constexpr uint32_t SB = PBa + QBa + CBa + BBa;
 };
 
 template <typename T> __device__ __forceinline__ void ld4(const T *p, float (&r)[4]);
@@ -143,8 +148,8 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bars, int j, int D, int *er
 // gave up.
 template <typename T, int TY, int L>
 __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
-                                          const CUtensorMap *mC, int bx, int by, int bz, int *err,
-                                          unsigned char *smem, uint64_t *bars, uint32_t &jg)
+                                          const CUtensorMap *mC, const CUtensorMap *mB, int bx, int by, int bz,
+                                          int *err, unsigned char *smem, uint64_t *bars, uint32_t &jg)
 {
     using S = Stage<T, TY>;
     constexpr int PAD = Geo<T>::PAD, PW = Geo<T>::PW;
@@ -164,6 +169,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     const size_t plane = (size_t)a.px * ny;
     T *Q = static_cast<T *>(a.q);
     const uint32_t j0 = jg;
+    const int seg = x0 / SEG, seg4 = seg & ~3; // prefix box starts on a 16-byte boundary
 
     auto issue = [&](int j) {
         const int k = z0 - 2 + j;
@@ -171,11 +177,12 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
         unsigned char *st = smem + (g % D) * S::SB;
         uint64_t *b = bars + (g % D);
         const bool full = j >= 2;
-        mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB : 0u));
+        mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB + S::BB : 0u));
         tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k + 1);
         if (full) {
             tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
             tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
+            tma_load_3d(st + S::PBa + S::QBa + S::CBa, mB, b, seg4, y0, k);
         }
     };
     if (tid == 0)
@@ -214,6 +221,14 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
         if (lane == 31) right = Io<T>::get(Pc[c0 + 4]);
 
         float r[4];
+        unsigned bmask = 0;
+        if (code4 == 0u) {
+            // four air voxels without wall neighbours: the common case
+            r[0] = leapfrog_air(cc[0], cc[1], left, yp[0], ym[0], zp[0], zm[0], qv[0], a.c2dt2, a.inv_h2);
+            r[1] = leapfrog_air(cc[1], cc[2], cc[0], yp[1], ym[1], zp[1], zm[1], qv[1], a.c2dt2, a.inv_h2);
+            r[2] = leapfrog_air(cc[2], cc[3], cc[1], yp[2], ym[2], zp[2], zm[2], qv[2], a.c2dt2, a.inv_h2);
+            r[3] = leapfrog_air(cc[3], right, cc[2], yp[3], ym[3], zp[3], zm[3], qv[3], a.c2dt2, a.inv_h2);
+        } else
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const uint8_t c = (uint8_t)(code4 >> (8 * k));
@@ -226,10 +241,33 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
                     const uint32_t sn = __ldg(a.ctr);
                     r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
                 }
-            } else if (c & CODE_BND) {
-                r[k] = qv[k]; // updated by the boundary pass, which needs p^{n-1}
             } else {
                 r[k] = leapfrog(c, cc[k], xp, xm, yp[k], ym[k], zp[k], zm[k], qv[k], a.c2dt2, a.inv_h2);
+                if (c & CODE_BND) bmask |= 1u << k;
+            }
+        }
+        // Boundary voxels: the record {free value, p, p^{n-1}} goes to their
+        // slot of the compacted list for the boundary pass, and p^{n-1} stays
+        // in place.  A warp covers consecutive voxels of one row, so the slot
+        // is the row segment's prefix (staged with the plane) plus a warp scan.
+        if (!act) bmask = 0;
+        if (__any_sync(FULL, bmask != 0)) {
+            const int cnt = __popc(bmask);
+            int inc = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (bmask) {
+                const uint32_t *bs = reinterpret_cast<const uint32_t *>(s2 + S::PBa + S::QBa + S::CBa);
+                uint64_t slot = (uint64_t)bs[ty * 4 + (seg - seg4)] + (uint64_t)(inc - cnt);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (bmask & (1u << k)) {
+                        a.side[slot++] = make_float4(r[k], cc[k], qv[k], 0.f);
+                        r[k] = qv[k];
+                    }
             }
         }
         if (act) st4(Q + (size_t)z * plane + (size_t)y * a.px + x, r);
@@ -251,14 +289,15 @@ template <typename T, int TY, int L>
 __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __grid_constant__ StepArgs a,
                                                                         const __grid_constant__ CUtensorMap mP,
                                                                         const __grid_constant__ CUtensorMap mQ,
-                                                                        const __grid_constant__ CUtensorMap mC, int *err)
+                                                                        const __grid_constant__ CUtensorMap mC,
+                                                                        const __grid_constant__ CUtensorMap mB, int *err)
 {
     constexpr int D = L + 3;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
     uint32_t jg = 0;
-    step_tile<T, TY, L>(a, &mP, &mQ, &mC, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
+    step_tile<T, TY, L>(a, &mP, &mQ, &mC, &mB, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
 }
 
 // Many simulations in one launch: a persistent grid walks the concatenated
@@ -281,8 +320,8 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma_batch(co
         const uint64_t local = w - b.first_tile;
         const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / ((uint64_t)b.gx * b.gy));
         __syncthreads(); // every thread is done with the previous tile's stages
-        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, bx, by, bz, err,
-                                 smem, bars, jg))
+        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, &b.mapB, bx, by, bz,
+                                 err, smem, bars, jg))
             return;
     }
 }
@@ -301,7 +340,7 @@ cudaError_t launch3(const StepArgs &a, const TmaMaps &m, int *err, cudaStream_t 
     if (e != cudaSuccess) return e;
     const unsigned gx = (a.px + TX - 1) / TX;
     const unsigned gz = (a.nz - 2 + a.zc - 1) / a.zc;
-    kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, TY), sm, s>>>(a, *m.p, *m.q, *m.c, err);
+    kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, TY), sm, s>>>(a, *m.p, *m.q, *m.c, *m.b, err);
     return cudaGetLastError();
 }
 

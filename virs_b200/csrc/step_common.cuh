@@ -132,12 +132,84 @@ __device__ __forceinline__ float leapfrog(uint8_t c, float ce, float xp, float x
     return __fmaf_rn(c2dt2, lap, t);
 }
 
+// the same update for an air voxel without wall neighbours (code 0): no
+// selects; bit-identical to leapfrog(0, ...)
+__device__ __forceinline__ float leapfrog_air(float ce, float xp, float xm, float yp, float ym, float zp, float zm,
+                                              float qv, float c2dt2, float inv_h2)
+{
+    float s = __fadd_rn(xp, xm);
+    s = __fadd_rn(s, yp);
+    s = __fadd_rn(s, ym);
+    s = __fadd_rn(s, zp);
+    s = __fadd_rn(s, zm);
+    const float lap = __fmul_rn(__fmaf_rn(-6.0f, ce, s), inv_h2);
+    const float t = __fsub_rn(__fmul_rn(2.0f, ce), qv);
+    return __fmaf_rn(c2dt2, lap, t);
+}
+
 // simulator_gpu.cu:126-148: biquad sections in series on d = p - p^{n-1}
 // (b0*in + b1*s0 contracted to fma(b0, in, b1*s0) as the reference build
-// does),
-// then p+ -= K*(0.1*y + 0.9*d)*0.4 (times the sponge weight) in double, or
-// the centered form of the same correction.
-__device__ __noinline__ float boundary(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+// does), then p+ -= K*(0.1*y + 0.9*d)*0.4 (times the sponge weight) in
+// double, or the centered form of the same correction.
+
+// the correction, given the cascade output y (double precision)
+__device__ __forceinline__ float correct(const StepArgs &a, float r, float d, float y, float qv, float wf)
+{
+    const double w = (double)wf;
+    if (a.form == VIRS_BOUNDARY_REFERENCE) {
+        const double t = __fma_rn((double)y, a.mix_y, __dmul_rn((double)d, a.mix_d));
+        const double u = __dmul_rn(__dmul_rn(__dmul_rn(a.K, t), a.gain), w);
+        return __double2float_rn(__dsub_rn((double)r, u));
+    }
+    // centered: the direct damping term at (p+ - p-)/2, solved for p+
+    const double kgw = __dmul_rn(__dmul_rn(a.K, a.gain), w);
+    const double ac = __dmul_rn(__dmul_rn(kgw, a.mix_d), 0.5);
+    const double num = __dadd_rn(__dsub_rn((double)r, __dmul_rn(kgw, __dmul_rn((double)y, a.mix_y))),
+                                 __dmul_rn(ac, (double)qv));
+    return __double2float_rn(__ddiv_rn(num, __dadd_rn(1.0, ac)));
+}
+
+// up to MAXS sections, fully unrolled: every state, the material and the
+// weight are loaded before any arithmetic, so one slot costs two dependent
+// memory round trips (states/material, then coefficients), not one per
+// section
+template <int MAXS>
+__device__ __forceinline__ float boundary_unrolled(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+{
+    const uint32_t ns = a.nsec;
+    const uint64_t nb = a.nb;
+    float *st = a.state + slot;
+    const uint32_t m = __ldg(a.bmat + slot);
+    const float wf = __ldg(a.bw + slot);
+    float s[MAXS][4];
+#pragma unroll
+    for (int q = 0; q < MAXS; ++q)
+        if (q < (int)ns)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) s[q][j] = st[(uint64_t)(4 * q + j) * nb];
+    const float *kc = a.coef + (uint64_t)m * ns * 5;
+    const float d = __fsub_rn(ce, qv);
+    float in = d;
+#pragma unroll
+    for (int q = 0; q < MAXS; ++q) {
+        if (q < (int)ns) {
+            const float *kq = kc + 5 * q;
+            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), s[q][0]));
+            y = __fmaf_rn(__ldg(kq + 2), s[q][1], y);
+            y = __fmaf_rn(-__ldg(kq + 3), s[q][2], y);
+            y = __fmaf_rn(-__ldg(kq + 4), s[q][3], y);
+            st[(uint64_t)(4 * q + 0) * nb] = in;
+            st[(uint64_t)(4 * q + 1) * nb] = s[q][0];
+            st[(uint64_t)(4 * q + 2) * nb] = y;
+            st[(uint64_t)(4 * q + 3) * nb] = s[q][2];
+            in = y;
+        }
+    }
+    return correct(a, r, d, in, qv, wf);
+}
+
+// any number of sections
+__device__ __noinline__ float boundary_loop(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
 {
     const float d = __fsub_rn(ce, qv);
     float in = d;
@@ -156,18 +228,15 @@ __device__ __noinline__ float boundary(const StepArgs &a, float r, float ce, flo
         st[3 * nb] = s2;
         in = y;
     }
-    const double w = (double)__ldg(a.bw + slot);
-    if (a.form == VIRS_BOUNDARY_REFERENCE) {
-        const double t = __fma_rn((double)in, a.mix_y, __dmul_rn((double)d, a.mix_d));
-        const double u = __dmul_rn(__dmul_rn(__dmul_rn(a.K, t), a.gain), w);
-        return __double2float_rn(__dsub_rn((double)r, u));
-    }
-    // centered: the direct damping term at (p+ - p-)/2, solved for p+
-    const double kgw = __dmul_rn(__dmul_rn(a.K, a.gain), w);
-    const double ac = __dmul_rn(__dmul_rn(kgw, a.mix_d), 0.5);
-    const double num = __dadd_rn(__dsub_rn((double)r, __dmul_rn(kgw, __dmul_rn((double)in, a.mix_y))),
-                                 __dmul_rn(ac, (double)qv));
-    return __double2float_rn(__ddiv_rn(num, __dadd_rn(1.0, ac)));
+    return correct(a, r, d, in, qv, __ldg(a.bw + slot));
+}
+
+// MAXS = 0: the loop form
+template <int MAXS>
+__device__ __forceinline__ float boundary(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+{
+    if constexpr (MAXS == 0) return boundary_loop(a, r, ce, qv, slot);
+    else return boundary_unrolled<MAXS>(a, r, ce, qv, slot);
 }
 
 } // namespace

@@ -198,6 +198,26 @@ def batched(seed: int = 5, steps: int = 3000, n_sources: int = 64, n_rooms: int 
     return out
 
 
+def inverse_design(seed: int = 6, steps: int = 4000, size=(128, 128, 96), h: float = 1.0 / 64.0,
+                   n_materials: int = 6, n_sections: int = 2, n_receivers: int = 4):
+    """The inverse-design workload: a room of `size` voxels whose six faces
+    carry six materials of two sections each (12 coefficient sets, the
+    learnable parameters), one source, four receivers.  Returns
+    (scene with the hidden coefficients, initial-guess coefficients)."""
+    rng = np.random.default_rng(seed)
+    L = np.array(size, np.float64) * h
+    v, t, m = box((0, 0, 0), L, np.arange(6) % n_materials)
+    fs = fs_of(h, 1.0)
+    hidden = np.stack([design_octave_cascade_np(fs, a)[:n_sections] for a in rng.uniform(0.1, 0.7, (n_materials, 3))])
+    guess = np.stack([design_octave_cascade_np(fs, a)[:n_sections] for a in rng.uniform(0.1, 0.7, (n_materials, 3))])
+    src = _interior_points(rng, (0, 0, 0), L, 1, 0.3)
+    rcv = _interior_points(rng, (0, 0, 0), L, n_receivers, 0.3)
+    sig = diff_gaussian(steps, 6.0)[None, :]
+    sc = Scene("inverse_design", v, t, m, np.arange(n_materials, dtype=np.uint8), h, 0.0, 1.0, 1, steps,
+               n_materials, n_sections, hidden, src, sig, rcv, seed=seed)
+    return sc, guess
+
+
 def reference_room(seed: int = 4, steps: int = 300, size=(48, 40, 32), h: float = 0.05) -> Scene:
     """The reference's configuration on a small grid: material 0 walls,
     material 1 a speaker box (hard source), default filter and constants."""
