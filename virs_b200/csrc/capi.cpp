@@ -1428,6 +1428,7 @@ struct virs_batch {
     std::vector<virs_sim *> mem;
     std::vector<uint64_t> gen;
     int dev = 0, storage = 0, rows = 8, depth = 2, planes = 0;
+    bool persistent = false;
     uint64_t ntiles = 0, nbnd = 0;
     uint32_t max_sections = 0;
     DevBuf desc, err;
@@ -1516,7 +1517,8 @@ cudaError_t batch_enqueue(const virs_batch *b, int parity, cudaStream_t st)
 {
     const BatchMember *d = b->desc.as<BatchMember>();
     const uint32_t n = (uint32_t)b->mem.size();
-    cudaError_t e = launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->err.as<int>(), st);
+    cudaError_t e =
+        launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->persistent, b->err.as<int>(), st);
     if (e != cudaSuccess) return e;
     e = launch_boundary_batch(b->storage, d, n, b->nbnd, parity, b->max_sections, st);
     if (e != cudaSuccess) return e;
@@ -1668,8 +1670,10 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
     VIRS_CUDA(cudaEventCreate(&e0));
     VIRS_CUDA(cudaEventCreate(&e1));
     virs_tiling pick{8, 0, 2, 0.f};
+    bool pick_persistent = false;
     float best_ms = 1e30f;
     virs_status st = VIRS_OK;
+    for (int pers : {0, 1})
     for (int d : {1, 2, 3})
         for (int r : {4, 8, 16})
             for (int pl : {8, 16, 32, 64}) {
@@ -1677,6 +1681,7 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
                 b->rows = r;
                 b->depth = d;
                 b->planes = pl;
+                b->persistent = pers != 0;
                 if ((st = batch_build(b)) != VIRS_OK) break;
                 if ((st = batch_steps(b, 1, b->stream, false)) != VIRS_OK) break;
                 cudaEventRecord(e0, b->stream);
@@ -1692,6 +1697,7 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
                 if (ms < best_ms) {
                     best_ms = ms;
                     pick = {r, pl, d, ms / trial_steps};
+                    pick_persistent = pers != 0;
                 }
                 for (virs_sim *s : b->mem)
                     if ((st = reset_state(s)) != VIRS_OK) break;
@@ -1702,6 +1708,7 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
     b->rows = pick.tile_rows;
     b->depth = pick.pipeline_depth;
     b->planes = pick.planes_per_block;
+    b->persistent = pick_persistent;
     VIRS_TRY(batch_build(b));
     VIRS_TRY(virs_batch_synchronize(b));
     if (best) *best = pick;

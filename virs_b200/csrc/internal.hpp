@@ -115,7 +115,7 @@ struct alignas(64) BatchMember {
     uint32_t gx, gy, gz;    // tile grid
 };
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
-                                  uint64_t ntiles, int parity, int *err, cudaStream_t s);
+                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s);
 cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
                                   uint32_t max_sections, cudaStream_t s);
 cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem, int parity, cudaStream_t s);

@@ -202,25 +202,30 @@ __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepAr
 }
 
 // batched: thread g belongs to the last member whose first boundary index
-// is <= g (members without boundary voxels are skipped by that rule)
+// is <= g (members without boundary voxels are skipped by that rule); the
+// members' first indices are searched in shared memory
 template <typename T, int MAXS>
 __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__restrict mem, uint32_t nmem,
                                                         uint64_t ntotal, int parity)
 {
+    constexpr uint32_t CACHE = 1024;
+    __shared__ uint64_t first[CACHE];
+    const bool cached = nmem <= CACHE;
+    if (cached)
+        for (uint32_t m = threadIdx.x; m < nmem; m += blockDim.x) first[m] = mem[m].first_bnd;
+    __syncthreads();
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ntotal) return;
     uint32_t lo = 0, hi = nmem - 1;
     while (lo < hi) {
         const uint32_t mid = (lo + hi + 1) / 2;
-        if (mem[mid].first_bnd <= g) lo = mid;
+        if ((cached ? first[mid] : mem[mid].first_bnd) <= g) lo = mid;
         else hi = mid - 1;
     }
     const BatchMember &b = mem[lo];
     boundary_record<T, MAXS>(b.step[parity], b.bidx, g - b.first_bnd);
 }
 
-// Additive sources, then receivers, then the step counter
-// (simulator_gpu.cu:292-300: the receiver reads the new field).
 template <typename T> __device__ __forceinline__ void post_body(const PostArgs &a)
 {
     using IO = Io<T>;

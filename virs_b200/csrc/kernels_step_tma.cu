@@ -300,9 +300,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
     step_tile<T, TY, L>(a, &mP, &mQ, &mC, &mB, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
 }
 
-// Many simulations in one launch: a persistent grid walks the concatenated
-// tile lists of all members (tiles of a member are consecutive, so
-// neighbouring tiles run at the same time and share the halo rows in L2).
+// Many simulations in one launch: the blocks walk the concatenated tile
+// lists of all members (tiles of a member are consecutive, so neighbouring
+// tiles run at the same time and share the halo rows in L2), either one
+// tile per block or, persistent, a single wave of blocks striding over all.
 template <typename T, int TY, int L>
 __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma_batch(const BatchMember *__restrict mem,
                                                                               uint32_t nmem, uint64_t ntiles,
@@ -380,7 +381,8 @@ __global__ void k_wait_probe(int *err, uint32_t limit)
 }
 
 template <typename T, int TY, int L>
-cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, int *err, cudaStream_t s)
+cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, bool persistent, int *err,
+                          cudaStream_t s)
 {
     auto kern = k_step_tma_batch<T, TY, L>;
     constexpr size_t sm = smem_bytes<T, TY, L>();
@@ -390,43 +392,48 @@ cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * TY, sm)) != cudaSuccess) return e;
-    const uint64_t grid = std::min<uint64_t>(ntiles, (uint64_t)nsm * (uint64_t)std::max(per, 1));
+    // persistent: one wave of blocks walks all tiles; otherwise one block per
+    // tile and the hardware scheduler overlaps the blocks' prologues
+    const uint64_t cap = persistent ? (uint64_t)nsm * (uint64_t)std::max(per, 1) : (uint64_t)INT32_MAX;
+    const uint64_t grid = std::min<uint64_t>(ntiles, cap);
     kern<<<(unsigned)grid, dim3(32, TY), sm, s>>>(mem, nmem, ntiles, parity, err);
     return cudaGetLastError();
 }
 
 template <typename T, int TY>
-cudaError_t launch_batch2(int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, int *err,
-                          cudaStream_t s)
+cudaError_t launch_batch2(int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity,
+                          bool persistent, int *err, cudaStream_t s)
 {
     switch (depth) {
-    case 1: return launch_batch3<T, TY, 1>(mem, nmem, ntiles, parity, err, s);
-    case 3: return launch_batch3<T, TY, 3>(mem, nmem, ntiles, parity, err, s);
-    default: return launch_batch3<T, TY, 2>(mem, nmem, ntiles, parity, err, s);
+    case 1: return launch_batch3<T, TY, 1>(mem, nmem, ntiles, parity, persistent, err, s);
+    case 3: return launch_batch3<T, TY, 3>(mem, nmem, ntiles, parity, persistent, err, s);
+    default: return launch_batch3<T, TY, 2>(mem, nmem, ntiles, parity, persistent, err, s);
     }
 }
 
 template <typename T>
 cudaError_t launch_batch1(int rows, int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity,
-                          int *err, cudaStream_t s)
+                          bool persistent, int *err, cudaStream_t s)
 {
     switch (rows) {
-    case 4: return launch_batch2<T, 4>(depth, mem, nmem, ntiles, parity, err, s);
-    case 16: return launch_batch2<T, 16>(depth, mem, nmem, ntiles, parity, err, s);
-    default: return launch_batch2<T, 8>(depth, mem, nmem, ntiles, parity, err, s);
+    case 4: return launch_batch2<T, 4>(depth, mem, nmem, ntiles, parity, persistent, err, s);
+    case 16: return launch_batch2<T, 16>(depth, mem, nmem, ntiles, parity, persistent, err, s);
+    default: return launch_batch2<T, 8>(depth, mem, nmem, ntiles, parity, persistent, err, s);
     }
 }
 
 } // namespace
 
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
-                                  uint64_t ntiles, int parity, int *err, cudaStream_t s)
+                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s)
 {
     if (ntiles == 0) return cudaSuccess;
     switch (storage) {
-    case VIRS_STORAGE_F16: return launch_batch1<__half>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
-    case VIRS_STORAGE_BF16: return launch_batch1<__nv_bfloat16>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
-    default: return launch_batch1<float>(tile_rows, depth, mem, nmem, ntiles, parity, err, s);
+    case VIRS_STORAGE_F16:
+        return launch_batch1<__half>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
+    case VIRS_STORAGE_BF16:
+        return launch_batch1<__nv_bfloat16>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
+    default: return launch_batch1<float>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
     }
 }
 
