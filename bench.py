@@ -53,6 +53,8 @@ sys.path.insert(0, str(ROOT))
 BYTES_F32 = 13.0   # per voxel update: p 4 + p^{n-1} 4 + p^{n+1} 4 + code 1
 BYTES_16 = 7.0     # 16-bit storage: 2 + 2 + 2 + 1
 METRIC = "Gvoxel-updates/s"
+STORAGE_NAMES = {"f32": "FP32", "bf16": "BF16 storage (FP32 update)", "f16": "FP16 storage (FP32 update)"}
+KERNEL_TYPES = {"f32": "float", "bf16": "__nv_bfloat16", "f16": "__half"}
 
 
 def env_rank():
@@ -65,6 +67,23 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_traffic(path: Path, storage: str, nvox: int):
+    """DRAM bytes (read + write) per launch of the stencil kernel, from the ncu
+    summary: lines `storage=<s> voxels=<n> bytes_per_launch=<b> ...`, scaled by
+    the voxel count when the capture ran a smaller grid."""
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        f = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
+        if f.get("storage") == storage and "voxels" in f and "bytes_per_launch" in f:
+            n, b = int(f["voxels"]), float(f["bytes_per_launch"])
+            src = f"ncu dram__bytes_read.sum + dram__bytes_write.sum, {path.name}"
+            if n != nvox:
+                src += f", captured on {n} voxels and scaled by {nvox / n:.3f}"
+            return {"bytes": round(b * nvox / n), "source": src}
+    return None
 
 
 def host_threads():
@@ -286,9 +305,11 @@ def run_virs(args):
     sc = scenes.large_hall(steps=total_steps, size=tuple(args.size))
     nvox = int(np.prod(args.size))
     stream = torch.cuda.Stream(device=dev)
-    r32 = bench_storage(sc, capi.STORAGE_F32, args, stream, dev, world, dist, want_e2e=True)
+    storage = {"f32": capi.STORAGE_F32, "bf16": capi.STORAGE_BF16, "f16": capi.STORAGE_F16}[args.storage]
+    bpv = BYTES_F32 if storage == capi.STORAGE_F32 else BYTES_16
+    r32 = bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e=True)
     variants = {}
-    if args.variants:
+    if args.variants and storage == capi.STORAGE_F32:
         rb = bench_storage(sc, capi.STORAGE_BF16, args, stream, dev, world, dist, want_e2e=False)
         gv = nvox * args.steps / (rb["ms"] * 1e-3) / 1e9 * world
         peak, _ = peaks()
@@ -311,7 +332,7 @@ def run_virs(args):
     peak, peak_kind = peaks()
     value = nvox * args.steps / (r32["ms"] * 1e-3) / 1e9 * world
     kernel_ms = r32.get("kernel_ms")
-    achieved = nvox * BYTES_F32 / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    achieved = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -323,14 +344,15 @@ def run_virs(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": args.storage,
         "data": "synthetic (seeded hall geometry, Gaussian-pulse source)",
         "config": {
-            "workload": "large_hall %dx%dx%d FP32, 2 materials x 3-section cascades, sponge 1, 1 source, "
-                        "8 receivers, Courant 1/sqrt(3), centered boundary form" % tuple(args.size),
+            "workload": "large_hall %dx%dx%d %s, 2 materials x 3-section cascades, sponge 1, 1 source, "
+                        "8 receivers, Courant 1/sqrt(3), centered boundary form"
+                        % (*args.size, STORAGE_NAMES[args.storage]),
             "voxels": nvox,
             "boundary_voxels": int(r32["meta"]["info"].boundary_count),
-            "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * 4 / 1e9),
+            "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * (bpv - 1) / 3 / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
             "timing": "CUDA events on the launching stream around virs_run (CUDA graph), max over ranks",
             "tiling": r32["tiling"],
@@ -343,9 +365,9 @@ def run_virs(args):
             "frac": round(achieved / peak, 4) if achieved else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
             "traffic": None,
-            "kernel": "k_step_tma<float> (stencil; boundary voxels in a separate list pass)",
+            "kernel": "k_step_tma<%s> (stencil; boundary voxels in a separate list pass)" % KERNEL_TYPES[args.storage],
             "kernel_ms": kernel_ms,
-            "bytes_per_voxel": BYTES_F32,
+            "bytes_per_voxel": bpv,
             "boundary_pass_ms": r32.get("boundary_ms"),
         },
         "e2e": {
@@ -362,8 +384,10 @@ def run_virs(args):
     }
     if "batched_bf16" in variants:
         variants["bf16_batched_vs_f32_plain"] = round(variants["batched_bf16"]["value"] / value, 3)
-    if args.traffic_json and Path(args.traffic_json).exists():
-        line["roofline"]["traffic"] = json.loads(Path(args.traffic_json).read_text()).get("bytes_per_launch")
+    tr = measured_traffic(Path(args.traffic), args.storage, nvox)
+    if tr:
+        line["roofline"]["traffic"] = tr["bytes"]
+        line["roofline"]["traffic_source"] = tr["source"]
     if world == 1 and not args.no_cpu:
         th = host_threads()
         gv, desc, secs = cpu_sample(tuple(args.size), args.cpu_seconds, th)
@@ -450,7 +474,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=60, help="timed steps of the batched workload (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--traffic-json", default=str(ROOT / "profiles" / "step_traffic.json"))
+    ap.add_argument("--storage", choices=list(STORAGE_NAMES), default="f32",
+                    help="field storage of the timed hall (f32 is the headline; bf16/f16 store 16-bit fields)")
+    ap.add_argument("--traffic", default=str(ROOT / "profiles" / "k_step_tma_dram_traffic.txt"),
+                    help="ncu DRAM-traffic summary of the stencil kernel")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

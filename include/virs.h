@@ -298,9 +298,9 @@ virs_status virs_batch_autotune(virs_batch *batch, uint32_t trial_steps, virs_ti
 virs_status virs_batch_destroy(virs_batch *batch);
 
 /* Failure-path self test (no reference counterpart): launches a kernel that
- * waits, `limit` times (1..2^20), on an mbarrier that nothing completes, the
- * way the step kernel's bounded waits give up; returns VIRS_E_TIMEOUT when
- * the timeout was reported, and the handle stays usable. */
+ * waits `limit` microseconds (1..2^20) on an mbarrier that nothing completes,
+ * with the bounded wait of the step kernels; returns VIRS_E_TIMEOUT when the
+ * timeout was reported, and the handle stays usable. */
 virs_status virs_check_bounded_wait(virs_sim *sim, uint32_t limit);
 
 #ifdef __cplusplus

@@ -40,7 +40,12 @@ using namespace step;
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int TX = 128;
-constexpr uint32_t WAIT_LIMIT = 1u << 22;
+// A waiting thread asks to be parked for up to WAIT_HINT_NS per try (it
+// resumes as soon as the stage's phase completes), so the waiting warp does
+// not spin on issue slots that the computing warps need; the whole wait is
+// bounded by WAIT_LIMIT_NS of the global timer.
+constexpr uint32_t WAIT_HINT_NS = 20000;
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -54,16 +59,23 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity)
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *b, uint32_t parity)
 {
     uint32_t ok;
     asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
                  "selp.u32 %0, 1, 0, p;\n\t}"
                  : "=r"(ok)
-                 : "r"(saddr(b)), "r"(parity)
+                 : "r"(saddr(b)), "r"(parity), "r"(WAIT_HINT_NS)
                  : "memory");
     return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z)
@@ -131,14 +143,21 @@ template <> __device__ __forceinline__ void st4<__nv_bfloat16>(__nv_bfloat16 *p,
     __stcs(reinterpret_cast<uint2 *>(p), v);
 }
 
-__device__ __forceinline__ bool wait_stage(uint64_t *bars, int j, int D, int *err)
+// waits for phase `parity` of *b for at most limit_ns; on timeout sets *err
+__device__ __forceinline__ bool bounded_wait(uint64_t *b, uint32_t parity, uint64_t limit_ns, int *err)
 {
-    uint64_t *b = bars + (j % D);
-    const uint32_t parity = (uint32_t)((j / D) & 1);
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-        if (mbar_try_wait(b, parity)) return true;
+    if (mbar_try_wait_hint(b, parity)) return true;
+    const uint64_t t0 = global_ns();
+    do {
+        if (mbar_try_wait_hint(b, parity)) return true;
+    } while (global_ns() - t0 < limit_ns);
     atomicExch(err, 1);
     return false;
+}
+
+__device__ __forceinline__ bool wait_stage(uint64_t *bars, int j, int D, int *err)
+{
+    return bounded_wait(bars + (j % D), (uint32_t)((j / D) & 1), WAIT_LIMIT_NS, err);
 }
 
 // One tile (bx, by, bz) of one simulation.  `jg` is the block's running
@@ -365,9 +384,10 @@ cudaError_t launch1(int rows, int depth, const StepArgs &a, const TmaMaps &m, in
     }
 }
 
-// Waits on an mbarrier that nothing completes, `limit` times, then reports
-// the timeout through *err as every bounded wait of the step does.
-__global__ void k_wait_probe(int *err, uint32_t limit)
+// Waits on an mbarrier that nothing completes, for limit_us microseconds,
+// with the bounded wait of the step kernels, which reports the timeout
+// through *err.
+__global__ void k_wait_probe(int *err, uint32_t limit_us)
 {
     __shared__ uint64_t bar;
     if (threadIdx.x == 0) {
@@ -375,9 +395,7 @@ __global__ void k_wait_probe(int *err, uint32_t limit)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    for (uint32_t it = 0; it < limit; ++it)
-        if (mbar_try_wait(&bar, 0)) return;
-    if (threadIdx.x == 0) atomicExch(err, 1);
+    if (threadIdx.x == 0) bounded_wait(&bar, 0, (uint64_t)limit_us * 1000ull, err);
 }
 
 template <typename T, int TY, int L>
