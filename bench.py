@@ -50,6 +50,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+GRAPH_WARMUP = 64  # warm-up steps at least: both step graphs (32 steps per parity) built and launched once
 BYTES_F32 = 13.0   # per voxel update: p 4 + p^{n-1} 4 + p^{n+1} 4 + code 1
 BYTES_16 = 7.0     # 16-bit storage: 2 + 2 + 2 + 1
 METRIC = "Gvoxel-updates/s"
@@ -174,10 +175,11 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     CUDA-event pass, and (optionally) the end-to-end host run."""
     import torch
     from virs_b200 import scenes
-    total = args.warmup + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
+    warm = max(args.warmup, GRAPH_WARMUP)
+    total = warm + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
     sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
     tiling = sim.autotune(args.tune_steps) if args.tune_steps else sim.tiling()
-    sim.run(args.warmup, stream.cuda_stream)
+    sim.run(warm, stream.cuda_stream)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -236,7 +238,7 @@ def bench_batch(storage, args, stream, dev):
     of 96^3..320^3, advanced by three launches per step (virs_batch)."""
     import torch
     from virs_b200 import capi, scenes
-    steps, warm = args.batch_steps, 5
+    steps, warm = args.batch_steps, GRAPH_WARMUP
     scs = scenes.batched(steps=steps + warm + 2 * 3 + 4)
     sims = [scenes.build_simulation(sc, storage=storage, device=dev)[0] for sc in scs]
     nvox = sum(int(np.prod(s.shape)) for s in sims)
@@ -301,7 +303,7 @@ def run_virs(args):
     dev = local
     torch.cuda.set_device(dev)
     from virs_b200 import capi, scenes
-    total_steps = args.warmup + 3 * args.steps + args.kernel_steps + 16
+    total_steps = max(args.warmup, GRAPH_WARMUP) + 3 * args.steps + args.kernel_steps + 16
     sc = scenes.large_hall(steps=total_steps, size=tuple(args.size))
     nvox = int(np.prod(args.size))
     stream = torch.cuda.Stream(device=dev)

@@ -85,13 +85,20 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
                  : "memory");
 }
 
-template <typename T> struct Geo {
+// Thread layout: every thread updates V consecutive voxels of one row, the
+// ones one 16-byte vector holds (4 FP32 or 8 16-bit values); a tile row is
+// TX = 128 voxels, so LPR = 128 / V lanes share a row and a warp covers RPW
+// rows (1 for FP32, 2 for 16-bit storage).
+template <typename T> struct Lay {
+    static constexpr int V = 16 / (int)sizeof(T);
+    static constexpr int LPR = TX / V;
+    static constexpr int RPW = 32 / LPR;
     static constexpr int PAD = 16 / (int)sizeof(T); // x halo: one 16-byte chunk on each side
     static constexpr int PW = TX + 2 * PAD;
 };
 
 template <typename T, int TY> struct Stage {
-    static constexpr uint32_t PB = Geo<T>::PW * (TY + 2) * sizeof(T);
+    static constexpr uint32_t PB = Lay<T>::PW * (TY + 2) * sizeof(T);
     static constexpr uint32_t QB = TX * TY * sizeof(T);
     static constexpr uint32_t CB = TX * TY;
     static constexpr uint32_t BB = 4 * TY * sizeof(uint32_t); // 4 prefix segments per tile row
@@ -102,46 +109,20 @@ template <typename T, int TY> struct Stage {
     static constexpr uint32_t SB = PBa + QBa + CBa + BBa;
 };
 
-template <typename T> __device__ __forceinline__ void ld4(const T *p, float (&r)[4]);
-template <> __device__ __forceinline__ void ld4<float>(const float *p, float (&r)[4])
-{
-    const float4 v = *reinterpret_cast<const float4 *>(p);
-    r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
-}
-template <> __device__ __forceinline__ void ld4<__half>(const __half *p, float (&r)[4])
-{
-    const uint2 v = *reinterpret_cast<const uint2 *>(p);
-    const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&v.x));
-    const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&v.y));
-    r[0] = a.x; r[1] = a.y; r[2] = b.x; r[3] = b.y;
-}
-template <> __device__ __forceinline__ void ld4<__nv_bfloat16>(const __nv_bfloat16 *p, float (&r)[4])
-{
-    const uint2 v = *reinterpret_cast<const uint2 *>(p);
-    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v.x));
-    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v.y));
-    r[0] = a.x; r[1] = a.y; r[2] = b.x; r[3] = b.y;
-}
-
-template <typename T> __device__ __forceinline__ void st4(T *p, const float (&r)[4]);
-template <> __device__ __forceinline__ void st4<float>(float *p, const float (&r)[4])
-{
-    __stcs(reinterpret_cast<float4 *>(p), make_float4(r[0], r[1], r[2], r[3]));
-}
-template <> __device__ __forceinline__ void st4<__half>(__half *p, const float (&r)[4])
-{
-    uint2 v;
-    *reinterpret_cast<__half2 *>(&v.x) = __floats2half2_rn(r[0], r[1]);
-    *reinterpret_cast<__half2 *>(&v.y) = __floats2half2_rn(r[2], r[3]);
-    __stcs(reinterpret_cast<uint2 *>(p), v);
-}
-template <> __device__ __forceinline__ void st4<__nv_bfloat16>(__nv_bfloat16 *p, const float (&r)[4])
-{
-    uint2 v;
-    *reinterpret_cast<__nv_bfloat162 *>(&v.x) = __floats2bfloat162_rn(r[0], r[1]);
-    *reinterpret_cast<__nv_bfloat162 *>(&v.y) = __floats2bfloat162_rn(r[2], r[3]);
-    __stcs(reinterpret_cast<uint2 *>(p), v);
-}
+// the V cell codes of a thread (4 or 8 bytes)
+template <int V> struct Codes;
+template <> struct Codes<4> {
+    uint32_t w;
+    __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint32_t *>(p); }
+    __device__ bool any() const { return w != 0u; }
+    __device__ uint32_t get(int k) const { return (w >> (8 * k)) & 0xffu; }
+};
+template <> struct Codes<8> {
+    uint2 w;
+    __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint2 *>(p); }
+    __device__ bool any() const { return (w.x | w.y) != 0u; }
+    __device__ uint32_t get(int k) const { return ((k < 4 ? w.x : w.y) >> (8 * (k & 3))) & 0xffu; }
+};
 
 // waits for phase `parity` of *b for at most limit_ns; on timeout sets *err
 __device__ __forceinline__ bool bounded_wait(uint64_t *b, uint32_t parity, uint64_t limit_ns, int *err)
@@ -155,143 +136,221 @@ __device__ __forceinline__ bool bounded_wait(uint64_t *b, uint32_t parity, uint6
     return false;
 }
 
-__device__ __forceinline__ bool wait_stage(uint64_t *bars, int j, int D, int *err)
+__device__ __forceinline__ bool wait_stage(uint64_t *bars, uint32_t j, int D, int *err)
 {
-    return bounded_wait(bars + (j % D), (uint32_t)((j / D) & 1), WAIT_LIMIT_NS, err);
+    return bounded_wait(bars + (j % D), (j / D) & 1u, WAIT_LIMIT_NS, err);
 }
 
-// One tile (bx, by, bz) of one simulation.  `jg` is the block's running
-// count of issued stages; it continues across tiles so that the ring slot
-// and mbarrier phase of every stage stay consistent when a block processes
-// several tiles (the batched kernel).  Returns false when a bounded wait
-// gave up.
-template <typename T, int TY, int L>
-__device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
-                                          const CUtensorMap *mC, const CUtensorMap *mB, int bx, int by, int bz,
-                                          int *err, unsigned char *smem, uint64_t *bars, uint32_t &jg)
-{
+// The per-tile constants of the plane loop.
+template <typename T, int TY, int L> struct Tile {
+    const StepArgs *a;
+    unsigned char *smem;
+    uint64_t *bars;
+    const CUtensorMap *mP, *mQ, *mC, *mB;
+    int *err;
+    int x0, y0, z0, nst, row, sl, c0, t0, seg, seg4;
+    uint32_t j0;
+    bool act, leader;
+    float hardv;
+    float2 c2dt2, inv_h2;
+    size_t plane;
+
+    static constexpr int D = L + 2;
     using S = Stage<T, TY>;
-    constexpr int PAD = Geo<T>::PAD, PW = Geo<T>::PW;
-    constexpr int D = L + 3;
 
-    const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
-    const int x0 = bx * TX;
-    const int x = x0 + lane * 4;
-    const int y0 = by * TY;
-    const int y = y0 + ty;
-    const int z0 = 1 + bz * a.zc;
-    const int z1 = min(z0 + a.zc, (int)a.nz - 1);
-    if (z0 >= z1) return true;
-    const int jmax = z1 - z0 + 1; // last stage ordinal (plane z1 - 1)
-    const int ny = (int)a.ny;
-    const bool act = x < (int)a.px && y < ny;
-    const size_t plane = (size_t)a.px * ny;
-    T *Q = static_cast<T *>(a.q);
-    const uint32_t j0 = jg;
-    const int seg = x0 / SEG, seg4 = seg & ~3; // prefix box starts on a 16-byte boundary
-
-    auto issue = [&](int j) {
-        const int k = z0 - 2 + j;
+    // stage j holds plane z0 - 1 + j (see step_tile)
+    __device__ __forceinline__ void issue(int j) const
+    {
+        constexpr int PAD = Lay<T>::PAD;
+        const int k = z0 - 1 + j;
         const uint32_t g = j0 + (uint32_t)j;
         unsigned char *st = smem + (g % D) * S::SB;
         uint64_t *b = bars + (g % D);
-        const bool full = j >= 2;
+        const bool full = j >= 1 && j <= nst - 2;
         mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB + S::BB : 0u));
-        tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k + 1);
+        tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k);
         if (full) {
             tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
             tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
             tma_load_3d(st + S::PBa + S::QBa + S::CBa, mB, b, seg4, y0, k);
         }
-    };
-    if (tid == 0)
-        for (int j = 0; j < D && j <= jmax; ++j) issue(j);
-
-    for (int i = 0, z = z0; z < z1; ++i, ++z) {
-        // thread 0 waits for the stage (bounded); the barrier then tells every
-        // thread that the stage is ready and that everyone is done with plane
-        // z-1, so the stage that held P(z-2) can be refilled
-        bool bad = false;
-        if (tid == 0) {
-            bad = !wait_stage(bars, j0 + i + 2, D, err);
-            if (i == 0) bad = bad || !wait_stage(bars, j0, D, err) || !wait_stage(bars, j0 + 1, D, err);
-        }
-        if (__syncthreads_or(bad)) return false;
-        if (tid == 0 && i >= 1 && i + L + 2 <= jmax) issue(i + L + 2);
-
-        const T *Pm = reinterpret_cast<const T *>(smem + ((j0 + i) % D) * S::SB);       // P(z-1)
-        const T *Pc = reinterpret_cast<const T *>(smem + ((j0 + i + 1) % D) * S::SB);   // P(z)
-        const unsigned char *s2 = smem + ((j0 + i + 2) % D) * S::SB;
-        const T *Pp = reinterpret_cast<const T *>(s2);                                   // P(z+1)
-        const T *Qs = reinterpret_cast<const T *>(s2 + S::PBa);
-        const uint32_t code4 = *reinterpret_cast<const uint32_t *>(s2 + S::PBa + S::QBa + ty * TX + lane * 4);
-
-        const int c0 = (ty + 1) * PW + PAD + lane * 4;
-        float cc[4], ym[4], yp[4], zm[4], zp[4], qv[4];
-        ld4(Pc + c0, cc);
-        ld4(Pc + c0 - PW, ym);
-        ld4(Pc + c0 + PW, yp);
-        ld4(Pm + c0, zm);
-        ld4(Pp + c0, zp);
-        ld4(Qs + ty * TX + lane * 4, qv);
-        float left = __shfl_up_sync(FULL, cc[3], 1);
-        float right = __shfl_down_sync(FULL, cc[0], 1);
-        if (lane == 0) left = Io<T>::get(Pc[c0 - 1]);
-        if (lane == 31) right = Io<T>::get(Pc[c0 + 4]);
-
-        float r[4];
-        unsigned bmask = 0;
-        if (code4 == 0u) {
-            // four air voxels without wall neighbours: the common case
-            r[0] = leapfrog_air(cc[0], cc[1], left, yp[0], ym[0], zp[0], zm[0], qv[0], a.c2dt2, a.inv_h2);
-            r[1] = leapfrog_air(cc[1], cc[2], cc[0], yp[1], ym[1], zp[1], zm[1], qv[1], a.c2dt2, a.inv_h2);
-            r[2] = leapfrog_air(cc[2], cc[3], cc[1], yp[2], ym[2], zp[2], zm[2], qv[2], a.c2dt2, a.inv_h2);
-            r[3] = leapfrog_air(cc[3], right, cc[2], yp[3], ym[3], zp[3], zm[3], qv[3], a.c2dt2, a.inv_h2);
-        } else
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint8_t c = (uint8_t)(code4 >> (8 * k));
-            const float xm = k == 0 ? left : cc[k - 1];
-            const float xp = k == 3 ? right : cc[k + 1];
-            if (c >= CODE_HARD) {
-                if (c == CODE_NONE) r[k] = qv[k];
-                else if (c == CODE_WALL) r[k] = 0.f;
-                else {
-                    const uint32_t sn = __ldg(a.ctr);
-                    r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
-                }
-            } else {
-                r[k] = leapfrog(c, cc[k], xp, xm, yp[k], ym[k], zp[k], zm[k], qv[k], a.c2dt2, a.inv_h2);
-                if (c & CODE_BND) bmask |= 1u << k;
-            }
-        }
-        // Boundary voxels: the record {free value, p, p^{n-1}} goes to their
-        // slot of the compacted list for the boundary pass, and p^{n-1} stays
-        // in place.  A warp covers consecutive voxels of one row, so the slot
-        // is the row segment's prefix (staged with the plane) plus a warp scan.
-        if (!act) bmask = 0;
-        if (__any_sync(FULL, bmask != 0)) {
-            const int cnt = __popc(bmask);
-            int inc = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(FULL, inc, o);
-                if (lane >= o) inc += t;
-            }
-            if (bmask) {
-                const uint32_t *bs = reinterpret_cast<const uint32_t *>(s2 + S::PBa + S::QBa + S::CBa);
-                uint64_t slot = (uint64_t)bs[ty * 4 + (seg - seg4)] + (uint64_t)(inc - cnt);
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (bmask & (1u << k)) {
-                        a.side[slot++] = make_float4(r[k], cc[k], qv[k], 0.f);
-                        r[k] = qv[k];
-                    }
-            }
-        }
-        if (act) st4(Q + (size_t)z * plane + (size_t)y * a.px + x, r);
     }
-    jg = j0 + (uint32_t)jmax + 1;
+
+    // Plane z = z0 + i: zm and cc hold the centres of P(z-1) and P(z); the
+    // centre of P(z+1) is loaded into zp.  `sh` is the ring slot of the
+    // stage of z, `out` the thread's first output voxel of plane z.
+    __device__ __forceinline__ bool plane_step(int i, const float (&zm)[Lay<T>::V], const float (&cc)[Lay<T>::V],
+                                               float (&zp)[Lay<T>::V], uint32_t &sh, T *&out) const
+    {
+        using IO = Io<T>;
+        constexpr int V = Lay<T>::V, LPR = Lay<T>::LPR, PW = Lay<T>::PW;
+        // the leader waits for the stage of z+1 (bounded); the barrier then
+        // tells every thread that it is ready and that everyone is done with
+        // the stage of z-1, which is refilled with the plane D on
+        bool bad = false;
+        if (leader) bad = !wait_stage(bars, j0 + (uint32_t)i + 2u, D, err);
+        if (__syncthreads_or(bad)) return false;
+        if (leader && i + D < nst) issue(i + D);
+        const uint32_t sz = sh + 1u == (uint32_t)D ? 0u : sh + 1u;
+
+        const unsigned char *s0 = smem + sh * S::SB;
+        const T *Ph = reinterpret_cast<const T *>(s0);
+        float ym[V], yp[V], qv[V];
+        IO::ld(reinterpret_cast<const T *>(smem + sz * S::SB) + c0, zp);
+        IO::ld(Ph + c0 - PW, ym);
+        IO::ld(Ph + c0 + PW, yp);
+        IO::ld(reinterpret_cast<const T *>(s0 + S::PBa) + t0, qv);
+        Codes<V> code;
+        code.load(s0 + S::PBa + S::QBa + t0);
+        float left = __shfl_up_sync(FULL, cc[V - 1], 1, LPR);
+        float right = __shfl_down_sync(FULL, cc[0], 1, LPR);
+        if (sl == 0) left = IO::ld1(Ph + c0 - 1);
+        if (sl == LPR - 1) right = IO::ld1(Ph + c0 + V);
+
+        // every voxel as air without wall neighbours, the common case, two
+        // at a time ...
+        float r[V];
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            const float2 x2 = make_float2(__fadd_rn(cc[k + 1], k > 0 ? cc[k - 1] : left),
+                                          __fadd_rn(k + 2 < V ? cc[k + 2] : right, cc[k]));
+            const float2 o = leapfrog_air2(make_float2(cc[k], cc[k + 1]), x2, make_float2(yp[k], yp[k + 1]),
+                                           make_float2(ym[k], ym[k + 1]), make_float2(zp[k], zp[k + 1]),
+                                           make_float2(zm[k], zm[k + 1]), make_float2(qv[k], qv[k + 1]), c2dt2, inv_h2);
+            r[k] = o.x;
+            r[k + 1] = o.y;
+        }
+        // ... then the voxels with another code, recomputed in full
+        if (__any_sync(FULL, code.any())) {
+            unsigned bmask = 0;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const uint32_t c = code.get(k);
+                if (c != 0u) {
+                    if (c >= CODE_HARD) {
+                        r[k] = c == CODE_NONE ? qv[k] : (c == CODE_WALL ? 0.f : hardv);
+                    } else {
+                        r[k] = leapfrog((uint8_t)c, cc[k], k == V - 1 ? right : cc[k + 1], k == 0 ? left : cc[k - 1],
+                                        yp[k], ym[k], zp[k], zm[k], qv[k], a->c2dt2, a->inv_h2);
+                        if (c & CODE_BND) bmask |= 1u << k;
+                    }
+                }
+            }
+            // Boundary voxels: the record {free value, p, p^{n-1}} goes to
+            // their slot of the compacted list for the boundary pass, and
+            // p^{n-1} stays in place.  The lanes of a row cover consecutive
+            // voxels of one 128-voxel segment, so the slot is the segment's
+            // prefix (staged with the plane) plus a scan over the row's lanes.
+            if (!act) bmask = 0;
+            if (__any_sync(FULL, bmask != 0)) {
+                const int cnt = __popc(bmask);
+                int inc = cnt;
+#pragma unroll
+                for (int o = 1; o < LPR; o <<= 1) {
+                    const int t = __shfl_up_sync(FULL, inc, o, LPR);
+                    if (sl >= o) inc += t;
+                }
+                if (bmask) {
+                    const uint32_t *bs = reinterpret_cast<const uint32_t *>(s0 + S::PBa + S::QBa + S::CBa);
+                    uint64_t slot = (uint64_t)bs[row * 4 + (seg - seg4)] + (uint64_t)(inc - cnt);
+#pragma unroll
+                    for (int k = 0; k < V; ++k)
+                        if (bmask & (1u << k)) {
+                            a->side[slot++] = make_float4(r[k], cc[k], qv[k], 0.f);
+                            r[k] = qv[k];
+                        }
+                }
+            }
+        }
+        if (act) IO::st(out, r);
+        out += plane;
+        sh = sz;
+        return true;
+    }
+};
+
+// One tile (bx, by, bz) of one simulation.  Stage j of the tile holds the
+// plane k = z0 - 1 + j: P(k) with its halo, and for k in [z0, z1) also Q(k),
+// the codes of plane k and the row prefixes of the boundary list.  The
+// centres of P(z-1) and P(z) stay in registers from the previous planes, so
+// plane z reads the stage of z (halo neighbours, Q, codes) and the centre
+// of the stage of z+1; the ring has D = L + 2 slots.  The plane loop is
+// unrolled three times so that the three centre planes change roles
+// without register copies.  `jg` is the block's running count of issued
+// stages: it continues across tiles so that the ring slot and mbarrier
+// phase of every stage stay consistent when a block processes several
+// tiles (the batched kernel).  Returns false when a bounded wait gave up.
+template <typename T, int TY, int L>
+__device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
+                                          const CUtensorMap *mC, const CUtensorMap *mB, int bx, int by, int bz,
+                                          int *err, unsigned char *smem, uint64_t *bars, uint32_t &jg)
+{
+    using G = Lay<T>;
+    using S = Stage<T, TY>;
+    using IO = Io<T>;
+    constexpr int V = G::V, LPR = G::LPR, PAD = G::PAD, PW = G::PW;
+    constexpr int D = L + 2;
+    static_assert(IO::VEC == V && V % 2 == 0, "one 16-byte vector per thread, an even number of voxels");
+
+    Tile<T, TY, L> t;
+    const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
+    t.a = &a;
+    t.smem = smem;
+    t.bars = bars;
+    t.mP = mP;
+    t.mQ = mQ;
+    t.mC = mC;
+    t.mB = mB;
+    t.err = err;
+    t.row = threadIdx.y * G::RPW + lane / LPR; // row of the tile
+    t.sl = lane % LPR;                         // lane within the row
+    t.x0 = bx * TX;
+    t.y0 = by * TY;
+    t.z0 = 1 + bz * a.zc;
+    const int z1 = min(t.z0 + a.zc, (int)a.nz - 1);
+    if (t.z0 >= z1) return true;
+    t.nst = z1 - t.z0 + 2; // stages: planes z0-1 .. z1
+    const int x = t.x0 + t.sl * V, y = t.y0 + t.row;
+    t.act = x < (int)a.px && y < (int)a.ny;
+    t.leader = tid == 0;
+    t.j0 = jg;
+    t.seg = t.x0 / SEG;
+    t.seg4 = t.seg & ~3; // prefix box starts on a 16-byte boundary
+    t.c0 = (t.row + 1) * PW + PAD + t.sl * V; // this thread's first voxel in a halo box
+    t.t0 = t.row * TX + t.sl * V;            // ... and in a tile box
+    t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
+    t.inv_h2 = make_float2(a.inv_h2, a.inv_h2);
+    t.plane = (size_t)a.px * a.ny;
+
+    if (t.leader)
+        for (int j = 0; j < D && j < t.nst; ++j) t.issue(j);
+
+    // the hard-source value of this step (flag-3 voxels)
+    const uint32_t sn = __ldg(a.ctr);
+    t.hardv = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
+
+    float A[V], B[V], C[V];
+    {
+        bool bad = false;
+        if (t.leader) bad = !wait_stage(bars, t.j0, D, err) || !wait_stage(bars, t.j0 + 1u, D, err);
+        if (__syncthreads_or(bad)) return false;
+        IO::ld(reinterpret_cast<const T *>(smem + (t.j0 % D) * S::SB) + t.c0, A);        // P(z0-1)
+        IO::ld(reinterpret_cast<const T *>(smem + ((t.j0 + 1u) % D) * S::SB) + t.c0, B); // P(z0)
+    }
+    uint32_t sh = (t.j0 + 1u) % D; // slot of the stage of plane z
+    T *out = static_cast<T *>(a.q) + ((size_t)t.z0 * a.ny + (size_t)y) * a.px + x;
+    const int n = t.nst - 2;
+    int i = 0;
+    for (; i + 3 <= n; i += 3) {
+        if (!t.plane_step(i, A, B, C, sh, out)) return false;
+        if (!t.plane_step(i + 1, B, C, A, sh, out)) return false;
+        if (!t.plane_step(i + 2, C, A, B, sh, out)) return false;
+    }
+    if (i < n) {
+        if (!t.plane_step(i, A, B, C, sh, out)) return false;
+        if (i + 1 < n && !t.plane_step(i + 1, B, C, A, sh, out)) return false;
+    }
+    jg = t.j0 + (uint32_t)t.nst;
     return true;
 }
 
@@ -304,14 +363,21 @@ template <int D> __device__ __forceinline__ void init_bars(uint64_t *bars)
     __syncthreads();
 }
 
+template <typename T, int TY> constexpr int block_threads() { return 32 * TY / Lay<T>::RPW; }
+// blocks per SM the register allocation must allow: at least 768 threads
+template <typename T, int TY> constexpr int min_blocks()
+{
+    return block_threads<T, TY>() >= 768 ? 1 : 768 / block_threads<T, TY>();
+}
+
 template <typename T, int TY, int L>
-__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __grid_constant__ StepArgs a,
+__global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k_step_tma(const __grid_constant__ StepArgs a,
                                                                         const __grid_constant__ CUtensorMap mP,
                                                                         const __grid_constant__ CUtensorMap mQ,
                                                                         const __grid_constant__ CUtensorMap mC,
                                                                         const __grid_constant__ CUtensorMap mB, int *err)
 {
-    constexpr int D = L + 3;
+    constexpr int D = L + 2;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
@@ -324,11 +390,11 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma(const __
 // tiles run at the same time and share the halo rows in L2), either one
 // tile per block or, persistent, a single wave of blocks striding over all.
 template <typename T, int TY, int L>
-__global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma_batch(const BatchMember *__restrict mem,
+__global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k_step_tma_batch(const BatchMember *__restrict mem,
                                                                               uint32_t nmem, uint64_t ntiles,
                                                                               int parity, int *err)
 {
-    constexpr int D = L + 3;
+    constexpr int D = L + 2;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
@@ -348,7 +414,7 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step_tma_batch(co
 
 template <typename T, int TY, int L> constexpr size_t smem_bytes()
 {
-    return (size_t)(L + 3) * Stage<T, TY>::SB + (L + 3) * sizeof(uint64_t);
+    return (size_t)(L + 2) * Stage<T, TY>::SB + (L + 2) * sizeof(uint64_t);
 }
 
 template <typename T, int TY, int L>
@@ -360,7 +426,8 @@ cudaError_t launch3(const StepArgs &a, const TmaMaps &m, int *err, cudaStream_t 
     if (e != cudaSuccess) return e;
     const unsigned gx = (a.px + TX - 1) / TX;
     const unsigned gz = (a.nz - 2 + a.zc - 1) / a.zc;
-    kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, TY), sm, s>>>(a, *m.p, *m.q, *m.c, *m.b, err);
+    kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, block_threads<T, TY>() / 32), sm, s>>>(a, *m.p, *m.q, *m.c,
+                                                                                             *m.b, err);
     return cudaGetLastError();
 }
 
@@ -409,12 +476,13 @@ cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles
     int dev = 0, nsm = 0, per = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * TY, sm)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block_threads<T, TY>(), sm)) != cudaSuccess)
+        return e;
     // persistent: one wave of blocks walks all tiles; otherwise one block per
     // tile and the hardware scheduler overlaps the blocks' prologues
     const uint64_t cap = persistent ? (uint64_t)nsm * (uint64_t)std::max(per, 1) : (uint64_t)INT32_MAX;
     const uint64_t grid = std::min<uint64_t>(ntiles, cap);
-    kern<<<(unsigned)grid, dim3(32, TY), sm, s>>>(mem, nmem, ntiles, parity, err);
+    kern<<<(unsigned)grid, dim3(32, block_threads<T, TY>() / 32), sm, s>>>(mem, nmem, ntiles, parity, err);
     return cudaGetLastError();
 }
 

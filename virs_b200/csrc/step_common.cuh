@@ -147,6 +147,25 @@ __device__ __forceinline__ float leapfrog_air(float ce, float xp, float xm, floa
     return __fmaf_rn(c2dt2, lap, t);
 }
 
+// two air voxels at once with the packed FP32 instructions of sm_100, whose
+// components round exactly like the scalar __fadd_rn / __fmul_rn /
+// __fmaf_rn: bit-identical to two leapfrog_air calls.  The first sum
+// (xp + xm) comes in as x2: its operands straddle the register pairs of a
+// loaded vector, so it is two scalar adds.  2*ce is exact, so
+// fma(2, ce, -qv) rounds like fsub(2*ce, qv) (they part only where 2*ce
+// overflows).
+__device__ __forceinline__ float2 leapfrog_air2(float2 ce, float2 x2, float2 yp, float2 ym, float2 zp, float2 zm,
+                                                float2 qv, float2 c2dt2, float2 inv_h2)
+{
+    float2 s = __fadd2_rn(x2, yp);
+    s = __fadd2_rn(s, ym);
+    s = __fadd2_rn(s, zp);
+    s = __fadd2_rn(s, zm);
+    const float2 lap = __fmul2_rn(__ffma2_rn(make_float2(-6.0f, -6.0f), ce, s), inv_h2);
+    const float2 t = __ffma2_rn(make_float2(2.0f, 2.0f), ce, __fmul2_rn(qv, make_float2(-1.0f, -1.0f)));
+    return __ffma2_rn(c2dt2, lap, t);
+}
+
 // simulator_gpu.cu:126-148: biquad sections in series on d = p - p^{n-1}
 // (b0*in + b1*s0 contracted to fma(b0, in, b1*s0) as the reference build
 // does), then p+ -= K*(0.1*y + 0.9*d)*0.4 (times the sponge weight) in
