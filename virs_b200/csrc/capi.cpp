@@ -120,7 +120,7 @@ struct virs_sim {
     // kernel variant: depth 0 = register-streaming kernel, 1..3 = TMA
     // kernel with that many planes in flight
     int tile_rows = 8, zc = 0, depth = 2;
-    CUtensorMap tmP[2], tmQ[2], tmC, tmB;
+    CUtensorMap tmP[2], tmQ[2], tmC;
     DevBuf side;                   // {free, p, p^{n-1}} per boundary slot (TMA kernel -> boundary pass)
     int maps_rows = 0;             // tile rows the maps were built for (0 = none)
     DevBuf err;                    // device error flag of bounded waits
@@ -389,12 +389,6 @@ virs_status encode(CUtensorMap *m, CUtensorMapDataType dt, size_t elem, void *ba
     return encode_dims(m, dt, elem, base, s->px, s->ny, s->nz, bx, by);
 }
 
-// the boundary prefix, [nz][ny][spr] (spr is a multiple of 4)
-virs_status encode_prefix(CUtensorMap *m, const virs_sim *s, uint32_t rows)
-{
-    return encode_dims(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, s->bseg.ptr, s->spr, s->ny, s->nz, 4, rows);
-}
-
 // tensor maps of the two field buffers (halo box and tile box) and of the
 // cell codes, for the current tile height
 virs_status build_maps(virs_sim *s)
@@ -409,7 +403,6 @@ virs_status build_maps(virs_sim *s)
         VIRS_TRY(encode(&s->tmQ[b], dt, el, s->field[b].ptr, s, (uint32_t)tma_tile_x(), rows));
     }
     VIRS_TRY(encode(&s->tmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), rows));
-    VIRS_TRY(encode_prefix(&s->tmB, s, rows));
     if (!s->err.ptr) VIRS_TRY(s->err.alloc(sizeof(int), "error flag"));
     s->maps_rows = rows;
     return VIRS_OK;
@@ -449,7 +442,6 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.p = s->field[parity].ptr;
     a.q = s->field[parity ^ 1].ptr;
     a.code = s->code.as<uint8_t>();
-    a.bseg = s->bseg.as<uint32_t>();
     a.bmat = s->bmat.as<uint8_t>();
     a.bw = s->bw.as<float>();
     a.state = s->state.as<float>();
@@ -463,7 +455,6 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.ny = s->ny;
     a.nz = s->nz;
     a.px = s->px;
-    a.spr = s->spr;
     a.zc = s->zc;
     a.c2dt2 = s->c2dt2;
     a.inv_h2 = s->inv_h2;
@@ -495,7 +486,7 @@ PostArgs post_args(const virs_sim *s, int parity)
 cudaError_t launch_stencil(const virs_sim *s, int parity, cudaStream_t st)
 {
     if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
-    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC, &s->tmB};
+    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
     return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, step_args(s, parity), m, s->err.as<int>(), st);
 }
 
@@ -503,7 +494,7 @@ cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
 {
     cudaError_t e = launch_stencil(s, parity, st);
     if (e != cudaSuccess) return e;
-    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), s->depth > 0, st);
+    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), BND_UPDATE, st);
     if (e != cudaSuccess) return e;
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
@@ -547,7 +538,7 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
             err = launch_stencil(s, par, st);
             cudaEventRecord(ev[2 * i + 1], st);
             if (err == cudaSuccess)
-                err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), s->depth > 0, st);
+                err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), BND_UPDATE, st);
             cudaEventRecord(ev[2 * n + i], st);
             if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
         }
@@ -1488,7 +1479,6 @@ virs_status batch_build(virs_batch *b)
             VIRS_TRY(encode(&m.mapQ[k], dt, el, s->field[k].ptr, s, (uint32_t)tma_tile_x(), b->rows));
         }
         VIRS_TRY(encode(&m.mapC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), b->rows));
-        VIRS_TRY(encode_prefix(&m.mapB, s, b->rows));
         const int zc = b->planes > 0 ? b->planes : (s->zc > 0 ? s->zc : default_planes(s->nz));
         for (int par = 0; par < 2; ++par) {
             m.step[par] = step_args(s, par);
@@ -1793,8 +1783,8 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
             const uint64_t k = n - n0;
             VIRS_CUDA(cudaMemcpyAsync(A.segst.as<char>() + k * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
             cudaError_t e = launch_stencil(s, s->cur, st);
+            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), s->bidx.as<uint32_t>(), BND_KEEP, st);
             if (e == cudaSuccess) e = launch_keep_records(s->side.as<float4>(), A.segrec.as<float4>() + k * nb, nb, st);
-            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), s->bidx.as<uint32_t>(), true, st);
             if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, s->cur), st);
             if (e != cudaSuccess) return cuda_fail(e, "adjoint recomputation");
             s->cur ^= 1;
@@ -1818,8 +1808,11 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
                 a.p = T;
                 a.q = RR;
                 a.nhard = 0;
-                const TmaMaps m{&A.mapP[t], &A.mapQ[t ^ 1], &s->tmC, &s->tmB};
+                const TmaMaps m{&A.mapP[t], &A.mapQ[t ^ 1], &s->tmC};
                 e = launch_step_tma(VIRS_STORAGE_F32, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
+                // the free value A F - RR at the boundary voxels, which the
+                // stencil left alone
+                if (e == cudaSuccess) e = launch_boundary(VIRS_STORAGE_F32, a, s->bidx.as<uint32_t>(), BND_RECORD, st);
             }
             if (e == cudaSuccess)
                 e = launch_adj_fix(RR, T, s->bidx.as<uint32_t>(), s->side.as<float4>(), A.dbar.as<float>(),

@@ -68,11 +68,10 @@ constexpr int SEG = 128;              // voxels per boundary-prefix segment
 // ---- kernel argument blocks -------------------------------------------------
 
 struct StepArgs {
-    float4 *side;           // per boundary slot {free, p, p^{n-1}, 0}, written by the TMA stencil kernel
+    float4 *side;           // per boundary slot {free, p, p^{n-1}, 0}, kept by the boundary pass for the adjoint
     const void *p;          // p^n (storage type)
     void *q;                // in p^{n-1}, out p^{n+1}
     const uint8_t *code;
-    const uint32_t *bseg;   // exclusive boundary prefix per 128-voxel segment
     const uint8_t *bmat;
     const float *bw;
     float *state;           // [S][4][nb]
@@ -82,7 +81,7 @@ struct StepArgs {
     uint64_t nb;
     uint32_t nhard;
     uint32_t nsec;
-    uint32_t nx, ny, nz, px, spr;
+    uint32_t nx, ny, nz, px;
     int zc;                 // planes per block
     int form;               // VIRS_BOUNDARY_*
     float c2dt2, inv_h2;
@@ -106,7 +105,6 @@ struct alignas(64) BatchMember {
     CUtensorMap mapP[2];    // halo box over field[0] / field[1]
     CUtensorMap mapQ[2];    // tile box over field[0] / field[1]
     CUtensorMap mapC;       // cell codes
-    CUtensorMap mapB;       // boundary prefix
     StepArgs step[2];       // per parity: p = field[parity], q = field[parity ^ 1]
     PostArgs post[2];
     const uint32_t *bidx;
@@ -123,9 +121,9 @@ cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem
 // kernel launchers (kernels_step.cu)
 cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStream_t s);
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
-// side == true: finish the records the TMA stencil kernel wrote; false:
-// gather the neighbours and do the whole update (after the register kernel)
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, bool side, cudaStream_t s);
+// modes of the boundary pass (kernels_step.cu)
+enum { BND_UPDATE = 0, BND_KEEP = 1, BND_RECORD = 2 };
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, int mode, cudaStream_t s);
 int default_planes(uint32_t nz);
 
 // TMA-staged step (kernels_step_tma.cu)
@@ -133,7 +131,6 @@ struct TmaMaps {
     const CUtensorMap *p;   // p^n with halo box
     const CUtensorMap *q;   // p^{n-1}, tile box
     const CUtensorMap *c;   // cell codes, tile box
-    const CUtensorMap *b;   // boundary prefix, 4 segments x tile rows
 };
 cudaError_t launch_step_tma(int storage, int tile_rows, int depth, const StepArgs &a, const TmaMaps &m, int *err,
                             cudaStream_t s);

@@ -160,9 +160,18 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
 }
 
 // The compacted boundary pass (simulator_gpu.cu:105-150): one thread per
-// boundary voxel in list order; the leapfrog update (the stencil kernel
-// left these voxels untouched) and the filter correction.
-template <typename T, int MAXS>
+// boundary voxel in list order.  The stencil kernels left these voxels
+// untouched (p^{n-1} in place); the pass gathers the seven p values and
+// p^{n-1} of its voxel, computes the leapfrog update with the wall mirror,
+// then the filter correction.  Consecutive slots are consecutive voxels of
+// a row (floor, ceiling and y walls) or the same x of consecutive rows
+// (x walls), so the gathers of a warp share lines.
+//   BND_UPDATE  leapfrog + filters, the result written to p^{n+1}
+//   BND_KEEP    the same, and the record {free value, p, p^{n-1}} of the
+//               slot kept in a.side (the adjoint's recomputation)
+//   BND_RECORD  the record only: no filters, nothing written to the fields
+//               (the adjoint step, on adjoint fields)
+template <typename T, int MODE, int MAXS>
 __device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
 {
     using IO = Io<T>;
@@ -176,29 +185,18 @@ __device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t
     const float ce = IO::get(P[i]), qv = IO::get(Q[i]);
     float r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
                        IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
+    if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, ce, qv, 0.f);
+    if (MODE == BND_RECORD) return;
     r = boundary<MAXS>(a, r, ce, qv, slot);
     Q[i] = IO::put(r);
 }
 
-// finishes the record the TMA stencil kernel left for this slot
-template <typename T, int MAXS>
-__device__ __forceinline__ void boundary_record(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
-{
-    const float4 rec = __ldcs(a.side + slot);
-    const uint32_t ref = __ldg(bidx + slot);
-    const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
-    const size_t i = ((size_t)z * a.ny + y) * a.px + x;
-    T *Q = static_cast<T *>(a.q);
-    Q[i] = Io<T>::put(boundary<MAXS>(a, rec.x, rec.y, rec.z, slot));
-}
-
-template <typename T, bool SIDE, int MAXS>
+template <typename T, int MODE, int MAXS>
 __global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a, const uint32_t *__restrict bidx)
 {
     const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.nb) return;
-    if (SIDE) boundary_record<T, MAXS>(a, bidx, slot);
-    else boundary_voxel<T, MAXS>(a, bidx, slot);
+    boundary_voxel<T, MODE, MAXS>(a, bidx, slot);
 }
 
 // batched: thread g belongs to the last member whose first boundary index
@@ -223,7 +221,7 @@ __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__res
         else hi = mid - 1;
     }
     const BatchMember &b = mem[lo];
-    boundary_record<T, MAXS>(b.step[parity], b.bidx, g - b.first_bnd);
+    boundary_voxel<T, BND_UPDATE, MAXS>(b.step[parity], b.bidx, g - b.first_bnd);
 }
 
 template <typename T> __device__ __forceinline__ void post_body(const PostArgs &a)
@@ -288,13 +286,23 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
 
 namespace {
 
-template <typename T, bool SIDE>
+template <typename T, int MODE>
 void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, const uint32_t *bidx, cudaStream_t s)
 {
-    if (ns <= 1) k_boundary<T, SIDE, 1><<<g, 256, 0, s>>>(a, bidx);
-    else if (ns == 2) k_boundary<T, SIDE, 2><<<g, 256, 0, s>>>(a, bidx);
-    else if (ns <= 4) k_boundary<T, SIDE, 4><<<g, 256, 0, s>>>(a, bidx);
-    else k_boundary<T, SIDE, 0><<<g, 256, 0, s>>>(a, bidx);
+    if (MODE == BND_RECORD || ns <= 1) k_boundary<T, MODE, 1><<<g, 256, 0, s>>>(a, bidx);
+    else if (ns == 2) k_boundary<T, MODE, 2><<<g, 256, 0, s>>>(a, bidx);
+    else if (ns <= 4) k_boundary<T, MODE, 4><<<g, 256, 0, s>>>(a, bidx);
+    else k_boundary<T, MODE, 0><<<g, 256, 0, s>>>(a, bidx);
+}
+
+template <typename T> void boundary_by_mode(int mode, uint32_t ns, unsigned g, const StepArgs &a, const uint32_t *bidx,
+                                            cudaStream_t s)
+{
+    switch (mode) {
+    case BND_KEEP: boundary_by_sections<T, BND_KEEP>(ns, g, a, bidx, s); break;
+    case BND_RECORD: boundary_by_sections<T, BND_RECORD>(ns, g, a, bidx, s); break;
+    default: boundary_by_sections<T, BND_UPDATE>(ns, g, a, bidx, s); break;
+    }
 }
 
 template <typename T>
@@ -307,23 +315,14 @@ void boundary_batch_by_sections(uint32_t maxs, unsigned g, const BatchMember *me
 
 } // namespace
 
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, bool side, cudaStream_t s)
+cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, int mode, cudaStream_t s)
 {
     if (a.nb == 0) return cudaSuccess;
     const unsigned g = (unsigned)((a.nb + 255) / 256);
     switch (storage) {
-    case VIRS_STORAGE_F16:
-        if (side) boundary_by_sections<__half, true>(a.nsec, g, a, bidx, s);
-        else boundary_by_sections<__half, false>(a.nsec, g, a, bidx, s);
-        break;
-    case VIRS_STORAGE_BF16:
-        if (side) boundary_by_sections<__nv_bfloat16, true>(a.nsec, g, a, bidx, s);
-        else boundary_by_sections<__nv_bfloat16, false>(a.nsec, g, a, bidx, s);
-        break;
-    default:
-        if (side) boundary_by_sections<float, true>(a.nsec, g, a, bidx, s);
-        else boundary_by_sections<float, false>(a.nsec, g, a, bidx, s);
-        break;
+    case VIRS_STORAGE_F16: boundary_by_mode<__half>(mode, a.nsec, g, a, bidx, s); break;
+    case VIRS_STORAGE_BF16: boundary_by_mode<__nv_bfloat16>(mode, a.nsec, g, a, bidx, s); break;
+    default: boundary_by_mode<float>(mode, a.nsec, g, a, bidx, s); break;
     }
     return cudaGetLastError();
 }

@@ -4,26 +4,28 @@
 // differs: a block owns a TX x TY tile of (x, y) and streams it along z, and
 // every input plane reaches shared memory through the Tensor Memory
 // Accelerator instead of through registers:
-//   stage j holds  P(k+1)  the pressure plane above, with a one-voxel halo in
-//                          y and a 16-byte halo in x   (TY+2) x (TX+2*PAD)
-//                  Q(k)    p^{n-1} of the tile          TY x TX
-//                  C(k)    the cell codes of the tile    TY x TX bytes
-// for plane k = z0 - 2 + j.  The ring has D = L + 3 stages: planes z-1, z
-// and z+1 are in use while L more are in flight, each stage guarded by one
-// mbarrier that the TMA completes (complete_tx).  One thread issues the
-// copies; after the block-wide barrier that ends the use of a stage it is
-// refilled with the plane L+3 further on.  Out-of-range boxes (the y halo
-// above row 0 or below the last row, x past the padded row) are zero-filled
-// by the TMA.  Results go straight from registers to global memory with
-// streaming 16-byte stores.  No multicast: every copy reads this GPU's own
-// memory into this block's shared memory.
+//   stage j holds  P(k)  the pressure plane k with a one-voxel halo in y and
+//                        a 16-byte halo in x      (TY+2) x (TX+2*PAD)
+//                  Q(k)  p^{n-1} of the tile       TY x TX
+//                  C(k)  the cell codes of the tile TY x TX bytes
+// for plane k = z0 - 1 + j.  Each thread updates the V voxels of one
+// 16-byte vector; the centres of P(z-1) and P(z) stay in its registers, so
+// the ring has D = L + 2 stages: planes z and z+1 are in use while L more
+// are in flight, each stage guarded by one mbarrier that the TMA completes
+// (complete_tx).  One thread issues the copies; after the block-wide
+// barrier that ends the use of a stage it is refilled with the plane D
+// further on.  Out-of-range boxes (the y halo above row 0 or below the last
+// row, x past the padded row) are zero-filled by the TMA.  Results go
+// straight from registers to global memory with streaming 16-byte stores.
+// No multicast: every copy reads this GPU's own memory into this block's
+// shared memory.
 //
-// Boundary voxels (flag 2): their leapfrog value is computed here with the
-// staged neighbours and written, with p and p^{n-1}, to the voxel's slot of
-// the compacted boundary list; p^{n-1} stays in place.  The boundary pass
-// (k_boundary) then applies the filters to those records, coalesced, so the
-// only divergent work here is one warp scan and one 16-byte store per
-// boundary voxel.
+// Every voxel is first updated as air without wall neighbours (packed FP32
+// pairs).  Warps whose codes are not all zero then fix the other voxels
+// with selects: border voxels and boundary voxels (flag 2) keep p^{n-1},
+// walls take 0 and hard sources their value.  The boundary pass
+// (k_boundary) updates the boundary voxels afterwards from the p^n buffer,
+// which this kernel does not write.
 //
 // Every wait on an mbarrier is bounded; a wait that gives up sets *err and
 // the block returns (the host turns that into VIRS_E_TIMEOUT).
@@ -101,12 +103,10 @@ template <typename T, int TY> struct Stage {
     static constexpr uint32_t PB = Lay<T>::PW * (TY + 2) * sizeof(T);
     static constexpr uint32_t QB = TX * TY * sizeof(T);
     static constexpr uint32_t CB = TX * TY;
-    static constexpr uint32_t BB = 4 * TY * sizeof(uint32_t); // 4 prefix segments per tile row
     static constexpr uint32_t PBa = (PB + 127u) & ~127u;
     static constexpr uint32_t QBa = (QB + 127u) & ~127u;
     static constexpr uint32_t CBa = (CB + 127u) & ~127u;
-    static constexpr uint32_t BBa = (BB + 127u) & ~127u;
-    static constexpr uint32_t SB = PBa + QBa + CBa + BBa;
+    static constexpr uint32_t SB = PBa + QBa + CBa;
 };
 
 // the V cell codes of a thread (4 or 8 bytes)
@@ -146,9 +146,9 @@ template <typename T, int TY, int L> struct Tile {
     const StepArgs *a;
     unsigned char *smem;
     uint64_t *bars;
-    const CUtensorMap *mP, *mQ, *mC, *mB;
+    const CUtensorMap *mP, *mQ, *mC;
     int *err;
-    int x0, y0, z0, nst, row, sl, c0, t0, seg, seg4;
+    int x0, y0, z0, nst, row, sl, c0, t0;
     uint32_t j0;
     bool act, leader;
     float hardv;
@@ -167,12 +167,11 @@ template <typename T, int TY, int L> struct Tile {
         unsigned char *st = smem + (g % D) * S::SB;
         uint64_t *b = bars + (g % D);
         const bool full = j >= 1 && j <= nst - 2;
-        mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB + S::BB : 0u));
+        mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB : 0u));
         tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k);
         if (full) {
             tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
             tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
-            tma_load_3d(st + S::PBa + S::QBa + S::CBa, mB, b, seg4, y0, k);
         }
     }
 
@@ -220,46 +219,27 @@ template <typename T, int TY, int L> struct Tile {
             r[k] = o.x;
             r[k + 1] = o.y;
         }
-        // ... then the voxels with another code, recomputed in full
+        // ... then the voxels with another code.  Border voxels and boundary
+        // voxels keep p^{n-1} (the boundary pass updates the latter from
+        // the untouched p^n buffer), walls take 0 and hard sources their
+        // value: selects, no divergence.  Only air next to a wall outside
+        // the boundary layer (a grid without a sponge layer) needs the
+        // update with the mirror rule.
         if (__any_sync(FULL, code.any())) {
-            unsigned bmask = 0;
+            unsigned mirror = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 const uint32_t c = code.get(k);
-                if (c != 0u) {
-                    if (c >= CODE_HARD) {
-                        r[k] = c == CODE_NONE ? qv[k] : (c == CODE_WALL ? 0.f : hardv);
-                    } else {
-                        r[k] = leapfrog((uint8_t)c, cc[k], k == V - 1 ? right : cc[k + 1], k == 0 ? left : cc[k - 1],
-                                        yp[k], ym[k], zp[k], zm[k], qv[k], a->c2dt2, a->inv_h2);
-                        if (c & CODE_BND) bmask |= 1u << k;
-                    }
-                }
+                if (c & CODE_BND) r[k] = c == CODE_WALL ? 0.f : (c == CODE_HARD ? hardv : qv[k]);
+                else if (c != 0u) mirror |= 1u << k;
             }
-            // Boundary voxels: the record {free value, p, p^{n-1}} goes to
-            // their slot of the compacted list for the boundary pass, and
-            // p^{n-1} stays in place.  The lanes of a row cover consecutive
-            // voxels of one 128-voxel segment, so the slot is the segment's
-            // prefix (staged with the plane) plus a scan over the row's lanes.
-            if (!act) bmask = 0;
-            if (__any_sync(FULL, bmask != 0)) {
-                const int cnt = __popc(bmask);
-                int inc = cnt;
+            if (__any_sync(FULL, mirror != 0)) {
 #pragma unroll
-                for (int o = 1; o < LPR; o <<= 1) {
-                    const int t = __shfl_up_sync(FULL, inc, o, LPR);
-                    if (sl >= o) inc += t;
-                }
-                if (bmask) {
-                    const uint32_t *bs = reinterpret_cast<const uint32_t *>(s0 + S::PBa + S::QBa + S::CBa);
-                    uint64_t slot = (uint64_t)bs[row * 4 + (seg - seg4)] + (uint64_t)(inc - cnt);
-#pragma unroll
-                    for (int k = 0; k < V; ++k)
-                        if (bmask & (1u << k)) {
-                            a->side[slot++] = make_float4(r[k], cc[k], qv[k], 0.f);
-                            r[k] = qv[k];
-                        }
-                }
+                for (int k = 0; k < V; ++k)
+                    if (mirror & (1u << k))
+                        r[k] = leapfrog((uint8_t)code.get(k), cc[k], k == V - 1 ? right : cc[k + 1],
+                                        k == 0 ? left : cc[k - 1], yp[k], ym[k], zp[k], zm[k], qv[k], a->c2dt2,
+                                        a->inv_h2);
             }
         }
         if (act) IO::st(out, r);
@@ -270,8 +250,8 @@ template <typename T, int TY, int L> struct Tile {
 };
 
 // One tile (bx, by, bz) of one simulation.  Stage j of the tile holds the
-// plane k = z0 - 1 + j: P(k) with its halo, and for k in [z0, z1) also Q(k),
-// the codes of plane k and the row prefixes of the boundary list.  The
+// plane k = z0 - 1 + j: P(k) with its halo, and for k in [z0, z1) also Q(k)
+// and the codes of plane k.  The
 // centres of P(z-1) and P(z) stay in registers from the previous planes, so
 // plane z reads the stage of z (halo neighbours, Q, codes) and the centre
 // of the stage of z+1; the ring has D = L + 2 slots.  The plane loop is
@@ -282,8 +262,8 @@ template <typename T, int TY, int L> struct Tile {
 // tiles (the batched kernel).  Returns false when a bounded wait gave up.
 template <typename T, int TY, int L>
 __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
-                                          const CUtensorMap *mC, const CUtensorMap *mB, int bx, int by, int bz,
-                                          int *err, unsigned char *smem, uint64_t *bars, uint32_t &jg)
+                                          const CUtensorMap *mC, int bx, int by, int bz, int *err, unsigned char *smem,
+                                          uint64_t *bars, uint32_t &jg)
 {
     using G = Lay<T>;
     using S = Stage<T, TY>;
@@ -300,7 +280,6 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.mP = mP;
     t.mQ = mQ;
     t.mC = mC;
-    t.mB = mB;
     t.err = err;
     t.row = threadIdx.y * G::RPW + lane / LPR; // row of the tile
     t.sl = lane % LPR;                         // lane within the row
@@ -314,8 +293,6 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.act = x < (int)a.px && y < (int)a.ny;
     t.leader = tid == 0;
     t.j0 = jg;
-    t.seg = t.x0 / SEG;
-    t.seg4 = t.seg & ~3; // prefix box starts on a 16-byte boundary
     t.c0 = (t.row + 1) * PW + PAD + t.sl * V; // this thread's first voxel in a halo box
     t.t0 = t.row * TX + t.sl * V;            // ... and in a tile box
     t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
@@ -374,15 +351,14 @@ template <typename T, int TY, int L>
 __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k_step_tma(const __grid_constant__ StepArgs a,
                                                                         const __grid_constant__ CUtensorMap mP,
                                                                         const __grid_constant__ CUtensorMap mQ,
-                                                                        const __grid_constant__ CUtensorMap mC,
-                                                                        const __grid_constant__ CUtensorMap mB, int *err)
+                                                                        const __grid_constant__ CUtensorMap mC, int *err)
 {
     constexpr int D = L + 2;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
     uint32_t jg = 0;
-    step_tile<T, TY, L>(a, &mP, &mQ, &mC, &mB, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
+    step_tile<T, TY, L>(a, &mP, &mQ, &mC, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
 }
 
 // Many simulations in one launch: the blocks walk the concatenated tile
@@ -406,8 +382,8 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k
         const uint64_t local = w - b.first_tile;
         const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / ((uint64_t)b.gx * b.gy));
         __syncthreads(); // every thread is done with the previous tile's stages
-        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, &b.mapB, bx, by, bz,
-                                 err, smem, bars, jg))
+        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, bx, by, bz, err, smem,
+                                 bars, jg))
             return;
     }
 }
@@ -427,7 +403,7 @@ cudaError_t launch3(const StepArgs &a, const TmaMaps &m, int *err, cudaStream_t 
     const unsigned gx = (a.px + TX - 1) / TX;
     const unsigned gz = (a.nz - 2 + a.zc - 1) / a.zc;
     kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, block_threads<T, TY>() / 32), sm, s>>>(a, *m.p, *m.q, *m.c,
-                                                                                             *m.b, err);
+                                                                                             err);
     return cudaGetLastError();
 }
 
