@@ -221,9 +221,12 @@ virs_status default_filters(virs_sim *s)
     return VIRS_OK;
 }
 
+// the filter states, [2(S+1)][nb] (see step_common.cuh)
+size_t state_bytes(const virs_sim *s) { return std::max<uint64_t>(s->nb, 1) * (s->nsec + 1) * 2 * sizeof(float); }
+
 virs_status alloc_states(virs_sim *s)
 {
-    VIRS_TRY(s->state.alloc(std::max<uint64_t>(s->nb, 1) * s->nsec * 4 * sizeof(float), "filter states"));
+    VIRS_TRY(s->state.alloc(state_bytes(s), "filter states"));
     s->graph_dirty = true;
     ++s->gen;
     return VIRS_OK;
@@ -1722,7 +1725,7 @@ VIRS_EXPORT virs_status virs_forward_checkpointed(virs_sim *s, uint64_t steps, u
     A.steps = steps;
     A.every = every;
     A.nck = (steps + every - 1) / every;
-    const size_t fb = s->nvox * 4, sb = std::max<uint64_t>(s->nb, 1) * s->nsec * 4 * 4;
+    const size_t fb = s->nvox * 4, sb = state_bytes(s);
     VIRS_TRY(A.ckp.alloc(A.nck * fb, "checkpoints"));
     VIRS_TRY(A.ckq.alloc(A.nck * fb, "checkpoints"));
     VIRS_TRY(A.cks.alloc(A.nck * sb, "checkpoints"));
@@ -1749,12 +1752,14 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
     VIRS_TRY(wait_done(s));
     cudaStream_t st = s->stream;
     const uint64_t steps = A.steps, every = A.every, nb = s->nb;
-    const size_t fb = s->nvox * 4, sb = std::max<uint64_t>(nb, 1) * s->nsec * 4 * 4;
+    // forward states (shared cascade layout) and the adjoint's own state
+    // adjoints, four per section
+    const size_t fb = s->nvox * 4, sb = state_bytes(s), sba = std::max<uint64_t>(nb, 1) * s->nsec * 4 * 4;
     const uint32_t ncoef = s->nmat * s->nsec * 5;
     VIRS_TRY(A.segrec.alloc(every * std::max<uint64_t>(nb, 1) * sizeof(float4), "adjoint segment records"));
     VIRS_TRY(A.segst.alloc(every * sb, "adjoint segment states"));
     for (int k = 0; k < 2; ++k) VIRS_TRY(A.buf[k].alloc(fb, "adjoint field"));
-    VIRS_TRY(A.ast.alloc(sb, "adjoint filter states"));
+    VIRS_TRY(A.ast.alloc(sba, "adjoint filter states"));
     VIRS_TRY(A.dbar.alloc(std::max<uint64_t>(nb, 1) * 4, "adjoint boundary terms"));
     VIRS_TRY(A.cq.alloc(std::max<uint64_t>(nb, 1) * 4, "adjoint boundary terms"));
     VIRS_TRY(A.grad.alloc(ncoef * sizeof(double), "coefficient gradients"));

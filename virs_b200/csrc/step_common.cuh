@@ -188,6 +188,15 @@ __device__ __forceinline__ float correct(const StepArgs &a, float r, float d, fl
     return __double2float_rn(__ddiv_rn(num, __dadd_rn(1.0, ac)));
 }
 
+// Filter states.  In a cascade the output of section q is the input of
+// section q+1, so the two past outputs a DF1 section keeps (y[n-1], y[n-2])
+// are the two past inputs of the next one: S sections need 2(S+1) values,
+// X_q[n-1] and X_q[n-2] for the input X_0 = p - p^{n-1} and the outputs
+// X_{q+1} = y_q.  They are stored [2(S+1)][nb] (entry 2q holds X_q[n-1],
+// 2q+1 holds X_q[n-2]).  This is the reference's four states per section
+// (simulator_gpu.cu:126-146) without the copies, so every value, and the
+// result, is the same.
+
 // up to MAXS sections, fully unrolled: every state, the material and the
 // weight are loaded before any arithmetic, so one slot costs two dependent
 // memory round trips (states/material, then coefficients), not one per
@@ -200,30 +209,32 @@ __device__ __forceinline__ float boundary_unrolled(const StepArgs &a, float r, f
     float *st = a.state + slot;
     const uint32_t m = __ldg(a.bmat + slot);
     const float wf = __ldg(a.bw + slot);
-    float s[MAXS][4];
+    float h[MAXS + 1][2];
 #pragma unroll
-    for (int q = 0; q < MAXS; ++q)
-        if (q < (int)ns)
+    for (int q = 0; q <= MAXS; ++q)
+        if (q <= (int)ns)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) s[q][j] = st[(uint64_t)(4 * q + j) * nb];
+            for (int j = 0; j < 2; ++j) h[q][j] = st[(uint64_t)(2 * q + j) * nb];
     const float *kc = a.coef + (uint64_t)m * ns * 5;
     const float d = __fsub_rn(ce, qv);
-    float in = d;
+    float in = d, last = h[0][0];
 #pragma unroll
     for (int q = 0; q < MAXS; ++q) {
         if (q < (int)ns) {
             const float *kq = kc + 5 * q;
-            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), s[q][0]));
-            y = __fmaf_rn(__ldg(kq + 2), s[q][1], y);
-            y = __fmaf_rn(-__ldg(kq + 3), s[q][2], y);
-            y = __fmaf_rn(-__ldg(kq + 4), s[q][3], y);
-            st[(uint64_t)(4 * q + 0) * nb] = in;
-            st[(uint64_t)(4 * q + 1) * nb] = s[q][0];
-            st[(uint64_t)(4 * q + 2) * nb] = y;
-            st[(uint64_t)(4 * q + 3) * nb] = s[q][2];
+            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), h[q][0]));
+            y = __fmaf_rn(__ldg(kq + 2), h[q][1], y);
+            y = __fmaf_rn(-__ldg(kq + 3), h[q + 1][0], y);
+            y = __fmaf_rn(-__ldg(kq + 4), h[q + 1][1], y);
+            st[(uint64_t)(2 * q + 0) * nb] = in;
+            st[(uint64_t)(2 * q + 1) * nb] = h[q][0];
             in = y;
+            last = h[q + 1][0];
         }
     }
+    // the history of the last output
+    st[(uint64_t)(2 * ns + 0) * nb] = in;
+    st[(uint64_t)(2 * ns + 1) * nb] = last;
     return correct(a, r, d, in, qv, wf);
 }
 
@@ -235,18 +246,21 @@ __device__ __noinline__ float boundary_loop(const StepArgs &a, float r, float ce
     const uint64_t nb = a.nb;
     const float *kc = a.coef + (uint64_t)__ldg(a.bmat + slot) * a.nsec * 5;
     float *st = a.state + slot;
-    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5, st += 4 * nb) {
-        const float s0 = st[0], s1 = st[nb], s2 = st[2 * nb], s3 = st[3 * nb];
-        float y = __fmaf_rn(__ldg(kc), in, __fmul_rn(__ldg(kc + 1), s0));
-        y = __fmaf_rn(__ldg(kc + 2), s1, y);
-        y = __fmaf_rn(-__ldg(kc + 3), s2, y);
-        y = __fmaf_rn(-__ldg(kc + 4), s3, y);
+    float x1 = st[0], x2 = st[nb];
+    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5, st += 2 * nb) {
+        const float y1 = st[2 * nb], y2 = st[3 * nb];
+        float y = __fmaf_rn(__ldg(kc), in, __fmul_rn(__ldg(kc + 1), x1));
+        y = __fmaf_rn(__ldg(kc + 2), x2, y);
+        y = __fmaf_rn(-__ldg(kc + 3), y1, y);
+        y = __fmaf_rn(-__ldg(kc + 4), y2, y);
         st[0] = in;
-        st[nb] = s0;
-        st[2 * nb] = y;
-        st[3 * nb] = s2;
+        st[nb] = x1;
         in = y;
+        x1 = y1;
+        x2 = y2;
     }
+    st[0] = in;
+    st[nb] = x1;
     return correct(a, r, d, in, qv, __ldg(a.bw + slot));
 }
 
