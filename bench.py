@@ -283,7 +283,7 @@ def cpu_sample(shape, steps_budget_s, threads):
     osc.run(2, state=st, step0=1)
     per_step = (time.perf_counter() - t0) / 2
     # grow the crop to fill the budget: steps of the crop until ~budget
-    k = max(2, min(200, int(steps_budget_s / max(per_step, 1e-6))))
+    k = max(2, min(20000, int(steps_budget_s / max(per_step, 1e-6))))
     t0 = time.perf_counter()
     osc.run(k, state=st, step0=3)
     dt = time.perf_counter() - t0

@@ -228,6 +228,7 @@ class _RunArgs(C.Structure):
         ("steps", C.c_uint64), ("step0", C.c_uint64), ("ir_stride", C.c_uint64),
         ("ir", C.c_void_p), ("p", C.c_void_p), ("pprev", C.c_void_p), ("state", C.c_void_p),
         ("ir64", C.c_void_p),
+        ("storage", C.c_int32), ("scale", C.c_float),
     ]
 
 
@@ -245,7 +246,7 @@ class Scene:
 
     def __init__(self, shape, flags, bidx, bmat, bw, coef32, n_sections, *, coef64=None,
                  hard=None, src_idx=(), src_sig=None, rcv_idx=(), consts=None, consts64=None,
-                 mix_y=0.1, mix_d=0.9, gain=float(np.float32(0.4)), form=0):
+                 mix_y=0.1, mix_d=0.9, gain=float(np.float32(0.4)), form=0, storage=0, scale=1.0):
         self.shape = tuple(int(s) for s in shape)
         self.flags = np.ascontiguousarray(flags, np.uint8)
         self.bidx = np.ascontiguousarray(bidx, np.uint32)
@@ -266,6 +267,8 @@ class Scene:
         self.consts64 = consts64      # (c2dt2, inv_h2, K) float64
         self.mix_y, self.mix_d, self.gain = float(mix_y), float(mix_d), float(gain)
         self.form = int(form)
+        self.storage = int(storage)   # FP32 run: 0 FP32 fields, 1 FP16, 2 BF16 (rounded as the GPU stores them)
+        self.scale = float(scale)     # 16-bit storage: fields hold scale * p (a power of two)
 
     def _args(self, steps, step0, ir, p, pp, st, f64):
         a = _RunArgs()
@@ -286,6 +289,7 @@ class Scene:
         a.n_rcv, a.rcv_idx = self.rcv_idx.size, _ptr(self.rcv_idx)
         a.steps, a.step0, a.ir_stride = steps, step0, steps
         a.ir, a.p, a.pprev, a.state = _ptr(ir), _ptr(p), _ptr(pp), _ptr(st)
+        a.storage, a.scale = self.storage, self.scale
         return a
 
     def run64(self, steps):
@@ -330,6 +334,14 @@ class Scene:
         if rc != 0:
             raise MemoryError("oracle run: allocation failed")
         return ir[: self.rcv_idx.size]
+
+
+def round16(x, storage: int):
+    """Values rounded as the 16-bit field storage stores them (1 FP16, 2 BF16)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().vo_round16(x.ctypes.data, out.ctypes.data, C.c_uint64(x.size), C.c_int32(storage))
+    return out
 
 
 def energy(shape, flags, p, pprev, lambda2: float) -> float:

@@ -429,7 +429,70 @@ typedef struct vo_run_args {
     void *pprev;                   /* in/out p^{n-1}                       */
     void *state;                   /* in/out [nb][S][4]                    */
     double *ir64;                  /* FP64 run: IR in double (may be NULL) */
+    int32_t storage;               /* FP32 run: 0 FP32 fields, 1 FP16, 2 BF16 */
+    float scale;                   /* 16-bit storage: fields hold scale * p  */
 } vo_run_args;
+
+/* 16-bit field storage, as the GPU path stores it: every value written to
+ * a field is rounded to the nearest FP16 / BF16 value (ties to even; FP16
+ * keeps its subnormals, overflow gives infinity); loads are exact.  The
+ * fields hold scale * p with a power-of-two scale, so the FP32 arithmetic
+ * on them is the same as on p, scaled. */
+static inline float vo_round_bf16(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) {            /* inf stays, NaN quiet */
+        if (u & 0x007fffffu) u |= 0x00400000u;
+        u &= 0xffff0000u;
+    } else {
+        u += 0x7fffu + ((u >> 16) & 1u);
+        u &= 0xffff0000u;
+    }
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+static inline float vo_round_f16(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    const uint32_t sign = u & 0x80000000u, a = u & 0x7fffffffu;
+    if (a >= 0x7f800000u) return x;                       /* inf, NaN */
+    if (a >= 0x477ff000u) {                               /* >= 65520: rounds to inf */
+        u = sign | 0x7f800000u;
+        memcpy(&x, &u, 4);
+        return x;
+    }
+    if (a < 0x38800000u) {                                /* below 2^-14: FP16 subnormal */
+        float m;
+        memcpy(&m, &a, 4);
+        const float q = nearbyintf(m * 16777216.0f);      /* multiples of 2^-24, ties to even */
+        float r = q * (1.0f / 16777216.0f);
+        uint32_t v;
+        memcpy(&v, &r, 4);
+        v |= sign;
+        memcpy(&x, &v, 4);
+        return x;
+    }
+    uint32_t v = a + 0xfffu + ((a >> 13) & 1u);           /* 23 -> 10 mantissa bits */
+    v = (v & ~0x1fffu) | sign;
+    memcpy(&x, &v, 4);
+    return x;
+}
+
+/* the storage rounding on its own (tests) */
+VO_API void vo_round16(const float *in, float *out, uint64_t n, int32_t storage)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = storage == 1 ? vo_round_f16(in[i]) : storage == 2 ? vo_round_bf16(in[i]) : in[i];
+}
+
+static void vo_round_field(float *f, uint64_t n, int storage)
+{
+    if (storage == 0) return;
+#pragma omp parallel for num_threads(vo_get_threads()) schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) f[i] = storage == 1 ? vo_round_f16(f[i]) : vo_round_bf16(f[i]);
+}
 
 static inline float vsel(const uint8_t *fl, const float *p, uint64_t n, float c)
 {
@@ -537,23 +600,30 @@ VO_API int vo_run_f32(const vo_run_args *a)
     if (a->pprev) memcpy(b1, a->pprev, N * sizeof(float));
     if (a->state) memcpy(st, a->state, nst * sizeof(float));
     float *pc = b0, *pp = b1, *pn = b2;
+    const int sto = a->storage;
+    const float scale = sto ? a->scale : 1.f, inv_scale = 1.f / scale;
     /* the next buffer starts as the reference's p_next would: it holds the
      * values the kernel never writes (the domain border stays 0). */
     for (uint64_t n = 0; n < a->steps; ++n) {
         const uint64_t sn = a->step0 + n;
-        const float hard = sn < a->n_hard ? a->hard[sn] : 0.f;
+        const float hard = sn < a->n_hard ? a->hard[sn] * scale : 0.f;
         interior_f32(a, pc, pp, pn, hard);
         if (a->nb) boundary_f32(a, pc, pp, pn, st);
-        ftz_on();
+        vo_round_field(pn, N, sto);
         for (uint32_t s = 0; s < a->n_src; ++s) {
             const uint64_t i = a->src_idx[s];
-            pn[i] = pn[i] + sig_at(a, s, sn);
+            const float v = sig_at(a, s, sn) * scale;   /* scaled on the host, without FTZ */
+            ftz_on();
+            pn[i] = pn[i] + v;
+            ftz_off();
+            if (sto) pn[i] = sto == 1 ? vo_round_f16(pn[i]) : vo_round_bf16(pn[i]);
         }
-        ftz_off();
         /* rotation (simulator_gpu.cu:292-293): prev <- curr <- next */
         float *t = pp; pp = pc; pc = pn; pn = t;
+        ftz_on();
         for (uint32_t r = 0; r < a->n_rcv; ++r)
-            a->ir[(uint64_t)r * a->ir_stride + n] = pc[a->rcv_idx[r]];
+            a->ir[(uint64_t)r * a->ir_stride + n] = sto ? pc[a->rcv_idx[r]] * inv_scale : pc[a->rcv_idx[r]];
+        ftz_off();
     }
     if (a->p) memcpy(a->p, pc, N * sizeof(float));
     if (a->pprev) memcpy(a->pprev, pp, N * sizeof(float));

@@ -273,3 +273,19 @@ def test_fp64_adjoint_matches_finite_differences(form, courant):
         dn = float(osc.src_sig[s, n])
         setv(np.float32(base))
         assert abs((lp - lm) / (up - dn) - gs[s, n]) <= 1e-6 * abs(gs[s, n])
+
+
+def test_storage_rounding_matches_ieee_conversions():
+    """The oracle's 16-bit storage rounding: FP16 as IEEE binary16 (ties to
+    even, subnormals, overflow to infinity), BF16 as the top half of the
+    FP32 word rounded to nearest even."""
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(100000).astype(np.float32) * np.float32(10.0) ** rng.integers(-12, 6, 100000).astype(np.float32)
+    x = np.concatenate([x, np.array([65504, 65519.99, 65520, -65520, 6.1e-5, 6.0e-5, 3e-8, 2.98e-8, 1e-9, 0.0, -0.0,
+                                     np.inf, -np.inf], np.float32)]).astype(np.float32)
+    with np.errstate(over="ignore"):
+        want16 = x.astype(np.float16).astype(np.float32)
+    assert np.array_equal(oracle.round16(x, 1).view(np.uint32), want16.view(np.uint32))
+    u = x.view(np.uint32).astype(np.uint64)
+    wantb = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    assert np.array_equal(oracle.round16(x, 2).view(np.uint32), wantb)

@@ -264,6 +264,41 @@ def test_16bit_storage_error_is_bounded(storage):
     sim.close()
 
 
+def _storage_scale(sc) -> float:
+    """The per-run scale the library chooses: the largest source amplitude
+    maps to about 1024, rounded to a power of two."""
+    peak = float(np.abs(sc.src_sig).max()) if sc.src_sig is not None and np.size(sc.src_sig) else 0.0
+    if sc.hard is not None:
+        peak = max(peak, float(np.abs(sc.hard).max()))
+    return float(2.0 ** np.round(np.log2(1024.0 / peak))) if peak > 0 else 1.0
+
+
+@pytest.mark.parametrize("storage", [capi.STORAGE_F16, capi.STORAGE_BF16])
+@pytest.mark.parametrize("depth", [0, 2])
+def test_16bit_storage_bit_exact(storage, depth):
+    """16-bit storage against the oracle run that rounds every stored value
+    the same way (FP32 update, the per-run scale): receiver samples and the
+    final fields match bit for bit, for the register and the TMA kernels."""
+    sc = scenes.plain_small(steps=400)
+    g = oracle_grid(sc)
+    scale = _storage_scale(sc)
+    osc = oracle_scene(sc, g)
+    osc.storage, osc.scale = storage, scale
+    n = int(np.prod(g["shape"]))
+    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
+    want = osc.run(sc.steps, state=st)
+    sim, _ = scenes.build_simulation(sc, storage=storage, storage_scale=scale)
+    sim.set_tiling(8, 0, depth)
+    sim.run(sc.steps)
+    got = sim.ir()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), np.abs(got - want).max()
+    p = sim.pressure().reshape(-1)
+    want_p = st[0] * np.float32(1.0 / scale)                    # unscaled on the GPU with flush-to-zero
+    want_p[np.abs(want_p) < np.finfo(np.float32).tiny] *= np.float32(0.0)
+    assert np.array_equal(p.view(np.uint32), want_p.view(np.uint32))
+    sim.close()
+
+
 def test_error_statuses():
     sim = capi.Simulation()
     with pytest.raises(capi.VirsError) as e:
