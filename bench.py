@@ -158,6 +158,18 @@ def gpu_uuid(dev):
     return u if u.startswith("GPU-") else "GPU-" + u
 
 
+def max_over_ranks(ms: float, dist, device: str) -> float:
+    """The slowest rank's time: every rank takes part, and every rank gets
+    the maximum (a no-op without a process group)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
 def time_run(sim, steps, stream):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -185,11 +197,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         dist.barrier()
     with Clocks(gpu_uuid(dev)) as clk:
         ms = time_run(sim, args.steps, stream)
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, f"cuda:{dev}")
     out = {"ms": ms, "clocks": clk.summary(), "meta": meta,
            "tiling": {"tile_rows": tiling.tile_rows, "planes_per_block": tiling.planes_per_block,
                       "pipeline_depth": tiling.pipeline_depth}}
@@ -220,10 +228,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         e1.synchronize()
         wall = (time.perf_counter() - t0) * 1e3
         ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, dist, f"cuda:{dev}")
         out["e2e_ms"] = ems
         out["e2e_wall_ms"] = wall
         out["h2d"] = 4 * nsrc
@@ -233,7 +238,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     return out
 
 
-def bench_batch(storage, args, stream, dev):
+def bench_batch(storage, args, stream, dev, dist=None):
     """The batched workload: 64 source positions in a 256^3 room plus 16 rooms
     of 96^3..320^3, advanced by three launches per step (virs_batch)."""
     import torch
@@ -248,11 +253,13 @@ def bench_batch(storage, args, stream, dev):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     e0.record(stream)
     b.run(steps, stream.cuda_stream)
     e1.record(stream)
     e1.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
     b.synchronize()
     ok = all(bool(np.isfinite(s.ir()).all()) for s in sims)
     b.close()
@@ -323,7 +330,7 @@ def run_virs(args):
         }
     if args.batch_steps:
         for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):
-            rb = bench_batch(st, args, stream, dev)
+            rb = bench_batch(st, args, stream, dev, dist)
             rb["value"] *= world
             variants[name] = rb
         variants["bf16_batched_vs_f32_plain"] = None   # filled below

@@ -297,6 +297,33 @@ virs_status virs_batch_set_tiling(virs_batch *batch, int tile_rows, int planes_p
 virs_status virs_batch_autotune(virs_batch *batch, uint32_t trial_steps, virs_tiling *best);
 virs_status virs_batch_destroy(virs_batch *batch);
 
+/* ---- IR post-processing ----------------------------------------------------- */
+
+/* Replaces designChebyshevI_LP with distributeDCGain
+ * (src/util/downsampling_filter_iir.cpp:11-193): a Chebyshev-I low-pass for
+ * anti-aliasing before resampling, as second-order sections
+ * sos [n][6] = {b0, b1, b2, a0, a1, a2} (a0 = 1), DC gain 1.  fstop <= 0
+ * means min(0.499 fs, 1.15 fc).  The sections equal the reference's bit for
+ * bit.  VIRS_E_ARG for invalid specs or when more than max_sections are
+ * needed (*n_sections is not written then). */
+virs_status virs_design_chebyshev_lowpass(double fs, double fc, double fstop, double ripple_db, double atten_db,
+                                          double *sos, uint32_t max_sections, uint32_t *n_sections);
+
+/* Replaces the IR post-processing of Simulator::simulate
+ * (simulator.cpp:1029-1080), which resamples the receiver trace from the
+ * simulation rate to 48 kHz with a library resampler (kfr) and divides it
+ * by its peak.  Here, on the GPU, for every receiver over the steps run so
+ * far: the cascade `sos` (n_sections <= 32, 0 = none) in FP64 transposed
+ * direct form II at the simulation rate, linear interpolation at k / rate
+ * (the interpolation written at simulator.cpp:1046-1057; the last sample
+ * is held past the end), and, if normalize, division by that receiver's
+ * peak magnitude (a silent receiver stays zero).  The output length is
+ * (uint64_t)(rate * steps * dt) as at simulator.cpp:1037-1038.
+ * out [n_receivers][*out_len]; out == NULL only reports *out_len;
+ * VIRS_E_ARG when capacity < *out_len. */
+virs_status virs_postprocess_ir(virs_sim *sim, double rate, const double *sos, uint32_t n_sections, int normalize,
+                                float *out, uint64_t capacity, uint64_t *out_len);
+
 /* Failure-path self test (no reference counterpart): launches a kernel that
  * waits `limit` microseconds (1..2^20) on an mbarrier that nothing completes,
  * with the bounded wait of the step kernels; returns VIRS_E_TIMEOUT when the

@@ -82,6 +82,16 @@ def lib():
         L.vo_adjoint_f64.argtypes = [C.c_void_p]
         L.vo_energy_f32.restype = C.c_double
         L.vo_energy_f32.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _u8p, _f32p, _f32p, C.c_double]
+        L.vo_cheby_design.restype = C.c_int
+        L.vo_cheby_design.argtypes = [C.c_double] * 5 + [C.c_void_p, C.c_int]
+        L.vo_sos_df2t.restype = None
+        L.vo_sos_df2t.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64]
+        L.vo_resample_len.restype = C.c_uint64
+        L.vo_resample_len.argtypes = [C.c_double, C.c_uint64, C.c_float]
+        L.vo_resample.restype = None
+        L.vo_resample.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_double, C.c_void_p, C.c_uint64, C.c_int]
+        L.vo_round16.restype = None
+        L.vo_round16.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32]
         L.vo_set_threads.argtypes = [C.c_int]
         L.vo_get_threads.restype = C.c_int
         _lib = L
@@ -336,6 +346,38 @@ class Scene:
         return ir[: self.rcv_idx.size]
 
 
+def cheby_design(fs, fc, fstop=0.0, ap_db=0.5, as_db=90.0):
+    """The anti-alias Chebyshev-I sections [n][6] (ValueError for invalid specs)."""
+    out = np.zeros((64, 6), np.float64)
+    n = lib().vo_cheby_design(fs, fc, fstop, ap_db, as_db, out.ctypes.data, 64)
+    if n < 0:
+        raise ValueError("invalid Chebyshev specification")
+    return out[:n].copy()
+
+
+def sos_df2t(sos, x):
+    """One channel through the cascade (FP64 transposed direct form II)."""
+    s = np.ascontiguousarray(sos, np.float64).reshape(-1, 6)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty_like(x)
+    lib().vo_sos_df2t(s.ctypes.data, s.shape[0], x.ctypes.data, y.ctypes.data, x.size)
+    return y
+
+
+def postprocess(ir, dt, rate=48000.0, sos=None, normalize=True):
+    """The receiver traces [R][steps] filtered, resampled to `rate` and
+    (optionally) peak-normalised, as virs_postprocess_ir defines it."""
+    ir = np.ascontiguousarray(ir, np.float32).reshape(-1, np.shape(ir)[-1])
+    steps = ir.shape[1]
+    n = int(lib().vo_resample_len(rate, steps, dt))
+    sim_rate = float(np.float32(1.0) / np.float32(dt))
+    out = np.zeros((ir.shape[0], n), np.float32)
+    for r in range(ir.shape[0]):
+        x = ir[r] if sos is None or len(sos) == 0 else sos_df2t(sos, ir[r])
+        lib().vo_resample(x.ctypes.data, steps, sim_rate, rate, out[r].ctypes.data, n, int(normalize))
+    return out
+
+
 def round16(x, storage: int):
     """Values rounded as the 16-bit field storage stores them (1 FP16, 2 BF16)."""
     x = np.ascontiguousarray(x, np.float32)
@@ -367,6 +409,20 @@ def ref_host(fast: bool = False):
     L.ref_sat_batch.argtypes = [_f32p, _f32p, C.c_uint64, _u8p]
     L.ref_highpass.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
     L.ref_lowpass.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
+    return L
+
+
+def ref_dsp():
+    """The reference's anti-alias filter design and cascade
+    (src/util/downsampling_filter_iir.cpp), compiled as it is."""
+    p = REF_DIR / "libref_dsp.so"
+    if not p.exists():
+        return None
+    L = C.CDLL(str(p))
+    L.ref_cheby_design.restype = C.c_int
+    L.ref_cheby_design.argtypes = [C.c_double] * 5 + [C.c_void_p, C.c_int]
+    L.ref_cheby_process.restype = None
+    L.ref_cheby_process.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64]
     return L
 
 

@@ -916,3 +916,158 @@ VO_API double vo_energy_f32(uint64_t nx, uint64_t ny, uint64_t nz, const uint8_t
             }
     return kin + lambda2 * pot;
 }
+
+/* ------------------------------------------------------------------------ */
+/* IR post-processing: anti-alias cascade, resampling, normalisation          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { double re, im; } vo_cplx;
+
+static int vo_cmp_imag(const void *a, const void *b)
+{
+    const double x = ((const vo_cplx *)a)->im, y = ((const vo_cplx *)b)->im;
+    return (x > y) - (x < y);
+}
+
+/* Chebyshev-I low-pass as second-order sections, restating
+ * designChebyshevI_LP (src/util/downsampling_filter_iir.cpp:58-193) and
+ * distributeDCGain (:11-56): bilinear prewarping, order from the ripple /
+ * attenuation specs, the N analogue poles sorted by imaginary part and
+ * taken two at a time (each pair's first pole with its conjugate gives a
+ * section with zeros at z = -1; a last unpaired pole a first-order section),
+ * then the DC gain spread over the sections in long double.  sos out
+ * [max][6] {b0, b1, b2, a0, a1, a2}; returns the section count, -1 for
+ * invalid specs, -2 when max is too small. */
+VO_API int vo_cheby_design(double fs, double fc, double fstop, double ap_db, double as_db, double *sos, int max)
+{
+    if (fs <= 0 || fc <= 0 || fc >= 0.5 * fs) return -1;
+    if (fstop <= 0.0) fstop = fmin(0.499 * fs, 1.15 * fc);
+    if (fstop <= fc) return -1;
+    const double T = 1.0 / fs;
+    const double wp = 2.0 / T * tan(M_PI * (fc / fs));
+    const double ws = 2.0 / T * tan(M_PI * (fstop / fs));
+    const double W = 2.0 / T;
+    const double ep = sqrt(pow(10.0, ap_db / 10.0) - 1.0);
+    const double x = sqrt((pow(10.0, as_db / 10.0) - 1.0) / (pow(10.0, ap_db / 10.0) - 1.0));
+    const double num = log(x + sqrt(x * x - 1.0));                 /* acosh */
+    const double r = ws / wp;
+    const double den = log(r + sqrt(r * r - 1.0));
+    int N = (int)ceil(num / den);
+    if (N < 1) N = 1;
+    const double ie = 1.0 / ep;
+    const double a = log(ie + sqrt(ie * ie + 1.0)) / N;            /* asinh */
+    vo_cplx *p = malloc(sizeof(vo_cplx) * (size_t)N);
+    if (!p) return -1;
+    for (int k = 1; k <= N; ++k) {
+        const double theta = M_PI * (2.0 * k - 1.0) / (2.0 * N);
+        const double sigma = -sinh(a) * sin(theta);
+        const double omega = cosh(a) * cos(theta);
+        vo_cplx s = {sigma * wp, omega * wp};
+        if (s.re >= 0) s.re = -fabs(s.re);
+        p[k - 1] = s;
+    }
+    qsort(p, (size_t)N, sizeof(vo_cplx), vo_cmp_imag);   /* the imaginary parts are distinct */
+    int n = 0;
+    for (int i = 0; i < N;) {
+        if (n >= max) { free(p); return -2; }
+        double *s = sos + 6 * n;
+        const vo_cplx q = p[i];
+        if (i + 1 == N || fabs(q.im) < 1e-12) {
+            const double a0 = W - q.re, a1 = -(W + q.re);
+            const double inva0 = 1.0 / a0;
+            s[0] = 1.0 * inva0; s[1] = 1.0 * inva0; s[2] = 0.0 * inva0;
+            s[3] = 1.0; s[4] = a1 * inva0; s[5] = 0.0 * inva0;
+            ++i;
+        } else {
+            const double are = q.re;
+            const double b2 = q.re * q.re + q.im * q.im;         /* |p|^2 */
+            const double A0 = (W * W - 2.0 * are * W + b2);
+            const double A1 = 2.0 * (b2 - W * W);
+            const double A2 = (W * W + 2.0 * are * W + b2);
+            const double inva0 = 1.0 / A0;
+            s[0] = 1.0 * inva0; s[1] = 2.0 * inva0; s[2] = 1.0 * inva0;
+            s[3] = 1.0; s[4] = A1 * inva0; s[5] = A2 * inva0;
+            i += 2;
+        }
+        ++n;
+    }
+    free(p);
+    /* DC gain 1, spread evenly, rounding error folded into section 0 */
+    long double H1 = 1.0L;
+    for (int i = 0; i < n; ++i) {
+        const double *s = sos + 6 * i;
+        const long double nu = (long double)s[0] + s[1] + s[2], de = (long double)s[3] + s[4] + s[5];
+        H1 *= nu / de;
+    }
+    if (!isfinite((double)H1) || fabsl(H1) < 1e-300L) return n;
+    const long double G = 1.0L / H1;
+    const long double g = powl(G, 1.0L / (long double)n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < 3; ++j) sos[6 * i + j] = (double)((long double)sos[6 * i + j] * g);
+    long double H1b = 1.0L;
+    for (int i = 0; i < n; ++i) {
+        const double *s = sos + 6 * i;
+        const long double nu = (long double)s[0] + s[1] + s[2], de = (long double)s[3] + s[4] + s[5];
+        H1b *= nu / de;
+    }
+    const long double c = 1.0L / H1b;
+    for (int j = 0; j < 3; ++j) sos[j] = (double)((long double)sos[j] * c);
+    return n;
+}
+
+/* One channel through the cascade from a zero state in FP64, transposed
+ * direct form II (processBlock, downsampling_filter_iir.cpp:210-240). */
+VO_API void vo_sos_df2t(const double *sos, int n, const float *in, float *out, uint64_t frames)
+{
+    double z[64][2] = {{0}};
+    for (uint64_t t = 0; t < frames; ++t) {
+        double y = (double)in[t];
+        for (int s = 0; s < n && s < 64; ++s) {
+            const double *b = sos + 6 * s;
+            const double x = y;
+            const double yo = b[0] * x + z[s][0];
+            const double z1 = b[1] * x - b[4] * yo + z[s][1];
+            const double z2 = b[2] * x - b[5] * yo;
+            z[s][0] = z1;
+            z[s][1] = z2;
+            y = yo;
+        }
+        out[t] = (float)y;
+    }
+}
+
+/* Output length for `steps` samples at step dt resampled to `rate`
+ * (simulator.cpp:1037-1038). */
+VO_API uint64_t vo_resample_len(double rate, uint64_t steps, float dt)
+{
+    return (uint64_t)(rate * ((double)steps * (double)dt));
+}
+
+/* Resampling of one filtered channel by linear interpolation at k / rate
+ * (the arithmetic of the interpolation at simulator.cpp:1046-1057: float
+ * time, index in double then float), the last sample held past the end;
+ * then, if normalize, division by the peak magnitude (simulator.cpp:
+ * 1067-1076; a silent channel stays zero).  FP32 with flush-to-zero, as on
+ * the GPU. */
+VO_API void vo_resample(const float *in, uint64_t len, double sim_rate, double rate, float *out, uint64_t out_len,
+                        int normalize)
+{
+    ftz_on();
+    for (uint64_t k = 0; k < out_len; ++k) {
+        const float t = (float)k / (float)rate;
+        const float index = (float)((double)t * sim_rate);
+        uint64_t lo = (uint64_t)floorf(index);
+        if (lo >= len) lo = len ? len - 1 : 0;
+        const uint64_t hi = lo + 1 < len ? lo + 1 : lo;
+        const float frac = index - (float)lo;
+        const float a = len ? in[lo] : 0.f, b = len ? in[hi] : 0.f;
+        out[k] = a * (1.f - frac) + b * frac;
+    }
+    if (normalize) {
+        float peak = 0.f;
+        for (uint64_t k = 0; k < out_len; ++k) peak = fmaxf(peak, fabsf(out[k]));
+        if (peak > 0.f)
+            for (uint64_t k = 0; k < out_len; ++k) out[k] = out[k] / peak;
+    }
+    ftz_off();
+}

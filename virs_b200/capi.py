@@ -76,6 +76,9 @@ _SIGS = {
     "virs_design_lowpass": ([C.c_float, C.c_float, C.c_float, C.c_float, _P], C.c_int),
     "virs_design_first_order": ([C.c_double, C.c_double, C.c_double, _P], C.c_int),
     "virs_design_octave_cascade": ([C.c_double, _P, _P, _P], C.c_int),
+    "virs_design_chebyshev_lowpass": ([C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _P, C.c_uint32,
+                                       C.POINTER(C.c_uint32)], C.c_int),
+    "virs_postprocess_ir": ([_P, C.c_double, _P, C.c_uint32, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     "virs_set_hard_source": ([_P, _P, C.c_size_t], C.c_int),
     "virs_set_sources": ([_P, C.c_uint32, _P, _P, C.c_size_t], C.c_int),
     "virs_set_receivers": ([_P, C.c_uint32, _P], C.c_int),
@@ -177,6 +180,16 @@ def design_octave_cascade(fs: float, alpha, freqs=None) -> np.ndarray:
     out = np.zeros(15, np.float64)
     check(lib().virs_design_octave_cascade(fs, _ptr(a), _ptr(f), _ptr(out)))
     return out.reshape(3, 5)
+
+
+def design_chebyshev_lowpass(fs: float, fc: float, fstop: float = 0.0, ripple_db: float = 0.5,
+                             atten_db: float = 90.0) -> np.ndarray:
+    """Chebyshev-I anti-alias low-pass as second-order sections [n][6]
+    {b0, b1, b2, a0, a1, a2}."""
+    out = np.zeros((32, 6), np.float64)
+    n = C.c_uint32(0)
+    check(lib().virs_design_chebyshev_lowpass(fs, fc, fstop, ripple_db, atten_db, _ptr(out), 32, C.byref(n)))
+    return out[: n.value].copy()
 
 
 class Simulation:
@@ -326,6 +339,19 @@ class Simulation:
         out = np.zeros((max(n, 1), steps), np.float32)
         check(lib().virs_get_ir(self._h, first, steps, _ptr(out)))
         return out[:n]
+
+    def postprocess_ir(self, rate: float = 48000.0, sos=None, normalize: bool = True) -> np.ndarray:
+        """The receiver traces of the steps run so far, anti-alias filtered
+        by `sos` ([n][6], None = no filter), resampled to `rate` and, if
+        asked, peak-normalised: [n_receivers][samples]."""
+        s6 = None if sos is None else _c(np.asarray(sos, np.float64).reshape(-1, 6), np.float64)
+        ns = 0 if s6 is None else s6.shape[0]
+        n = C.c_uint64(0)
+        check(lib().virs_postprocess_ir(self._h, rate, _ptr(s6), ns, int(normalize), None, 0, C.byref(n)))
+        nr = getattr(self, "_nrcv", 0)
+        out = np.zeros((max(nr, 1), n.value), np.float32)
+        check(lib().virs_postprocess_ir(self._h, rate, _ptr(s6), ns, int(normalize), _ptr(out), out.size, C.byref(n)))
+        return out[:nr]
 
     def pressure(self, prev: bool = False):
         cur = np.empty(self.nvox, np.float32)

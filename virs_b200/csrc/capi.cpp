@@ -1130,6 +1130,43 @@ VIRS_EXPORT virs_status virs_get_ir(const virs_sim *s, uint64_t first, uint64_t 
     return VIRS_OK;
 }
 
+VIRS_EXPORT virs_status virs_postprocess_ir(virs_sim *s, double rate, const double *sos, uint32_t ns, int normalize,
+                                            float *out, uint64_t capacity, uint64_t *out_len)
+{
+    if (!s || !out_len || (ns && !sos)) return fail(VIRS_E_ARG, "virs_postprocess_ir: null argument");
+    if (!(rate > 0.0) || !std::isfinite(rate)) return fail(VIRS_E_ARG, "virs_postprocess_ir: rate must be > 0");
+    if (ns > 32) return fail(VIRS_E_ARG, "virs_postprocess_ir: at most 32 sections");
+    if (!(s->dt > 0.f)) return fail(VIRS_E_STATE, "virs_postprocess_ir: no grid");
+    const uint64_t steps = s->steps_done;
+    const uint64_t len = (uint64_t)(rate * ((double)steps * (double)s->dt));
+    *out_len = len;
+    if (!out || !len || !s->nrcv) return VIRS_OK;
+    if (capacity < len) return fail(VIRS_E_ARG, "virs_postprocess_ir: capacity smaller than the output length");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(check_err(s));
+    // the simulation rate as the reference forms it: 1.f / dt in float
+    const double sim_rate = (double)(1.f / s->dt);
+    cudaStream_t st = s->stream;
+    DevBuf dsos, filt, res;
+    const float *src = s->ir.as<float>();
+    uint64_t stride = s->ircap;
+    if (ns) {
+        VIRS_TRY(dsos.alloc((size_t)ns * 6 * sizeof(double), "post-processing sections"));
+        VIRS_TRY(filt.alloc((size_t)s->nrcv * steps * sizeof(float), "filtered receiver traces"));
+        VIRS_CUDA(cudaMemcpyAsync(dsos.ptr, sos, (size_t)ns * 6 * sizeof(double), cudaMemcpyHostToDevice, st));
+        VIRS_CUDA(launch_ir_sos(src, stride, steps, dsos.as<double>(), (int)ns, filt.as<float>(), steps, s->nrcv, st));
+        src = filt.as<float>();
+        stride = steps;
+    }
+    VIRS_TRY(res.alloc((size_t)s->nrcv * len * sizeof(float), "resampled receiver traces"));
+    VIRS_CUDA(launch_ir_resample(src, stride, steps, sim_rate, (float)rate, res.as<float>(), len, normalize ? 1 : 0,
+                                 s->nrcv, st));
+    VIRS_CUDA(cudaMemcpyAsync(out, res.ptr, (size_t)s->nrcv * len * sizeof(float), cudaMemcpyDeviceToHost, st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_get_pressure(const virs_sim *s, float *cur, float *prev, size_t n)
 {
     if (!s || !cur) return fail(VIRS_E_ARG, "virs_get_pressure: null argument");

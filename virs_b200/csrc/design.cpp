@@ -9,10 +9,21 @@
 //                                absorbing-boundary filters (no reference
 //                                counterpart); published formulas of the RBJ
 //                                "Audio EQ Cookbook" for the shelves and the
-//                                peaking section.
+//                                peaking section;
+//   virs_design_chebyshev_lowpass
+//                                the anti-alias low-pass of the IR
+//                                post-processing: designChebyshevI_LP and
+//                                distributeDCGain
+//                                (src/util/downsampling_filter_iir.cpp:11-193),
+//                                the same steps and precisions (FP64, the DC
+//                                gain in long double), so the sections are
+//                                the reference's bit for bit.
 //
 // Compiled with -ffp-contract=off.
+#include <algorithm>
 #include <cmath>
+#include <complex>
+#include <vector>
 
 #include "internal.hpp"
 
@@ -131,6 +142,86 @@ __attribute__((visibility("default"))) virs_status virs_design_octave_cascade(do
              A * ((A + 1) + (A - 1) * cw - sA), (A + 1) - (A - 1) * cw + sA, 2 * ((A - 1) - (A + 1) * cw),
              (A + 1) - (A - 1) * cw - sA);
     }
+    return VIRS_OK;
+}
+
+
+// Chebyshev-I low-pass, second-order sections {b0, b1, b2, a0, a1, a2}:
+// prewarped analogue edges, the order that meets the ripple and
+// attenuation specs, the analogue poles ordered by imaginary part and
+// taken two at a time (the first of each two with its conjugate makes a
+// section with a double zero at z = -1; a last single pole makes a
+// first-order section), bilinear transform, and the DC gain set to 1 by
+// one common factor per section plus a final correction of section 0.
+__attribute__((visibility("default"))) virs_status virs_design_chebyshev_lowpass(double fs, double fc, double fstop,
+                                                                                 double ripple_db, double atten_db,
+                                                                                 double *sos, uint32_t max_sections,
+                                                                                 uint32_t *n_sections)
+{
+    if (!sos || !n_sections) return virs::fail(VIRS_E_ARG, "virs_design_chebyshev_lowpass: null argument");
+    if (!(fs > 0) || !(fc > 0) || !(fc < 0.5 * fs))
+        return virs::fail(VIRS_E_ARG, "virs_design_chebyshev_lowpass: need fs > 0 and 0 < fc < fs/2");
+    if (fstop <= 0.0) fstop = std::min(0.499 * fs, 1.15 * fc);
+    if (!(fstop > fc)) return virs::fail(VIRS_E_ARG, "virs_design_chebyshev_lowpass: the stop edge must lie above fc");
+    const auto acosh_ = [](double x) { return std::log(x + std::sqrt(x * x - 1.0)); };
+    const auto asinh_ = [](double x) { return std::log(x + std::sqrt(x * x + 1.0)); };
+    const double T = 1.0 / fs, W = 2.0 / T;
+    const double wp = 2.0 / T * std::tan(M_PI * (fc / fs));
+    const double ws = 2.0 / T * std::tan(M_PI * (fstop / fs));
+    const double eps = std::sqrt(std::pow(10.0, ripple_db / 10.0) - 1.0);
+    const double order =
+        acosh_(std::sqrt((std::pow(10.0, atten_db / 10.0) - 1.0) / (std::pow(10.0, ripple_db / 10.0) - 1.0))) /
+        acosh_(ws / wp);
+    const int N = std::max(1, (int)std::ceil(order));
+    const double a = asinh_(1.0 / eps) / N;
+    std::vector<std::complex<double>> poles;
+    for (int k = 1; k <= N; ++k) {
+        const double th = M_PI * (2.0 * k - 1.0) / (2.0 * N);
+        std::complex<double> p(-std::sinh(a) * std::sin(th) * wp, std::cosh(a) * std::cos(th) * wp);
+        if (p.real() >= 0) p = {-std::fabs(p.real()), p.imag()};
+        poles.push_back(p);
+    }
+    std::sort(poles.begin(), poles.end(), [](const auto &x, const auto &y) { return x.imag() < y.imag(); });
+    std::vector<double> o;
+    for (int i = 0; i < N;) {
+        const std::complex<double> p = poles[(size_t)i];
+        double b[3], d[3];
+        if (i + 1 == N || std::fabs(p.imag()) < 1e-12) {
+            b[0] = 1.0; b[1] = 1.0; b[2] = 0.0;
+            d[0] = W - p.real(); d[1] = -(W + p.real()); d[2] = 0.0;
+            ++i;
+        } else {
+            const double m2 = p.real() * p.real() + p.imag() * p.imag();
+            b[0] = 1.0; b[1] = 2.0; b[2] = 1.0;
+            d[0] = W * W - 2.0 * p.real() * W + m2;
+            d[1] = 2.0 * (m2 - W * W);
+            d[2] = W * W + 2.0 * p.real() * W + m2;
+            i += 2;
+        }
+        const double inv = 1.0 / d[0];
+        o.insert(o.end(), {b[0] * inv, b[1] * inv, b[2] * inv, 1.0, d[1] * inv, d[2] * inv});
+    }
+    const size_t n = o.size() / 6;
+    if (n > max_sections) return virs::fail(VIRS_E_ARG, "virs_design_chebyshev_lowpass: needs " + std::to_string(n) +
+                                                            " sections, room for " + std::to_string(max_sections));
+    const auto dc = [&]() {
+        long double h = 1.0L;
+        for (size_t q = 0; q < n; ++q) {
+            const double *s = &o[6 * q];
+            h *= ((long double)s[0] + s[1] + s[2]) / ((long double)s[3] + s[4] + s[5]);
+        }
+        return h;
+    };
+    const long double h = dc();
+    if (std::isfinite((double)h) && fabsl(h) >= 1e-300L) {
+        const long double g = powl(1.0L / h, 1.0L / (long double)n);
+        for (size_t q = 0; q < n; ++q)
+            for (int j = 0; j < 3; ++j) o[6 * q + j] = (double)((long double)o[6 * q + j] * g);
+        const long double c = 1.0L / dc();
+        for (int j = 0; j < 3; ++j) o[j] = (double)((long double)o[j] * c);
+    }
+    std::copy(o.begin(), o.end(), sos);
+    *n_sections = (uint32_t)n;
     return VIRS_OK;
 }
 

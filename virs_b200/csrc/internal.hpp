@@ -189,6 +189,12 @@ cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const flo
                            const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s);
 cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s);
 
+// IR post-processing (kernels_ir.cu)
+cudaError_t launch_ir_sos(const float *in, uint64_t in_stride, uint64_t len, const double *sos, int ns, float *out,
+                          uint64_t out_stride, uint32_t channels, cudaStream_t s);
+cudaError_t launch_ir_resample(const float *in, uint64_t in_stride, uint64_t len, double sim_rate, float rate,
+                               float *out, uint64_t out_len, int normalize, uint32_t channels, cudaStream_t s);
+
 // misc kernels (kernels_misc.cu)
 cudaError_t launch_energy(int storage, const void *p, const void *q, const uint8_t *code, uint32_t nx, uint32_t ny,
                           uint32_t nz, uint32_t px, double lambda2, double inv_scale2, double *partial,
