@@ -33,7 +33,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fvi
 # per-file extra flags: the step kernels flush subnormals like the reference
 # build (--use_fast_math implies -ftz=true) and keep every rounding explicit
 PER_FILE = {"kernels_step.cu": ["-ftz=true"], "kernels_step_tma.cu": ["-ftz=true"], "kernels_misc.cu": ["-ftz=true"],
-            "kernels_ir.cu": ["-ftz=true"]}
+            "kernels_ir.cu": ["-ftz=true"], "kernels_voxelize.cu": ["-fmad=false", "-ftz=false"]}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-Wall",
              f"-I{CUDA_HOME / 'include'}", *INC]
 

@@ -276,8 +276,9 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     if (!finite_pos(h)) return fail(VIRS_E_ARG, "cell size must be finite and positive");
     const size_t n = nx * ny * nz;
     uint8_t mx = 0;
-    for (size_t i = 0; i < n; ++i)
-        if (flags[i] > 3) return fail(VIRS_E_ARG, "flags must be 0..3 (flag " + std::to_string(flags[i]) + " at " + std::to_string(i) + ")");
+    if (flags)
+        for (size_t i = 0; i < n; ++i)
+            if (flags[i] > 3) return fail(VIRS_E_ARG, "flags must be 0..3 (flag " + std::to_string(flags[i]) + " at " + std::to_string(i) + ")");
     if (wmat)
         for (size_t i = 0; i < n; ++i) mx = std::max(mx, wmat[i]);
     s->drop_graphs();
@@ -300,7 +301,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
         b->release();
     VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
     VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
-    VIRS_TRY(h2d_rows(s->flags_raw.ptr, flags, 1, s));
+    if (flags) VIRS_TRY(h2d_rows(s->flags_raw.ptr, flags, 1, s));
     if (wmat) VIRS_TRY(h2d_rows(s->wall_mat.ptr, wmat, 1, s));
     VIRS_TRY(s->flags.alloc(s->nvox, "classified flags"));
     VIRS_TRY(s->field[0].alloc(s->nvox * s->storage_bytes(), "pressure field"));
@@ -317,6 +318,8 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     return VIRS_OK;
 }
 
+// mesh -> grid: bounding box and sizing on the host, the triangle sweep on
+// the GPU (kernels_voxelize.cu) straight into the padded flag arrays
 virs_status install_mesh(virs_sim *s, const Mesh &m)
 {
     float bmin[3], bmax[3];
@@ -326,17 +329,36 @@ virs_status install_mesh(virs_sim *s, const Mesh &m)
     grid_dims(bmin, bmax, h, d);
     if (d[0] < 3 || d[1] < 3 || d[2] < 3) return fail(VIRS_E_ARG, "mesh bounding box gives a grid below 3 voxels per axis");
     if (d[0] * d[1] * d[2] >= (1ull << 32)) return fail(VIRS_E_ARG, "mesh gives a grid of 2^32 voxels or more");
-    const size_t n = d[0] * d[1] * d[2];
-    std::vector<uint8_t> flags, wmat;
-    try {
-        flags.assign(n, 0);
-        wmat.assign(n, 0);
-    } catch (const std::bad_alloc &) {
-        return fail(VIRS_E_OOM, "host allocation of the voxel grid failed");
-    }
-    voxelize(m, s->roles, h, bmin, d[0], d[1], d[2], flags.data(), wmat.data());
-    VIRS_TRY(install_grid(s, d[0], d[1], d[2], h, flags.data(), wmat.data()));
+    const uint64_t ntri = m.tri_mat.size();
+    if (ntri >= 0xffffffffull) return fail(VIRS_E_ARG, "too many triangles");
+    for (uint32_t v : m.tris)
+        if ((uint64_t)v * 3 + 2 >= m.verts.size()) return fail(VIRS_E_ARG, "triangle vertex index out of range");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(install_grid(s, d[0], d[1], d[2], h, nullptr, nullptr));
     std::memcpy(s->bmin, bmin, sizeof(bmin));
+    if (ntri) {
+        DevBuf dv, dt, dm, dr, tri, la, lw, mx;
+        VIRS_TRY(dv.alloc(m.verts.size() * sizeof(float), "mesh vertices"));
+        VIRS_TRY(dt.alloc(m.tris.size() * sizeof(uint32_t), "mesh triangles"));
+        VIRS_TRY(dm.alloc(ntri * sizeof(int32_t), "triangle materials"));
+        VIRS_TRY(dr.alloc(std::max<size_t>(s->roles.size(), 1), "material roles"));
+        VIRS_TRY(tri.alloc(ntri * voxelize_tri_bytes(), "triangle table"));
+        VIRS_TRY(la.alloc(s->nvox * sizeof(uint32_t), "voxelisation marks"));
+        VIRS_TRY(lw.alloc(s->nvox * sizeof(uint32_t), "voxelisation marks"));
+        VIRS_TRY(mx.alloc(sizeof(uint32_t), "wall material maximum"));
+        VIRS_CUDA(cudaMemcpy(dv.ptr, m.verts.data(), dv.bytes, cudaMemcpyHostToDevice));
+        VIRS_CUDA(cudaMemcpy(dt.ptr, m.tris.data(), dt.bytes, cudaMemcpyHostToDevice));
+        VIRS_CUDA(cudaMemcpy(dm.ptr, m.tri_mat.data(), dm.bytes, cudaMemcpyHostToDevice));
+        if (!s->roles.empty()) VIRS_CUDA(cudaMemcpy(dr.ptr, s->roles.data(), s->roles.size(), cudaMemcpyHostToDevice));
+        VIRS_CUDA(launch_voxelize(dv.as<float>(), dt.as<uint32_t>(), dm.as<int32_t>(), ntri, dr.as<uint8_t>(),
+                                  (uint32_t)s->roles.size(), h, bmin, s->nx, s->ny, s->nz, s->px, tri.ptr,
+                                  la.as<uint32_t>(), lw.as<uint32_t>(), s->flags_raw.as<uint8_t>(),
+                                  s->wall_mat.as<uint8_t>(), mx.as<uint32_t>(), s->stream));
+        uint32_t mxh = 0;
+        VIRS_CUDA(cudaMemcpyAsync(&mxh, mx.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        VIRS_CUDA(cudaStreamSynchronize(s->stream));
+        s->max_wall_mat = (uint8_t)mxh;
+    }
     return VIRS_OK;
 }
 

@@ -189,6 +189,14 @@ cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const flo
                            const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s);
 cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s);
 
+// mesh voxelisation (kernels_voxelize.cu)
+size_t voxelize_tri_bytes();
+cudaError_t launch_voxelize(const float *verts, const uint32_t *tris, const int32_t *tri_mat, uint64_t ntri,
+                            const uint8_t *roles, uint32_t nroles, float h, const float bmin[3], uint32_t nx,
+                            uint32_t ny, uint32_t nz, uint32_t px, void *tri_buf, uint32_t *last_any,
+                            uint32_t *last_wall, uint8_t *flags, uint8_t *wall_mat, uint32_t *max_mat,
+                            cudaStream_t s);
+
 // IR post-processing (kernels_ir.cu)
 cudaError_t launch_ir_sos(const float *in, uint64_t in_stride, uint64_t len, const double *sos, int ns, float *out,
                           uint64_t out_stride, uint32_t channels, cudaStream_t s);
@@ -228,8 +236,7 @@ struct Mesh {
 virs_status load_obj(const char *path, Mesh &out);
 void mesh_bbox(const Mesh &m, float nudge, float bmin[3], float bmax[3]);
 void grid_dims(const float bmin[3], const float bmax[3], float h, uint64_t dims[3]);
-void voxelize(const Mesh &m, const std::vector<uint8_t> &roles, float h, const float bmin[3], uint64_t nx,
-              uint64_t ny, uint64_t nz, uint8_t *flags, uint8_t *wall_mat);
+
 
 void rbj_highpass(float fs, float cutoff, float q, float gain, float out5[5]);
 void rbj_lowpass(float fs, float cutoff, float q, float gain, float out5[5]);
