@@ -175,6 +175,18 @@ virs_status virs_set_sources(virs_sim *sim, uint32_t n, const uint64_t *idx, con
  * step, simulator_gpu.cu:295-300).  idx [n] voxel indices. */
 virs_status virs_set_receivers(virs_sim *sim, uint32_t n, const uint64_t *idx);
 
+/* Audio-driven sources (the design written out, commented, at
+ * simulator_gpu.cu:219-231, and TODO.md "Audio file implementation"): a
+ * signal sampled at sample_rate is read at the simulation times step * dt
+ * by linear interpolation (float time and sample index; 0 once index + 1
+ * reaches the end) for `steps` steps.  The hard-source form drives the
+ * flag-3 voxels, as the reference's design does; the soft-source form
+ * gives one channel per source, samples [n][len].  Need a grid (dt). */
+virs_status virs_set_hard_source_audio(virs_sim *sim, const float *samples, size_t len, float sample_rate,
+                                       uint64_t steps);
+virs_status virs_set_sources_audio(virs_sim *sim, uint32_t n, const uint64_t *idx, const float *samples, size_t len,
+                                   float sample_rate, uint64_t steps);
+
 /* ---- running ---------------------------------------------------------------- */
 
 /* Replaces fdtd_start_simulation (simulator_dispatch.cpp:93-100): reserve

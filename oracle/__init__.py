@@ -90,6 +90,8 @@ def lib():
         L.vo_resample_len.argtypes = [C.c_double, C.c_uint64, C.c_float]
         L.vo_resample.restype = None
         L.vo_resample.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.c_double, C.c_void_p, C.c_uint64, C.c_int]
+        L.vo_audio_to_steps.restype = None
+        L.vo_audio_to_steps.argtypes = [C.c_void_p, C.c_uint64, C.c_float, C.c_float, C.c_uint64, C.c_void_p]
         L.vo_round16.restype = None
         L.vo_round16.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32]
         L.vo_set_threads.argtypes = [C.c_int]
@@ -375,6 +377,14 @@ def postprocess(ir, dt, rate=48000.0, sos=None, normalize=True):
     for r in range(ir.shape[0]):
         x = ir[r] if sos is None or len(sos) == 0 else sos_df2t(sos, ir[r])
         lib().vo_resample(x.ctypes.data, steps, sim_rate, rate, out[r].ctypes.data, n, int(normalize))
+    return out
+
+
+def audio_to_steps(x, rate: float, dt: float, steps: int):
+    """An audio signal at `rate` read at step * dt (linear interpolation)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros(steps, np.float32)
+    lib().vo_audio_to_steps(x.ctypes.data, x.size, rate, dt, steps, out.ctypes.data)
     return out
 
 

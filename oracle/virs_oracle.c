@@ -1071,3 +1071,22 @@ VO_API void vo_resample(const float *in, uint64_t len, double sim_rate, double r
     }
     ftz_off();
 }
+
+/* An audio signal at `rate` read at step * dt by linear interpolation: the
+ * design commented at simulator_gpu.cu:219-231 (float time and index, 0
+ * once index + 1 reaches the end of the signal).  IEEE single, no
+ * contraction. */
+VO_API void vo_audio_to_steps(const float *x, uint64_t len, float rate, float dt, uint64_t steps, float *out)
+{
+    for (uint64_t n = 0; n < steps; ++n) {
+        const float t = (float)n * dt;
+        const float si = t * rate;
+        float v = 0.f;
+        if (si + 1.f < (float)len) {
+            const uint64_t lo = (uint64_t)si;
+            const float fr = si - (float)lo;
+            v = x[lo] + fr * (x[lo + 1] - x[lo]);
+        }
+        out[n] = v;
+    }
+}

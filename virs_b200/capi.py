@@ -78,6 +78,8 @@ _SIGS = {
     "virs_design_octave_cascade": ([C.c_double, _P, _P, _P], C.c_int),
     "virs_design_chebyshev_lowpass": ([C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _P, C.c_uint32,
                                        C.POINTER(C.c_uint32)], C.c_int),
+    "virs_set_hard_source_audio": ([_P, _P, C.c_size_t, C.c_float, C.c_uint64], C.c_int),
+    "virs_set_sources_audio": ([_P, C.c_uint32, _P, _P, C.c_size_t, C.c_float, C.c_uint64], C.c_int),
     "virs_postprocess_ir": ([_P, C.c_double, _P, C.c_uint32, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     "virs_set_hard_source": ([_P, _P, C.c_size_t], C.c_int),
     "virs_set_sources": ([_P, C.c_uint32, _P, _P, C.c_size_t], C.c_int),
@@ -303,6 +305,18 @@ class Simulation:
         s = _c(signal, np.float32).reshape(i.size, -1)
         check(lib().virs_set_sources(self._h, i.size, _ptr(i), _ptr(s), s.shape[1]))
         self._nsrc = i.size
+
+    def set_hard_source_audio(self, samples, sample_rate: float, steps: int):
+        """Flag-3 voxels driven by an audio signal at its own sample rate."""
+        x = _c(samples, np.float32).reshape(-1)
+        check(lib().virs_set_hard_source_audio(self._h, _ptr(x), x.size, sample_rate, steps))
+
+    def set_sources_audio(self, idx, samples, sample_rate: float, steps: int):
+        """Soft sources driven by audio channels [n][len] at their own sample rate."""
+        ix = _c(np.atleast_1d(idx), np.uint64)
+        x = _c(samples, np.float32).reshape(ix.size, -1)
+        check(lib().virs_set_sources_audio(self._h, ix.size, _ptr(ix), _ptr(x), x.shape[1], sample_rate, steps))
+        self._nsrc = ix.size
 
     def set_receivers(self, idx):
         i = _c(np.atleast_1d(idx), np.uint64)

@@ -943,6 +943,60 @@ VIRS_EXPORT virs_status virs_set_hard_source(virs_sim *s, const float *v, size_t
     return VIRS_OK;
 }
 
+namespace {
+// An audio signal sampled at `rate` read at the simulation times step * dt
+// with linear interpolation, following the design written out (commented)
+// at simulator_gpu.cu:219-231: float time, float sample index, zero once
+// index + 1 reaches the end of the signal.
+void audio_to_steps(const float *x, size_t len, float rate, float dt, uint64_t steps, float *out)
+{
+    for (uint64_t n = 0; n < steps; ++n) {
+        const float t = (float)n * dt;
+        const float si = t * rate;
+        float v = 0.f;
+        if (si + 1.f < (float)len) {
+            const size_t lo = (size_t)si;
+            const float fr = si - (float)lo;
+            v = x[lo] + fr * (x[lo + 1] - x[lo]);
+        }
+        out[n] = v;
+    }
+}
+
+bool audio_args_ok(const float *x, size_t len, float rate, uint64_t steps)
+{
+    if (!(rate > 0.f) || !std::isfinite(rate) || steps >= (1ull << 32)) return false;
+    for (size_t i = 0; i < len; ++i)
+        if (!std::isfinite(x[i])) return false;
+    return true;
+}
+} // namespace
+
+VIRS_EXPORT virs_status virs_set_hard_source_audio(virs_sim *s, const float *samples, size_t len, float sample_rate,
+                                                   uint64_t steps)
+{
+    if (!s || (!samples && len)) return fail(VIRS_E_ARG, "virs_set_hard_source_audio: null argument");
+    if (!(s->dt > 0.f)) return fail(VIRS_E_STATE, "no grid: the step size is not known yet");
+    if (!audio_args_ok(samples, len, sample_rate, steps))
+        return fail(VIRS_E_ARG, "virs_set_hard_source_audio: need a positive sample rate, finite samples, steps < 2^32");
+    std::vector<float> v(steps);
+    audio_to_steps(samples, len, sample_rate, s->dt, steps, v.data());
+    return virs_set_hard_source(s, v.data(), v.size());
+}
+
+VIRS_EXPORT virs_status virs_set_sources_audio(virs_sim *s, uint32_t n, const uint64_t *idx, const float *samples,
+                                               size_t len, float sample_rate, uint64_t steps)
+{
+    if (!s || (n && (!idx || (!samples && len)))) return fail(VIRS_E_ARG, "virs_set_sources_audio: null argument");
+    if (!(s->dt > 0.f)) return fail(VIRS_E_STATE, "no grid: the step size is not known yet");
+    if (!audio_args_ok(samples, (size_t)n * len, sample_rate, steps))
+        return fail(VIRS_E_ARG, "virs_set_sources_audio: need a positive sample rate, finite samples, steps < 2^32");
+    std::vector<float> sig((size_t)n * steps);
+    for (uint32_t i = 0; i < n; ++i)
+        audio_to_steps(samples + (size_t)i * len, len, sample_rate, s->dt, steps, sig.data() + (size_t)i * steps);
+    return virs_set_sources(s, n, idx, sig.data(), steps);
+}
+
 VIRS_EXPORT virs_status virs_set_sources(virs_sim *s, uint32_t n, const uint64_t *idx, const float *sig, size_t len)
 {
     if (!s || (n && (!idx || (!sig && len)))) return fail(VIRS_E_ARG, "virs_set_sources: null argument");
