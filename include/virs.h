@@ -68,6 +68,11 @@ typedef struct virs_params {
     float boundary_k;        /* 0 = (c*dt)/h*0.95 on the host (simulator_gpu.cu:147)  */
     double mix_filtered;     /* 0.1                    (simulator_gpu.cu:148)          */
     double mix_direct;       /* 0.9                    (simulator_gpu.cu:148)          */
+    int32_t rigid_walls;     /* 1: boundary voxels take the rigid-wall update from their
+                              * air neighbours (fdtd_kernel_rigid_walls,
+                              * simulator_gpu.cu:152-180, whose launch the reference
+                              * keeps commented at :280) before the filter correction;
+                              * 0 = the interior update with the wall mirror          */
 } virs_params;
 
 typedef struct virs_grid_info {

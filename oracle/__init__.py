@@ -241,6 +241,7 @@ class _RunArgs(C.Structure):
         ("ir", C.c_void_p), ("p", C.c_void_p), ("pprev", C.c_void_p), ("state", C.c_void_p),
         ("ir64", C.c_void_p),
         ("storage", C.c_int32), ("scale", C.c_float),
+        ("rigid", C.c_int32), ("l2", C.c_float), ("normals", C.c_void_p),
     ]
 
 
@@ -258,7 +259,8 @@ class Scene:
 
     def __init__(self, shape, flags, bidx, bmat, bw, coef32, n_sections, *, coef64=None,
                  hard=None, src_idx=(), src_sig=None, rcv_idx=(), consts=None, consts64=None,
-                 mix_y=0.1, mix_d=0.9, gain=float(np.float32(0.4)), form=0, storage=0, scale=1.0):
+                 mix_y=0.1, mix_d=0.9, gain=float(np.float32(0.4)), form=0, storage=0, scale=1.0,
+                 normals=None, rigid=False, l2=0.0):
         self.shape = tuple(int(s) for s in shape)
         self.flags = np.ascontiguousarray(flags, np.uint8)
         self.bidx = np.ascontiguousarray(bidx, np.uint32)
@@ -281,6 +283,9 @@ class Scene:
         self.form = int(form)
         self.storage = int(storage)   # FP32 run: 0 FP32 fields, 1 FP16, 2 BF16 (rounded as the GPU stores them)
         self.scale = float(scale)     # 16-bit storage: fields hold scale * p (a power of two)
+        self.normals = None if normals is None else np.ascontiguousarray(normals, np.uint8)
+        self.rigid = bool(rigid)      # FP32 run: rigid-wall update of the boundary voxels
+        self.l2 = float(l2)           # its (c dt / h)^2
 
     def _args(self, steps, step0, ir, p, pp, st, f64):
         a = _RunArgs()
@@ -302,6 +307,10 @@ class Scene:
         a.steps, a.step0, a.ir_stride = steps, step0, steps
         a.ir, a.p, a.pprev, a.state = _ptr(ir), _ptr(p), _ptr(pp), _ptr(st)
         a.storage, a.scale = self.storage, self.scale
+        if self.rigid:
+            if self.normals is None:
+                raise ValueError("the rigid-wall update needs the normals")
+            a.rigid, a.l2, a.normals = 1, self.l2, _ptr(self.normals)
         return a
 
     def run64(self, steps):
@@ -445,6 +454,9 @@ def ref_gpu():
     L = C.CDLL(str(p))
     L.ref_gpu_sponge.restype = C.c_int
     L.ref_gpu_sponge.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, _u8p, _u8p]
+    L.ref_gpu_run_rigid.restype = C.c_int
+    L.ref_gpu_run_rigid.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, _u8p, _u8p, _u32p, C.c_uint64,
+                                    _f32p, C.c_uint32, C.c_uint32, _u64p, _f32p, _f32p, _f32p]
     L.ref_gpu_run.restype = C.c_int
     L.ref_gpu_run.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, _u8p, _u32p, C.c_uint64, _f32p,
                               C.c_uint32, C.c_uint32, _u64p, _f32p, _f32p, _f32p]

@@ -28,6 +28,9 @@ __global__ void probe_constants(float *out)
     // the boundary scale exactly as fdtd_kernel_boundary_biquad evaluates it
     // (simulator_gpu.cu:147), compiled with the same flags
     out[0] = (d_c_sound * d_dt) / d_dx * 0.95f;
+    // the rigid-wall update's l2 as fdtd_kernel_rigid_walls evaluates it
+    // (simulator_gpu.cu:165)
+    out[1] = (d_c_sound * d_dt / d_dx) * (d_c_sound * d_dt / d_dx);
 }
 
 struct DevBuf {
@@ -66,11 +69,37 @@ __attribute__((visibility("default"))) int ref_gpu_sponge(uint64_t nx, uint64_t 
 
 // consts_out: dt, c2dt2, inv_h2 (host-computed and uploaded) and the device
 // value of the boundary scale.
+static int run_impl(uint64_t nx, uint64_t ny, uint64_t nz, float h, const uint8_t *flags, const uint8_t *normals,
+                    int rigid, const uint32_t *bidx, uint64_t nb, const float *coeffs5, uint32_t steps, uint32_t nrcv,
+                    const uint64_t *rcv, float *ir, float *p_final, float *consts_out);
+
 __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny, uint64_t nz, float h,
                                                        const uint8_t *flags, const uint32_t *bidx, uint64_t nb,
                                                        const float *coeffs5, uint32_t steps, uint32_t nrcv,
                                                        const uint64_t *rcv, float *ir, float *p_final,
                                                        float *consts_out)
+{
+    return run_impl(nx, ny, nz, h, flags, nullptr, 0, bidx, nb, coeffs5, steps, nrcv, rcv, ir, p_final, consts_out);
+}
+
+// The same step with fdtd_kernel_rigid_walls launched between the interior
+// and the filter kernels, as the commented launch at simulator_gpu.cu:280
+// places it; `normals` is the air-neighbour mask of every voxel.
+__attribute__((visibility("default"))) int ref_gpu_run_rigid(uint64_t nx, uint64_t ny, uint64_t nz, float h,
+                                                             const uint8_t *flags, const uint8_t *normals,
+                                                             const uint32_t *bidx, uint64_t nb,
+                                                             const float *coeffs5, uint32_t steps, uint32_t nrcv,
+                                                             const uint64_t *rcv, float *ir, float *p_final,
+                                                             float *consts_out)
+{
+    return run_impl(nx, ny, nz, h, flags, normals, 1, bidx, nb, coeffs5, steps, nrcv, rcv, ir, p_final, consts_out);
+}
+
+} // extern "C"
+
+static int run_impl(uint64_t nx, uint64_t ny, uint64_t nz, float h, const uint8_t *flags, const uint8_t *normals,
+                    int rigid, const uint32_t *bidx, uint64_t nb, const float *coeffs5, uint32_t steps, uint32_t nrcv,
+                    const uint64_t *rcv, float *ir, float *p_final, float *consts_out)
 {
     const size_t n = nx * ny * nz;
     DevBuf bp[3], dflags, dnorm, dbidx, dstate, dcoef, dprobe;
@@ -81,7 +110,8 @@ __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny,
     RCHECK(cudaMalloc(&dflags.p, n));
     RCHECK(cudaMemcpy(dflags.p, flags, n, cudaMemcpyHostToDevice));
     RCHECK(cudaMalloc(&dnorm.p, n));
-    RCHECK(cudaMemset(dnorm.p, 0, n));
+    if (normals) RCHECK(cudaMemcpy(dnorm.p, normals, n, cudaMemcpyHostToDevice));
+    else RCHECK(cudaMemset(dnorm.p, 0, n));
     RCHECK(cudaMalloc(&dbidx.p, (nb ? nb : 1) * sizeof(uint32_t)));
     if (nb) RCHECK(cudaMemcpy(dbidx.p, bidx, nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
     const size_t sections = 3; // simulator.cpp:339
@@ -89,7 +119,7 @@ __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny,
     RCHECK(cudaMemset(dstate.p, 0, (nb ? nb : 1) * sections * 4 * sizeof(float)));
     RCHECK(cudaMalloc(&dcoef.p, 5 * sizeof(float)));
     RCHECK(cudaMemcpy(dcoef.p, coeffs5, 5 * sizeof(float), cudaMemcpyHostToDevice));
-    RCHECK(cudaMalloc(&dprobe.p, sizeof(float)));
+    RCHECK(cudaMalloc(&dprobe.p, 2 * sizeof(float)));
 
     // simulator_gpu.cu:191-209
     int iNx = (int)nx, iNy = (int)ny, iNz = (int)nz;
@@ -114,6 +144,7 @@ __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny,
         consts_out[1] = c2_dt2;
         consts_out[2] = inv_h2;
         RCHECK(cudaMemcpy(&consts_out[3], dprobe.p, sizeof(float), cudaMemcpyDeviceToHost));
+        if (rigid) RCHECK(cudaMemcpy(&consts_out[4], (float *)dprobe.p + 1, sizeof(float), cudaMemcpyDeviceToHost));
     }
 
     float *d_prev = (float *)bp[0].p, *d_curr = (float *)bp[1].p, *d_next = (float *)bp[2].p;
@@ -125,6 +156,12 @@ __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny,
         float source_value = step < 10 ? 10.f : 0.f; // simulator_gpu.cu:214-218
         RCHECK(cudaMemcpyToSymbol(d_source_value, &source_value, sizeof(float)));
         fdtd_kernel<<<G, B>>>(d_prev, d_curr, d_next, (const uint8_t *)dflags.p, (const uint8_t *)dnorm.p);
+        RCHECK(cudaGetLastError());
+        RCHECK(cudaDeviceSynchronize());
+        if (rigid && nbb)
+            fdtd_kernel_rigid_walls<<<(unsigned)nbb, (unsigned)tpb>>>(d_curr, d_next, d_prev, (const uint8_t *)dflags.p,
+                                                                       (const uint8_t *)dnorm.p,
+                                                                       (const uint32_t *)dbidx.p);
         RCHECK(cudaGetLastError());
         RCHECK(cudaDeviceSynchronize());
         if (nbb)
@@ -144,4 +181,4 @@ __attribute__((visibility("default"))) int ref_gpu_run(uint64_t nx, uint64_t ny,
     return 0;
 }
 
-} // extern "C"
+

@@ -431,6 +431,9 @@ typedef struct vo_run_args {
     double *ir64;                  /* FP64 run: IR in double (may be NULL) */
     int32_t storage;               /* FP32 run: 0 FP32 fields, 1 FP16, 2 BF16 */
     float scale;                   /* 16-bit storage: fields hold scale * p  */
+    int32_t rigid;                 /* FP32 run: rigid-wall update of boundary voxels */
+    float l2;                      /* (c dt / h)^2 of that update            */
+    const uint8_t *normals;        /* air-neighbour mask per voxel           */
 } vo_run_args;
 
 /* 16-bit field storage, as the GPU path stores it: every value written to
@@ -582,6 +585,37 @@ static void boundary_f32(const vo_run_args *a, const float *pc, const float *pp,
     }
 }
 
+/* fdtd_kernel_rigid_walls (simulator_gpu.cu:152-180): a boundary voxel's
+ * update from its air neighbours only (the normals mask: neighbour flag 0),
+ * p+ = (2 - l2 n) p - p- + sum over the six neighbours, in the order +x,
+ * -x, +y, -y, +z, -z, of (l2 * s) * p_nb with s = 1 for an air neighbour
+ * and 0 otherwise; it replaces the interior update before the filter
+ * correction.  With the contractions of the reference build (found against
+ * its own kernel, tests/golden/rigid_room.npz): b1 = fma(-l2, n, 2),
+ * p = fma(b1, p, -p-), then fma(l2 * s, p_nb, p) per neighbour. */
+static void rigid_f32(const vo_run_args *a, const float *pc, const float *pp, float *pn)
+{
+    const uint64_t sy = a->nx, sz = a->nx * a->ny;
+    const float l2 = a->l2;
+#pragma omp parallel num_threads(vo_get_threads())
+    {
+        ftz_on();
+#pragma omp for schedule(static)
+        for (int64_t b = 0; b < (int64_t)a->nb; ++b) {
+            const uint64_t i = a->bidx[b];
+            const uint8_t m = a->normals[i];
+            int nn = 0;
+            for (uint8_t v = m; v; v &= (uint8_t)(v - 1)) ++nn;
+            const float b1 = fmaf(-l2, (float)nn, 2.f);
+            float r = fmaf(b1, pc[i], -pp[i]);
+            const uint64_t nb6[6] = {i + 1, i - 1, i + sy, i - sy, i + sz, i - sz};
+            for (int k = 0; k < 6; ++k) r = fmaf(l2 * ((m & (1u << k)) ? 1.f : 0.f), pc[nb6[k]], r);
+            pn[i] = r;
+        }
+        ftz_off();
+    }
+}
+
 static float sig_at(const vo_run_args *a, uint32_t s, uint64_t n)
 {
     return n < a->sig_len ? a->src_sig[(uint64_t)s * a->sig_len + n] : 0.f;
@@ -608,6 +642,7 @@ VO_API int vo_run_f32(const vo_run_args *a)
         const uint64_t sn = a->step0 + n;
         const float hard = sn < a->n_hard ? a->hard[sn] * scale : 0.f;
         interior_f32(a, pc, pp, pn, hard);
+        if (a->nb && a->rigid) rigid_f32(a, pc, pp, pn);
         if (a->nb) boundary_f32(a, pc, pp, pn, st);
         vo_round_field(pn, N, sto);
         for (uint32_t s = 0; s < a->n_src; ++s) {
@@ -681,6 +716,7 @@ static void f64_step(const vo_run_args *a, const double *pc, const double *pp, d
  * are measured against.  Coefficients come from a->coef64. */
 VO_API int vo_run_f64(const vo_run_args *a)
 {
+    if (a->rigid) return -2; /* the rigid-wall update is an FP32-run option */
     const uint64_t N = a->nx * a->ny * a->nz;
     double *b0 = calloc(N, sizeof(double)), *b1 = calloc(N, sizeof(double)), *b2 = calloc(N, sizeof(double));
     const uint64_t nst = a->nb * a->n_sections * 4;

@@ -10,7 +10,8 @@ the inputs and outputs of each case to tests/golden/<case>.npz:
   bidx        boundary list built from flags_ref (simulator.cpp:572-605)
   coef        the filter coefficients (RBJ high-pass 440 Hz, Q 0.1)
   consts      dt, c2dt2, inv_h2 as uploaded, and the boundary scale as the
-              reference kernel computes it on the device
+              reference kernel computes it on the device (rigid case: also
+              the rigid-wall l2 as that kernel computes it)
   rcv, ir     receiver indices and their samples after every step
   p_final     the pressure field after the last step
 
@@ -30,7 +31,7 @@ from helpers import oracle_grid  # noqa: E402
 from virs_b200 import scenes  # noqa: E402
 
 
-def run_case(L, name, shape, flags_raw, h, rcv, steps, out):
+def run_case(L, name, shape, flags_raw, h, rcv, steps, out, rigid=False):
     nx, ny, nz = shape
     flags_ref = np.empty_like(flags_raw)
     rc = L.ref_gpu_sponge(nx, ny, nz, flags_raw, flags_ref)
@@ -44,9 +45,15 @@ def run_case(L, name, shape, flags_raw, h, rcv, steps, out):
     rcv = np.asarray(rcv, np.uint64)
     ir = np.zeros((rcv.size, steps), np.float32)
     p_final = np.zeros(flags_raw.size, np.float32)
-    consts = np.zeros(4, np.float32)
-    rc = L.ref_gpu_run(nx, ny, nz, h, flags_ref, bidx if bidx.size else np.zeros(1, np.uint32), bidx.size, coef,
-                       steps, rcv.size, rcv, ir, p_final, consts)
+    consts = np.zeros(5, np.float32)
+    b = bidx if bidx.size else np.zeros(1, np.uint32)
+    if rigid:
+        normals = oracle.normals(shape, flags_ref)
+        rc = L.ref_gpu_run_rigid(nx, ny, nz, h, flags_ref, normals, b, bidx.size, coef, steps, rcv.size, rcv, ir,
+                                 p_final, consts)
+    else:
+        rc = L.ref_gpu_run(nx, ny, nz, h, flags_ref, b, bidx.size, coef, steps, rcv.size, rcv, ir, p_final, consts)
+        consts = consts[:4]
     assert rc == 0, rc
     np.savez_compressed(out / f"{name}.npz", shape=np.array(shape), h=np.float32(h), flags_raw=flags_raw,
                         flags_ref=flags_ref, bidx=bidx, coef=coef, consts=consts, rcv=rcv, ir=ir, p_final=p_final)
@@ -73,6 +80,12 @@ def main():
     f[rng.random(n) < 0.002] = 3
     rcv = rng.choice(np.flatnonzero(f == 0), 5, replace=False)
     run_case(L, "ref_scatter", shape, f, float(np.float32(0.03)), rcv, 300, out)
+    # 3. the reference room with the rigid-wall kernel launched (its launch is
+    #    commented at simulator_gpu.cu:280); consts[4] is its device l2
+    sc = scenes.reference_room(steps=400, size=(40, 34, 28), h=0.05)
+    g = oracle_grid(sc)
+    rcv = scenes.voxel_index(sc.rcv_pos, g["bmin"], g["h"], g["shape"])
+    run_case(L, "rigid_room", g["shape"], g["flags_raw"], g["h"], rcv, sc.steps, out, rigid=True)
 
 
 if __name__ == "__main__":

@@ -10,6 +10,9 @@ import oracle
 
 GOLD = Path(__file__).resolve().parent / "golden"
 CASES = sorted(p.stem for p in GOLD.glob("ref_*.npz"))
+# the same reference step with its rigid-wall kernel launched (consts[4]:
+# that kernel's l2 as it evaluates it on the device)
+RIGID = "rigid_room"
 
 
 def _load(name):
@@ -17,12 +20,13 @@ def _load(name):
     return {k: d[k] for k in d.files}
 
 
-def _oracle_run(d):
+def _oracle_run(d, rigid=False):
     shape = tuple(int(s) for s in d["shape"])
     c = d["consts"]
+    extra = dict(normals=oracle.normals(shape, d["flags_ref"]), rigid=True, l2=float(c[4])) if rigid else {}
     sc = oracle.Scene(shape, d["flags_ref"], d["bidx"], np.zeros(d["bidx"].size, np.uint8),
                       np.ones(d["bidx"].size, np.float32), d["coef"], 1, hard=np.full(10, 10.0, np.float32),
-                      rcv_idx=d["rcv"], consts=(c[1], c[2], c[3]))
+                      rcv_idx=d["rcv"], consts=(c[1], c[2], c[3]), **extra)
     n = int(np.prod(shape))
     st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(d["bidx"].size * 4 + 1, np.float32))
     ir = sc.run(d["ir"].shape[1], state=st)
@@ -51,13 +55,23 @@ def test_oracle_step_matches_reference_gpu(name):
     assert np.array_equal(p.view(np.uint32), d["p_final"].view(np.uint32))
 
 
+def test_oracle_rigid_walls_match_reference_gpu():
+    d = _load(RIGID)
+    ir, p = _oracle_run(d, rigid=True)
+    assert np.abs(d["ir"]).max() > 0
+    assert np.array_equal(ir.view(np.uint32), d["ir"].view(np.uint32))
+    assert np.array_equal(p.view(np.uint32), d["p_final"].view(np.uint32))
+    plain, _ = _oracle_run(d)                  # the rigid update does change the result
+    assert not np.array_equal(plain, d["ir"])
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + [RIGID])
 def test_cuda_path_matches_reference_gpu(name):
     from virs_b200 import capi
     d = _load(name)
     shape = tuple(int(s) for s in d["shape"])
-    p = capi.default_params(boundary_k=float(d["consts"][3]))
+    p = capi.default_params(boundary_k=float(d["consts"][3]), rigid_walls=int(name == RIGID))
     sim = capi.Simulation(p)
     sim.set_grid(shape, float(d["h"]), d["flags_raw"])
     sim.classify()

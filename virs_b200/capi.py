@@ -33,7 +33,7 @@ class Params(C.Structure):
         ("cell_size", C.c_float), ("bbox_nudge", C.c_float), ("sponge_width", C.c_int32), ("storage", C.c_int32),
         ("boundary_form", C.c_int32),
         ("storage_scale", C.c_float), ("boundary_gain", C.c_float), ("boundary_k", C.c_float),
-        ("mix_filtered", C.c_double), ("mix_direct", C.c_double),
+        ("mix_filtered", C.c_double), ("mix_direct", C.c_double), ("rigid_walls", C.c_int32),
     ]
 
 

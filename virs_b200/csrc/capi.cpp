@@ -113,7 +113,7 @@ struct virs_sim {
     uint64_t steps_done = 0;
 
     // constants
-    float dt = 0, c2dt2 = 0, inv_h2 = 0, K = 0;
+    float dt = 0, c2dt2 = 0, inv_h2 = 0, K = 0, l2 = 0;
     double fs = 0;
     float scale = 1.f, inv_scale = 1.f;
 
@@ -191,6 +191,9 @@ void compute_constants(virs_sim *s)
     s->c2dt2 = c * c * s->dt * s->dt;
     s->inv_h2 = 1.f / (h * h);
     s->K = s->prm.boundary_k != 0.f ? s->prm.boundary_k : (c * s->dt) / h * 0.95f;
+    // the rigid-wall update's (c dt / dx)^2 (simulator_gpu.cu:165)
+    const float cdh = c * s->dt / h;
+    s->l2 = cdh * cdh;
     const double dtd = (double)s->prm.courant * (double)h / ((double)c * std::sqrt(3.0));
     s->fs = 1.f / dtd;
 }
@@ -467,6 +470,9 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.p = s->field[parity].ptr;
     a.q = s->field[parity ^ 1].ptr;
     a.code = s->code.as<uint8_t>();
+    a.normals = s->normals.as<uint8_t>();
+    a.l2 = s->l2;
+    a.rigid = s->prm.rigid_walls ? 1 : 0;
     a.bmat = s->bmat.as<uint8_t>();
     a.bw = s->bw.as<float>();
     a.state = s->state.as<float>();
@@ -650,6 +656,7 @@ VIRS_EXPORT virs_status virs_create(const virs_params *p, virs_sim **out)
     if (prm.boundary_form != VIRS_BOUNDARY_REFERENCE && prm.boundary_form != VIRS_BOUNDARY_CENTERED)
         return fail(VIRS_E_ARG, "unknown boundary form");
     if (!(prm.storage_scale >= 0.f) || !std::isfinite(prm.storage_scale)) return fail(VIRS_E_ARG, "storage scale must be >= 0");
+    if (prm.rigid_walls != 0 && prm.rigid_walls != 1) return fail(VIRS_E_ARG, "rigid_walls must be 0 or 1");
     int ndev = 0;
     VIRS_CUDA(cudaGetDeviceCount(&ndev));
     if (prm.device < 0 || prm.device >= ndev) return fail(VIRS_E_ARG, "no CUDA device " + std::to_string(prm.device));
@@ -1831,6 +1838,8 @@ VIRS_EXPORT virs_status virs_forward_checkpointed(virs_sim *s, uint64_t steps, u
     if (steps == 0 || every == 0 || every > 4096) return fail(VIRS_E_ARG, "need steps > 0 and 1 <= every <= 4096");
     if (s->prm.storage != VIRS_STORAGE_F32) return fail(VIRS_E_ARG, "the adjoint runs with FP32 storage");
     if (s->depth == 0) return fail(VIRS_E_STATE, "the adjoint needs the TMA kernel (pipeline depth 1..3)");
+    if (s->prm.rigid_walls)
+        return fail(VIRS_E_STATE, "the adjoint assumes the mirrored update at boundary voxels, not rigid_walls");
     VIRS_TRY(virs_start_simulation(s, steps));
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     auto &A = s->adj;

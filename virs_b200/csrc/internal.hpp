@@ -72,6 +72,7 @@ struct StepArgs {
     const void *p;          // p^n (storage type)
     void *q;                // in p^{n-1}, out p^{n+1}
     const uint8_t *code;
+    const uint8_t *normals; // air-neighbour mask (rigid-wall update)
     const uint8_t *bmat;
     const float *bw;
     float *state;           // [S][4][nb]
@@ -85,6 +86,8 @@ struct StepArgs {
     int zc;                 // planes per block
     int form;               // VIRS_BOUNDARY_*
     float c2dt2, inv_h2;
+    float l2;               // (c dt / h)^2 of the rigid-wall update
+    int rigid;              // boundary voxels: rigid-wall update instead of the mirrored leapfrog
     double K, mix_y, mix_d, gain;
 };
 

@@ -183,8 +183,23 @@ __device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t
     T *Q = static_cast<T *>(a.q);
     const uint8_t c = __ldg(a.code + i);
     const float ce = IO::get(P[i]), qv = IO::get(Q[i]);
-    float r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
-                       IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
+    float r;
+    if (a.rigid) {
+        // fdtd_kernel_rigid_walls (simulator_gpu.cu:152-180): the air
+        // neighbours only (normals mask), p+ = (2 - l2 n) p - p- + the sum
+        // of (l2 * s) * p_nb over +x, -x, +y, -y, +z, -z with s = 1 for air;
+        // with the reference build's contractions
+        const uint8_t m = __ldg(a.normals + i);
+        const float b1 = __fmaf_rn(-a.l2, (float)__popc(m), 2.f);
+        r = __fmaf_rn(b1, ce, -qv);
+        const size_t nb6[6] = {i + 1, i - 1, i + sy, i - sy, i + sz, i - sz};
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            r = __fmaf_rn(__fmul_rn(a.l2, (m & (1u << k)) ? 1.f : 0.f), IO::get(P[nb6[k]]), r);
+    } else {
+        r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
+                     IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
+    }
     if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, ce, qv, 0.f);
     if (MODE == BND_RECORD) return;
     r = boundary<MAXS>(a, r, ce, qv, slot);
