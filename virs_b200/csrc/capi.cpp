@@ -87,7 +87,7 @@ struct virs_sim {
 
     // boundary
     uint64_t nb = 0;
-    DevBuf bidx, bmat, bw, state;
+    DevBuf bidx, bpos, bmat, bw, state;
 
     // filters
     uint32_t nmat = 0, nsec = 0;
@@ -274,8 +274,8 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
                          const uint8_t *wmat)
 {
     if (nx < 3 || ny < 3 || nz < 3) return fail(VIRS_E_ARG, "grid must be at least 3 voxels along each axis");
-    if (nx > (1u << 30) || ny > (1u << 30) || nz > (1u << 30) || nx * ny * nz >= (1ull << 32))
-        return fail(VIRS_E_ARG, "grid too large: boundary indices are 32-bit (nx*ny*nz < 2^32)");
+    if (nx > (1u << 30) || ny > (1u << 30) || nz > (1u << 30) || ((nx + 31) / 32 * 32) * ny * nz >= (1ull << 32))
+        return fail(VIRS_E_ARG, "grid too large: voxel positions are 32-bit (nx rounded up to 32, times ny*nz, < 2^32)");
     if (!finite_pos(h)) return fail(VIRS_E_ARG, "cell size must be finite and positive");
     const size_t n = nx * ny * nz;
     uint8_t mx = 0;
@@ -300,7 +300,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bmat, &s->bw, &s->state, &s->side})
+                      &s->field[1], &s->bidx, &s->bpos, &s->bmat, &s->bw, &s->state, &s->side})
         b->release();
     VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
     VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
@@ -471,6 +471,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.q = s->field[parity ^ 1].ptr;
     a.code = s->code.as<uint8_t>();
     a.normals = s->normals.as<uint8_t>();
+    a.bpos = s->bpos.as<uint32_t>();
     a.l2 = s->l2;
     a.rigid = s->prm.rigid_walls ? 1 : 0;
     a.bmat = s->bmat.as<uint8_t>();
@@ -525,7 +526,7 @@ cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
 {
     cudaError_t e = launch_stencil(s, parity, st);
     if (e != cudaSuccess) return e;
-    e = launch_boundary(s->prm.storage, step_args(s, parity), s->bidx.as<uint32_t>(), BND_UPDATE, st);
+    e = launch_boundary(s->prm.storage, step_args(s, parity), BND_UPDATE, st);
     if (e != cudaSuccess) return e;
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
@@ -569,7 +570,7 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
             err = launch_stencil(s, par, st);
             cudaEventRecord(ev[2 * i + 1], st);
             if (err == cudaSuccess)
-                err = launch_boundary(s->prm.storage, step_args(s, par), s->bidx.as<uint32_t>(), BND_UPDATE, st);
+                err = launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, st);
             cudaEventRecord(ev[2 * n + i], st);
             if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
         }
@@ -810,6 +811,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(wtab.alloc(wt.size() * 4, "sponge weights"));
         VIRS_CUDA(cudaMemcpy(wtab.ptr, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice));
         VIRS_TRY(s->bidx.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary indices"));
+        VIRS_TRY(s->bpos.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary positions"));
         VIRS_TRY(s->bmat.alloc(std::max<uint64_t>(nb, 1), "boundary materials"));
         VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
         VIRS_TRY(s->side.alloc(std::max<uint64_t>(nb, 1) * sizeof(float4), "boundary records"));
@@ -820,6 +822,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         cp.bd2_full = bd2_full.as<uint16_t>();
         cp.wtab = wtab.as<float>();
         cp.bidx = s->bidx.as<uint32_t>();
+        cp.bpos = s->bpos.as<uint32_t>();
         cp.bmat = s->bmat.as<uint8_t>();
         cp.bw = s->bw.as<float>();
         cp.nx = s->nx;
@@ -1910,7 +1913,7 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
             const uint64_t k = n - n0;
             VIRS_CUDA(cudaMemcpyAsync(A.segst.as<char>() + k * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
             cudaError_t e = launch_stencil(s, s->cur, st);
-            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), s->bidx.as<uint32_t>(), BND_KEEP, st);
+            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), BND_KEEP, st);
             if (e == cudaSuccess) e = launch_keep_records(s->side.as<float4>(), A.segrec.as<float4>() + k * nb, nb, st);
             if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, s->cur), st);
             if (e != cudaSuccess) return cuda_fail(e, "adjoint recomputation");
@@ -1939,7 +1942,7 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
                 e = launch_step_tma(VIRS_STORAGE_F32, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
                 // the free value A F - RR at the boundary voxels, which the
                 // stencil left alone
-                if (e == cudaSuccess) e = launch_boundary(VIRS_STORAGE_F32, a, s->bidx.as<uint32_t>(), BND_RECORD, st);
+                if (e == cudaSuccess) e = launch_boundary(VIRS_STORAGE_F32, a, BND_RECORD, st);
             }
             if (e == cudaSuccess)
                 e = launch_adj_fix(RR, T, s->bidx.as<uint32_t>(), s->side.as<float4>(), A.dbar.as<float>(),

@@ -73,6 +73,7 @@ struct StepArgs {
     void *q;                // in p^{n-1}, out p^{n+1}
     const uint8_t *code;
     const uint8_t *normals; // air-neighbour mask (rigid-wall update)
+    const uint32_t *bpos;   // [nb] padded device index of each boundary slot
     const uint8_t *bmat;
     const float *bw;
     float *state;           // [S][4][nb]
@@ -126,7 +127,7 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
 cudaError_t launch_post(int storage, const PostArgs &a, cudaStream_t s);
 // modes of the boundary pass (kernels_step.cu)
 enum { BND_UPDATE = 0, BND_KEEP = 1, BND_RECORD = 2 };
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, int mode, cudaStream_t s);
+cudaError_t launch_boundary(int storage, const StepArgs &a, int mode, cudaStream_t s);
 int default_planes(uint32_t nz);
 
 // TMA-staged step (kernels_step_tma.cu)
@@ -174,6 +175,7 @@ struct CompactArgs {
     const uint16_t *bd2_full;
     const float *wtab;         // sponge weight per d2
     uint32_t *bidx;
+    uint32_t *bpos;            // padded device index of each slot's voxel
     uint8_t *bmat;
     float *bw;
     uint32_t nx, ny, nz, px, spr;

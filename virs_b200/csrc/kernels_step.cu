@@ -171,47 +171,83 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
 //               slot kept in a.side (the adjoint's recomputation)
 //   BND_RECORD  the record only: no filters, nothing written to the fields
 //               (the adjoint step, on adjoint fields)
+// The loads of one boundary voxel (first part) and its update (second).
+template <typename T, int MAXS> struct BVox {
+    size_t i;
+    uint8_t c, nm;
+    float ce, qv, nb[6];
+    BState<MAXS> st;
+};
+
 template <typename T, int MODE, int MAXS>
-__device__ __forceinline__ void boundary_voxel(const StepArgs &a, const uint32_t *__restrict bidx, uint64_t slot)
+__device__ __forceinline__ void bvox_load(const StepArgs &a, uint64_t slot, BVox<T, MAXS> &v)
 {
     using IO = Io<T>;
-    const uint32_t ref = __ldg(bidx + slot);
-    const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
+    const size_t i = __ldg(a.bpos + slot);
     const size_t sy = a.px, sz = (size_t)a.px * a.ny;
-    const size_t i = (size_t)z * sz + (size_t)y * sy + x;
     const T *P = static_cast<const T *>(a.p);
-    T *Q = static_cast<T *>(a.q);
-    const uint8_t c = __ldg(a.code + i);
-    const float ce = IO::get(P[i]), qv = IO::get(Q[i]);
+    const T *Q = static_cast<const T *>(a.q);
+    v.i = i;
+    v.c = __ldg(a.code + i);
+    v.nm = a.rigid ? __ldg(a.normals + i) : 0;
+    v.ce = IO::get(P[i]);
+    v.qv = IO::get(Q[i]);
+    v.nb[0] = IO::get(P[i + 1]);
+    v.nb[1] = IO::get(P[i - 1]);
+    v.nb[2] = IO::get(P[i + sy]);
+    v.nb[3] = IO::get(P[i - sy]);
+    v.nb[4] = IO::get(P[i + sz]);
+    v.nb[5] = IO::get(P[i - sz]);
+    if (MODE != BND_RECORD && MAXS > 0) bload<MAXS>(a, slot, v.st);
+}
+
+template <typename T, int MODE, int MAXS>
+__device__ __forceinline__ void bvox_update(const StepArgs &a, uint64_t slot, const BVox<T, MAXS> &v)
+{
     float r;
     if (a.rigid) {
         // fdtd_kernel_rigid_walls (simulator_gpu.cu:152-180): the air
         // neighbours only (normals mask), p+ = (2 - l2 n) p - p- + the sum
         // of (l2 * s) * p_nb over +x, -x, +y, -y, +z, -z with s = 1 for air;
         // with the reference build's contractions
-        const uint8_t m = __ldg(a.normals + i);
-        const float b1 = __fmaf_rn(-a.l2, (float)__popc(m), 2.f);
-        r = __fmaf_rn(b1, ce, -qv);
-        const size_t nb6[6] = {i + 1, i - 1, i + sy, i - sy, i + sz, i - sz};
+        const float b1 = __fmaf_rn(-a.l2, (float)__popc(v.nm), 2.f);
+        r = __fmaf_rn(b1, v.ce, -v.qv);
 #pragma unroll
-        for (int k = 0; k < 6; ++k)
-            r = __fmaf_rn(__fmul_rn(a.l2, (m & (1u << k)) ? 1.f : 0.f), IO::get(P[nb6[k]]), r);
+        for (int k = 0; k < 6; ++k) r = __fmaf_rn(__fmul_rn(a.l2, (v.nm & (1u << k)) ? 1.f : 0.f), v.nb[k], r);
     } else {
-        r = leapfrog(c, ce, IO::get(P[i + 1]), IO::get(P[i - 1]), IO::get(P[i + sy]), IO::get(P[i - sy]),
-                     IO::get(P[i + sz]), IO::get(P[i - sz]), qv, a.c2dt2, a.inv_h2);
+        r = leapfrog(v.c, v.ce, v.nb[0], v.nb[1], v.nb[2], v.nb[3], v.nb[4], v.nb[5], v.qv, a.c2dt2, a.inv_h2);
     }
-    if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, ce, qv, 0.f);
+    if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, v.ce, v.qv, 0.f);
     if (MODE == BND_RECORD) return;
-    r = boundary<MAXS>(a, r, ce, qv, slot);
-    Q[i] = IO::put(r);
+    r = MAXS > 0 ? bcompute<MAXS>(a, r, v.ce, v.qv, slot, v.st) : boundary_loop(a, r, v.ce, v.qv, slot);
+    static_cast<T *>(a.q)[v.i] = Io<T>::put(r);
 }
 
+// The compacted boundary pass (simulator_gpu.cu:105-150), in list order.
+// The stencil kernels left these voxels untouched (p^{n-1} in place); the
+// pass gathers the seven p values, p^{n-1} and the code of each voxel from
+// the p^n buffer (not written during the step), computes the leapfrog
+// update with the wall mirror (or the rigid-wall update), then the filter
+// correction, and writes p^{n+1}.  A thread takes two slots, BT apart, and
+// issues all loads of both before any arithmetic: the pass is bound by the
+// latency of its gathers, and two independent voxels in flight hide it.
+//   BND_UPDATE  the step
+//   BND_KEEP    the same, and the record {free value, p, p^{n-1}} of the
+//               slot kept in a.side (the adjoint's recomputation)
+//   BND_RECORD  the record only: no filters, nothing written to the fields
+//               (the adjoint step, on adjoint fields)
+constexpr int BT = 256;
+
 template <typename T, int MODE, int MAXS>
-__global__ void __launch_bounds__(256) k_boundary(const __grid_constant__ StepArgs a, const uint32_t *__restrict bidx)
+__global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArgs a)
 {
-    const uint64_t slot = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= a.nb) return;
-    boundary_voxel<T, MODE, MAXS>(a, bidx, slot);
+    const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
+    const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
+    BVox<T, MAXS> v0, v1;
+    if (h0) bvox_load<T, MODE, MAXS>(a, s0, v0);
+    if (h1) bvox_load<T, MODE, MAXS>(a, s1, v1);
+    if (h0) bvox_update<T, MODE, MAXS>(a, s0, v0);
+    if (h1) bvox_update<T, MODE, MAXS>(a, s1, v1);
 }
 
 // batched: thread g belongs to the last member whose first boundary index
@@ -236,7 +272,9 @@ __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__res
         else hi = mid - 1;
     }
     const BatchMember &b = mem[lo];
-    boundary_voxel<T, BND_UPDATE, MAXS>(b.step[parity], b.bidx, g - b.first_bnd);
+    BVox<T, MAXS> v;
+    bvox_load<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
+    bvox_update<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
 }
 
 template <typename T> __device__ __forceinline__ void post_body(const PostArgs &a)
@@ -302,21 +340,20 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
 namespace {
 
 template <typename T, int MODE>
-void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, const uint32_t *bidx, cudaStream_t s)
+void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, cudaStream_t s)
 {
-    if (MODE == BND_RECORD || ns <= 1) k_boundary<T, MODE, 1><<<g, 256, 0, s>>>(a, bidx);
-    else if (ns == 2) k_boundary<T, MODE, 2><<<g, 256, 0, s>>>(a, bidx);
-    else if (ns <= 4) k_boundary<T, MODE, 4><<<g, 256, 0, s>>>(a, bidx);
-    else k_boundary<T, MODE, 0><<<g, 256, 0, s>>>(a, bidx);
+    if (MODE == BND_RECORD || ns <= 1) k_boundary<T, MODE, 1><<<g, BT, 0, s>>>(a);
+    else if (ns == 2) k_boundary<T, MODE, 2><<<g, BT, 0, s>>>(a);
+    else if (ns <= 4) k_boundary<T, MODE, 4><<<g, BT, 0, s>>>(a);
+    else k_boundary<T, MODE, 0><<<g, BT, 0, s>>>(a);
 }
 
-template <typename T> void boundary_by_mode(int mode, uint32_t ns, unsigned g, const StepArgs &a, const uint32_t *bidx,
-                                            cudaStream_t s)
+template <typename T> void boundary_by_mode(int mode, uint32_t ns, unsigned g, const StepArgs &a, cudaStream_t s)
 {
     switch (mode) {
-    case BND_KEEP: boundary_by_sections<T, BND_KEEP>(ns, g, a, bidx, s); break;
-    case BND_RECORD: boundary_by_sections<T, BND_RECORD>(ns, g, a, bidx, s); break;
-    default: boundary_by_sections<T, BND_UPDATE>(ns, g, a, bidx, s); break;
+    case BND_KEEP: boundary_by_sections<T, BND_KEEP>(ns, g, a, s); break;
+    case BND_RECORD: boundary_by_sections<T, BND_RECORD>(ns, g, a, s); break;
+    default: boundary_by_sections<T, BND_UPDATE>(ns, g, a, s); break;
     }
 }
 
@@ -330,14 +367,14 @@ void boundary_batch_by_sections(uint32_t maxs, unsigned g, const BatchMember *me
 
 } // namespace
 
-cudaError_t launch_boundary(int storage, const StepArgs &a, const uint32_t *bidx, int mode, cudaStream_t s)
+cudaError_t launch_boundary(int storage, const StepArgs &a, int mode, cudaStream_t s)
 {
     if (a.nb == 0) return cudaSuccess;
-    const unsigned g = (unsigned)((a.nb + 255) / 256);
+    const unsigned g = (unsigned)((a.nb + 2 * BT - 1) / (2 * BT));
     switch (storage) {
-    case VIRS_STORAGE_F16: boundary_by_mode<__half>(mode, a.nsec, g, a, bidx, s); break;
-    case VIRS_STORAGE_BF16: boundary_by_mode<__nv_bfloat16>(mode, a.nsec, g, a, bidx, s); break;
-    default: boundary_by_mode<float>(mode, a.nsec, g, a, bidx, s); break;
+    case VIRS_STORAGE_F16: boundary_by_mode<__half>(mode, a.nsec, g, a, s); break;
+    case VIRS_STORAGE_BF16: boundary_by_mode<__nv_bfloat16>(mode, a.nsec, g, a, s); break;
+    default: boundary_by_mode<float>(mode, a.nsec, g, a, s); break;
     }
     return cudaGetLastError();
 }

@@ -197,45 +197,58 @@ __device__ __forceinline__ float correct(const StepArgs &a, float r, float d, fl
 // (simulator_gpu.cu:126-146) without the copies, so every value, and the
 // result, is the same.
 
-// up to MAXS sections, fully unrolled: every state, the material and the
-// weight are loaded before any arithmetic, so one slot costs two dependent
-// memory round trips (states/material, then coefficients), not one per
-// section
-template <int MAXS>
-__device__ __forceinline__ float boundary_unrolled(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
+// up to MAXS sections, fully unrolled, in two parts so that a caller can
+// issue the loads of several voxels before any arithmetic: bload reads the
+// material, the weight and every state of a slot; bcompute reads the
+// coefficients (they depend on the material), runs the cascade, writes the
+// states and returns the corrected value.
+template <int MAXS> struct BState {
+    uint32_t m;
+    float wf;
+    float h[MAXS + 1][2];
+};
+
+template <int MAXS> __device__ __forceinline__ void bload(const StepArgs &a, uint64_t slot, BState<MAXS> &b)
 {
     const uint32_t ns = a.nsec;
-    const uint64_t nb = a.nb;
-    float *st = a.state + slot;
-    const uint32_t m = __ldg(a.bmat + slot);
-    const float wf = __ldg(a.bw + slot);
-    float h[MAXS + 1][2];
+    const float *st = a.state + slot;
+    b.m = __ldg(a.bmat + slot);
+    b.wf = __ldg(a.bw + slot);
 #pragma unroll
     for (int q = 0; q <= MAXS; ++q)
         if (q <= (int)ns)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) h[q][j] = st[(uint64_t)(2 * q + j) * nb];
-    const float *kc = a.coef + (uint64_t)m * ns * 5;
+            for (int j = 0; j < 2; ++j) b.h[q][j] = st[(uint64_t)(2 * q + j) * a.nb];
+}
+
+template <int MAXS>
+__device__ __forceinline__ float bcompute(const StepArgs &a, float r, float ce, float qv, uint64_t slot,
+                                          const BState<MAXS> &b)
+{
+    const uint32_t ns = a.nsec;
+    const uint64_t nb = a.nb;
+    float *st = a.state + slot;
+    const float *kc = a.coef + (uint64_t)b.m * ns * 5;
     const float d = __fsub_rn(ce, qv);
-    float in = d, last = h[0][0];
+    float in = d, last = b.h[0][0];
 #pragma unroll
     for (int q = 0; q < MAXS; ++q) {
         if (q < (int)ns) {
             const float *kq = kc + 5 * q;
-            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), h[q][0]));
-            y = __fmaf_rn(__ldg(kq + 2), h[q][1], y);
-            y = __fmaf_rn(-__ldg(kq + 3), h[q + 1][0], y);
-            y = __fmaf_rn(-__ldg(kq + 4), h[q + 1][1], y);
+            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), b.h[q][0]));
+            y = __fmaf_rn(__ldg(kq + 2), b.h[q][1], y);
+            y = __fmaf_rn(-__ldg(kq + 3), b.h[q + 1][0], y);
+            y = __fmaf_rn(-__ldg(kq + 4), b.h[q + 1][1], y);
             st[(uint64_t)(2 * q + 0) * nb] = in;
-            st[(uint64_t)(2 * q + 1) * nb] = h[q][0];
+            st[(uint64_t)(2 * q + 1) * nb] = b.h[q][0];
             in = y;
-            last = h[q + 1][0];
+            last = b.h[q + 1][0];
         }
     }
     // the history of the last output
     st[(uint64_t)(2 * ns + 0) * nb] = in;
     st[(uint64_t)(2 * ns + 1) * nb] = last;
-    return correct(a, r, d, in, qv, wf);
+    return correct(a, r, d, in, qv, b.wf);
 }
 
 // any number of sections
@@ -262,14 +275,6 @@ __device__ __noinline__ float boundary_loop(const StepArgs &a, float r, float ce
     st[0] = in;
     st[nb] = x1;
     return correct(a, r, d, in, qv, __ldg(a.bw + slot));
-}
-
-// MAXS = 0: the loop form
-template <int MAXS>
-__device__ __forceinline__ float boundary(const StepArgs &a, float r, float ce, float qv, uint64_t slot)
-{
-    if constexpr (MAXS == 0) return boundary_loop(a, r, ce, qv, slot);
-    else return boundary_unrolled<MAXS>(a, r, ce, qv, slot);
 }
 
 } // namespace
