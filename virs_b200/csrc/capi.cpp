@@ -88,6 +88,8 @@ struct virs_sim {
     // boundary
     uint64_t nb = 0;
     DevBuf bidx, bpos, bmat, bw, state;
+    DevBuf hpos;                   // hard-source voxel positions
+    uint32_t nhpos = 0;
 
     // filters
     uint32_t nmat = 0, nsec = 0;
@@ -300,7 +302,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bpos, &s->bmat, &s->bw, &s->state, &s->side})
+                      &s->field[1], &s->bidx, &s->bpos, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
         b->release();
     VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
     VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
@@ -512,6 +514,10 @@ PostArgs post_args(const virs_sim *s, int parity)
     a.siglen = s->siglen;
     a.cap = s->ircap;
     a.inv_scale = s->inv_scale;
+    a.hpos = s->hpos.as<uint32_t>();
+    a.nhpos = s->nhpos;
+    a.hard = s->hard.as<float>();
+    a.nhard = s->nhard;
     return a;
 }
 
@@ -798,6 +804,20 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         co.px = s->px;
         co.spr = s->spr;
         VIRS_CUDA(launch_codes(co, st));
+        {
+            DevBuf cnt;
+            VIRS_TRY(cnt.alloc(4, "hard-source count"));
+            VIRS_CUDA(launch_hard_list(s->code.as<uint8_t>(), s->nvox, cnt.as<uint32_t>(), nullptr, 0, st));
+            uint32_t nh = 0;
+            VIRS_CUDA(cudaMemcpyAsync(&nh, cnt.ptr, 4, cudaMemcpyDeviceToHost, st));
+            VIRS_CUDA(cudaStreamSynchronize(st));
+            VIRS_TRY(s->hpos.alloc(std::max<uint32_t>(nh, 1) * 4, "hard-source positions"));
+            VIRS_CUDA(cudaMemsetAsync(cnt.ptr, 0, 4, st));
+            VIRS_CUDA(launch_hard_list(s->code.as<uint8_t>(), s->nvox, cnt.as<uint32_t>(), s->hpos.as<uint32_t>(), nh,
+                                       st));
+            VIRS_CUDA(cudaStreamSynchronize(st));
+            s->nhpos = nh;
+        }
         VIRS_TRY(scan_tmp.alloc(scan_tmp_words(nseg) * 4, "scan scratch"));
         VIRS_TRY(total.alloc(4, "boundary count"));
         VIRS_CUDA(launch_scan(s->bseg.as<uint32_t>(), nseg, scan_tmp.as<uint32_t>(), total.as<uint32_t>(), st));
@@ -1940,6 +1960,7 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
                 a.nhard = 0;
                 const TmaMaps m{&A.mapP[t], &A.mapQ[t ^ 1], &s->tmC};
                 e = launch_step_tma(VIRS_STORAGE_F32, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
+                if (e == cudaSuccess) e = launch_zero_at(RR, s->hpos.as<uint32_t>(), s->nhpos, st);
                 // the free value A F - RR at the boundary voxels, which the
                 // stencil left alone
                 if (e == cudaSuccess) e = launch_boundary(VIRS_STORAGE_F32, a, BND_RECORD, st);

@@ -102,6 +102,10 @@ struct PostArgs {
     uint32_t nsrc, nrcv;
     uint64_t siglen, cap;
     float inv_scale;
+    const uint32_t *hpos;   // device positions of the hard-source voxels
+    uint32_t nhpos;
+    uint32_t nhard;         // per-step hard-source values (scaled) in `hard`
+    const float *hard;
 };
 
 // one member of a batched run (device-resident descriptor)
@@ -181,6 +185,8 @@ struct CompactArgs {
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);
+cudaError_t launch_hard_list(const uint8_t *code, uint64_t n, uint32_t *count, uint32_t *out, uint32_t cap,
+                             cudaStream_t s);
 
 // adjoint kernels (kernels_adjoint.cu)
 cudaError_t launch_adj_inject(float *T, const uint8_t *code, const uint64_t *rcv, uint32_t nrcv, const float *dl,
@@ -193,6 +199,7 @@ cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *b
 cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const float4 *rec, const float *dbar,
                            const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s);
 cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s);
+cudaError_t launch_zero_at(float *f, const uint32_t *pos, uint32_t n, cudaStream_t s);
 
 // mesh voxelisation (kernels_voxelize.cu)
 size_t voxelize_tri_bytes();

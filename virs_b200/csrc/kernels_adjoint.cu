@@ -189,6 +189,23 @@ cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const flo
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_zero_at(float *f, const uint32_t *__restrict pos, uint32_t n)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) f[pos[k]] = 0.f;
+}
+} // namespace
+
+// the adjoint at the hard-source voxels is 0 (their forward value does not
+// depend on the field); the stencil leaves them alone
+cudaError_t launch_zero_at(float *f, const uint32_t *pos, uint32_t n, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    k_zero_at<<<(n + 255) / 256, 256, 0, s>>>(f, pos, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s)
 {
     if (nb == 0) return cudaSuccess;

@@ -283,6 +283,27 @@ cudaError_t launch_scan(uint32_t *data, size_t n, uint32_t *tmp, uint32_t *total
     return cudaGetLastError();
 }
 
+namespace {
+// device positions of the hard-source voxels (code CODE_HARD); with
+// out == nullptr only counts them.  The order is arbitrary: every step
+// writes the same value to all of them.
+__global__ void k_hard_list(const uint8_t *__restrict code, uint64_t n, uint32_t *count, uint32_t *out, uint32_t cap)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (code[i] == CODE_HARD) {
+            const uint32_t k = atomicAdd(count, 1u);
+            if (out && k < cap) out[k] = (uint32_t)i;
+        }
+}
+} // namespace
+
+cudaError_t launch_hard_list(const uint8_t *code, uint64_t n, uint32_t *count, uint32_t *out, uint32_t cap,
+                             cudaStream_t s)
+{
+    k_hard_list<<<1184, 256, 0, s>>>(code, n, count, out, cap);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s)
 {
     k_compact<<<dim3(a.spr, a.ny, a.nz), dim3(SEG), 0, s>>>(a);

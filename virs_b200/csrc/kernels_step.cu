@@ -123,15 +123,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
             const float yp = sm[b][ty + 2][lane * VEC + k];
             const float xm = k == 0 ? left : cc[k - 1];
             const float xp = k == VEC - 1 ? right : cc[k + 1];
-            if (c >= CODE_HARD) {
-                if (c == CODE_NONE) r[k] = qv[k];
-                else if (c == CODE_WALL) r[k] = 0.f;
-                else {
-                    const uint32_t sn = __ldg(a.ctr);
-                    r[k] = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
-                }
+            if (c == CODE_WALL) {
+                r[k] = 0.f;
             } else if (c & CODE_BND) {
-                r[k] = qv[k]; // the boundary pass updates it
+                r[k] = qv[k]; // border and hard-source voxels keep theirs, the boundary pass updates boundary voxels
             } else {
                 r[k] = leapfrog(c, cc[k], xp, xm, yp, ym, cp[k], cm[k], qv[k], a.c2dt2, a.inv_h2);
             }
@@ -282,6 +277,14 @@ template <typename T> __device__ __forceinline__ void post_body(const PostArgs &
     using IO = Io<T>;
     T *Q = static_cast<T *>(a.q);
     const uint32_t sn = *a.ctr;
+    // hard-source voxels (flag 3, simulator_gpu.cu:59-63): the stencils leave
+    // them alone; their value of this step is written here, before the soft
+    // sources are added
+    if (a.nhpos) {
+        const T hv = IO::put(sn < a.nhard ? a.hard[sn] : 0.f);
+        for (uint32_t i = threadIdx.x; i < a.nhpos; i += blockDim.x) Q[a.hpos[i]] = hv;
+        __syncthreads();
+    }
     for (uint32_t i = threadIdx.x; i < a.nsrc; i += blockDim.x) {
         const float v = sn < a.siglen ? a.sig[(uint64_t)i * a.siglen + sn] : 0.f;
         const uint64_t j = a.src[i];

@@ -111,17 +111,29 @@ template <typename T, int TY> struct Stage {
 
 // the V cell codes of a thread (4 or 8 bytes)
 template <int V> struct Codes;
+// bytes with bit 7 clear and some other bit set: bit 7 of each byte of
+// ((w & 0x7f..) + 0x7f..) & ~w
+__device__ __forceinline__ uint32_t mirror_bytes(uint32_t w)
+{
+    return ((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) & ~w & 0x80808080u;
+}
 template <> struct Codes<4> {
     uint32_t w;
     __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint32_t *>(p); }
     __device__ bool any() const { return w != 0u; }
     __device__ uint32_t get(int k) const { return (w >> (8 * k)) & 0xffu; }
+    __device__ uint32_t mirror() const { return mirror_bytes(w); }
+    __device__ bool is_mirror(uint32_t m, int k) const { return (m >> (8 * k + 7)) & 1u; }
 };
 template <> struct Codes<8> {
     uint2 w;
     __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint2 *>(p); }
     __device__ bool any() const { return (w.x | w.y) != 0u; }
     __device__ uint32_t get(int k) const { return ((k < 4 ? w.x : w.y) >> (8 * (k & 3))) & 0xffu; }
+    // the mirror bytes of the two words folded into one: bit 7 of byte k
+    // (k < 4) from w.x, bit 6 of byte k - 4 from w.y
+    __device__ uint32_t mirror() const { return mirror_bytes(w.x) | (mirror_bytes(w.y) >> 1); }
+    __device__ bool is_mirror(uint32_t m, int k) const { return (m >> (8 * (k & 3) + (k < 4 ? 7 : 6))) & 1u; }
 };
 
 // waits for phase `parity` of *b for at most limit_ns; on timeout sets *err
@@ -151,7 +163,6 @@ template <typename T, int TY, int L> struct Tile {
     int x0, y0, z0, nst, row, sl, c0, t0;
     uint32_t j0;
     bool act, leader;
-    float hardv;
     float2 c2dt2, inv_h2;
     size_t plane;
 
@@ -219,24 +230,25 @@ template <typename T, int TY, int L> struct Tile {
             r[k] = o.x;
             r[k + 1] = o.y;
         }
-        // ... then the voxels with another code.  Border voxels and boundary
-        // voxels keep p^{n-1} (the boundary pass updates the latter from
-        // the untouched p^n buffer), walls take 0 and hard sources their
-        // value: selects, no divergence.  Only air next to a wall outside
-        // the boundary layer (a grid without a sponge layer) needs the
-        // update with the mirror rule.
+        // ... then the voxels with another code.  Walls take 0; border,
+        // hard-source and boundary voxels keep p^{n-1} (the post kernel
+        // writes the hard-source value, the boundary pass updates boundary
+        // voxels from the untouched p^n buffer): a test and a select per
+        // voxel, no divergence.  Only air next to a wall outside the
+        // boundary layer (a grid without a sponge layer) needs the update
+        // with the mirror rule; such codes have bit 7 clear and other bits
+        // set, found for four bytes at once.
         if (__any_sync(FULL, code.any())) {
-            unsigned mirror = 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 const uint32_t c = code.get(k);
-                if (c & CODE_BND) r[k] = c == CODE_WALL ? 0.f : (c == CODE_HARD ? hardv : qv[k]);
-                else if (c != 0u) mirror |= 1u << k;
+                if (c & CODE_BND) r[k] = c == CODE_WALL ? 0.f : qv[k];
             }
-            if (__any_sync(FULL, mirror != 0)) {
+            const uint32_t mirror = code.mirror();
+            if (__any_sync(FULL, mirror != 0u)) {
 #pragma unroll
                 for (int k = 0; k < V; ++k)
-                    if (mirror & (1u << k))
+                    if (code.is_mirror(mirror, k))
                         r[k] = leapfrog((uint8_t)code.get(k), cc[k], k == V - 1 ? right : cc[k + 1],
                                         k == 0 ? left : cc[k - 1], yp[k], ym[k], zp[k], zm[k], qv[k], a->c2dt2,
                                         a->inv_h2);
@@ -301,10 +313,6 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
 
     if (t.leader)
         for (int j = 0; j < D && j < t.nst; ++j) t.issue(j);
-
-    // the hard-source value of this step (flag-3 voxels)
-    const uint32_t sn = __ldg(a.ctr);
-    t.hardv = sn < a.nhard ? __ldg(a.hard + sn) : 0.f;
 
     float A[V], B[V], C[V];
     {
