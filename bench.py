@@ -285,15 +285,19 @@ def cpu_sample(shape, steps_budget_s, threads):
     osc = oracle_scene(sc, g)
     n = nx * ny * nzc
     st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
-    osc.run(1, state=st)                               # touch the pages
+    osc.run(4, state=st)                               # touch the pages, start the threads
     t0 = time.perf_counter()
-    osc.run(2, state=st, step0=1)
-    per_step = (time.perf_counter() - t0) / 2
-    # grow the crop to fill the budget: steps of the crop until ~budget
-    k = max(2, min(20000, int(steps_budget_s / max(per_step, 1e-6))))
-    t0 = time.perf_counter()
-    osc.run(k, state=st, step0=3)
-    dt = time.perf_counter() - t0
+    osc.run(4, state=st, step0=4)
+    per_step = (time.perf_counter() - t0) / 4
+    # chunks of about a second until the budget is spent
+    chunk = max(1, min(20000, int(1.0 / max(per_step, 1e-6))))
+    k, dt, step = 0, 0.0, 8
+    while dt < steps_budget_s and k < 200000:
+        t0 = time.perf_counter()
+        osc.run(chunk, state=st, step0=step)
+        dt += time.perf_counter() - t0
+        k += chunk
+        step += chunk
     return n * k / dt / 1e9, f"{k} steps of a {nx}x{ny}x{nzc} crop of the hall ({n * k / 1e9:.2f} G voxel updates)", dt
 
 
