@@ -87,7 +87,7 @@ struct virs_sim {
 
     // boundary
     uint64_t nb = 0;
-    DevBuf bidx, bpos, bmat, bw, state;
+    DevBuf bidx, bpos, bcode, bnrm, bmat, bw, state;
     DevBuf hpos;                   // hard-source voxel positions
     uint32_t nhpos = 0;
 
@@ -302,7 +302,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bpos, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
+                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
         b->release();
     VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
     VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
@@ -477,6 +477,8 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.l2 = s->l2;
     a.rigid = s->prm.rigid_walls ? 1 : 0;
     a.bmat = s->bmat.as<uint8_t>();
+    a.bcode = s->bcode.as<uint8_t>();
+    a.bnrm = s->bnrm.as<uint8_t>();
     a.bw = s->bw.as<float>();
     a.state = s->state.as<float>();
     a.coef = s->coef.as<float>();
@@ -833,6 +835,8 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(s->bidx.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary indices"));
         VIRS_TRY(s->bpos.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary positions"));
         VIRS_TRY(s->bmat.alloc(std::max<uint64_t>(nb, 1), "boundary materials"));
+        VIRS_TRY(s->bcode.alloc(std::max<uint64_t>(nb, 1), "boundary codes"));
+        VIRS_TRY(s->bnrm.alloc(std::max<uint64_t>(nb, 1), "boundary normals"));
         VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
         VIRS_TRY(s->side.alloc(std::max<uint64_t>(nb, 1) * sizeof(float4), "boundary records"));
         CompactArgs cp{};
@@ -844,6 +848,10 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         cp.bidx = s->bidx.as<uint32_t>();
         cp.bpos = s->bpos.as<uint32_t>();
         cp.bmat = s->bmat.as<uint8_t>();
+        cp.code = s->code.as<uint8_t>();
+        cp.normals = s->normals.as<uint8_t>();
+        cp.bcode = s->bcode.as<uint8_t>();
+        cp.bnrm = s->bnrm.as<uint8_t>();
         cp.bw = s->bw.as<float>();
         cp.nx = s->nx;
         cp.ny = s->ny;

@@ -74,6 +74,8 @@ struct StepArgs {
     const uint8_t *code;
     const uint8_t *normals; // air-neighbour mask (rigid-wall update)
     const uint32_t *bpos;   // [nb] padded device index of each boundary slot
+    const uint8_t *bcode;   // [nb] cell code of each slot's voxel (read in slot order, not gathered)
+    const uint8_t *bnrm;    // [nb] air-neighbour mask of each slot's voxel (rigid-wall update)
     const uint8_t *bmat;
     const float *bw;
     float *state;           // [S][4][nb]
@@ -180,6 +182,9 @@ struct CompactArgs {
     const float *wtab;         // sponge weight per d2
     uint32_t *bidx;
     uint32_t *bpos;            // padded device index of each slot's voxel
+    const uint8_t *code;       // padded cell codes and air-neighbour masks
+    const uint8_t *normals;
+    uint8_t *bcode, *bnrm;     // ... copied per slot
     uint8_t *bmat;
     float *bw;
     uint32_t nx, ny, nz, px, spr;

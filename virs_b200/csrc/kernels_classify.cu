@@ -169,6 +169,8 @@ __global__ void k_compact(const CompactArgs a)
     const uint64_t slot = (uint64_t)a.bseg[((size_t)z * ny + y) * a.spr + blockIdx.x] + before;
     a.bidx[slot] = (uint32_t)(((uint64_t)z * ny + y) * nx + x);
     a.bpos[slot] = (uint32_t)i;
+    a.bcode[slot] = a.code[i];
+    a.bnrm[slot] = a.normals[i];
     a.bmat[slot] = a.bmat_full[i];
     a.bw[slot] = a.wtab[a.bd2_full[i]];
 }

@@ -183,8 +183,8 @@ __device__ __forceinline__ void bvox_load(const StepArgs &a, uint64_t slot, BVox
     const T *P = static_cast<const T *>(a.p);
     const T *Q = static_cast<const T *>(a.q);
     v.i = i;
-    v.c = __ldg(a.code + i);
-    v.nm = a.rigid ? __ldg(a.normals + i) : 0;
+    v.c = __ldg(a.bcode + slot);
+    v.nm = a.rigid ? __ldg(a.bnrm + slot) : 0;
     v.ce = IO::get(P[i]);
     v.qv = IO::get(Q[i]);
     v.nb[0] = IO::get(P[i + 1]);
@@ -220,10 +220,12 @@ __device__ __forceinline__ void bvox_update(const StepArgs &a, uint64_t slot, co
 
 // The compacted boundary pass (simulator_gpu.cu:105-150), in list order.
 // The stencil kernels left these voxels untouched (p^{n-1} in place); the
-// pass gathers the seven p values, p^{n-1} and the code of each voxel from
-// the p^n buffer (not written during the step), computes the leapfrog
-// update with the wall mirror (or the rigid-wall update), then the filter
-// correction, and writes p^{n+1}.  A thread takes two slots, BT apart, and
+// pass gathers the seven p values from the p^n buffer (not written during
+// the step) and p^{n-1}, reads the voxel's code from the per-slot copy made
+// at classification (in slot order: no 32-byte sector fetched for one
+// byte), computes the leapfrog update with the wall mirror (or the
+// rigid-wall update), then the filter correction, and writes p^{n+1}.  A
+// thread takes two slots, BT apart, and
 // issues all loads of both before any arithmetic: the pass is bound by the
 // latency of its gathers, and two independent voxels in flight hide it.
 //   BND_UPDATE  the step
