@@ -130,6 +130,39 @@ virs_status virs_set_mesh(virs_sim *sim, const float *verts, size_t nverts, cons
 virs_status virs_set_grid(virs_sim *sim, uint64_t nx, uint64_t ny, uint64_t nz, float cell_size,
                           const uint8_t *flags, const uint8_t *wall_material);
 
+/* z-slabs: one grid over several GPUs (no reference counterpart, which runs
+ * one grid on one GPU; the step is a nearest-neighbour stencil, so a split
+ * along z needs one plane of p^n from each neighbour per step).  The interior
+ * planes 1..nz-2 of an nx*ny*nz grid are split into contiguous ranges, one
+ * per handle.  A slab handle owns the planes [z_lo, z_hi)
+ * (1 <= z_lo < z_hi <= nz-1) and keeps one ghost plane on each side: its
+ * own grid is nx*ny*(z_hi - z_lo + 2), local plane k = global plane
+ * z_lo - 1 + k, and voxel indices given to it (sources, receivers) are
+ * local.  At a global border the ghost is the border plane itself (never
+ * written, 0).  flags / wall_material (NULL: absorber 0) hold the global
+ * planes [z_first, z_first + nz_ext), which must include the planes
+ * max(0, z_lo - W - 2) .. min(nz, z_hi + W + 2) - 1 for sponge width W:
+ * virs_classify classifies them all and keeps the slab's planes, so the
+ * sponge layer, normals, cell codes and boundary list of the owned planes
+ * are the whole grid's.  Before every step the caller copies the
+ * neighbours' first / last owned planes of p^n into the ghost planes
+ * (virs_slab_planes); the slabs then advance exactly as the whole grid.
+ * 16-bit storage needs an explicit storage_scale (every slab stores
+ * alike). */
+virs_status virs_set_grid_slab(virs_sim *sim, uint64_t nx, uint64_t ny, uint64_t nz, float cell_size, uint64_t z_lo,
+                               uint64_t z_hi, const uint8_t *flags, const uint8_t *wall_material, uint64_t z_first,
+                               uint64_t nz_ext);
+
+/* Device addresses of the planes of p^n (the state the next step reads)
+ * that a slab exchanges before that step, each plane_bytes long (rows of nx
+ * rounded up to 32 voxels, in the storage type): first / last = its first
+ * and last owned planes (sent to the slab below / above), ghost_lo /
+ * ghost_hi = its ghost planes (received from the slab below / above).
+ * They alternate between two buffers from step to step: ask before each
+ * step, after queueing the previous one. */
+virs_status virs_slab_planes(const virs_sim *sim, void **first, void **last, void **ghost_lo, void **ghost_hi,
+                             size_t *plane_bytes);
+
 virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);
 
 /* Replaces buildSpongeLayer / buildSpongeLayerGPU (simulator_dispatch.cpp:83-91,
@@ -139,8 +172,11 @@ virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);
  * All on the GPU. */
 virs_status virs_classify(virs_sim *sim);
 
-/* Parity exports (reference layout). */
+/* Parity exports (reference layout).  Flags are the voxeliser's (0..3)
+ * before virs_classify and the classified ones after; wall materials are
+ * the absorber index of each wall voxel as voxelised or set. */
 virs_status virs_get_flags(const virs_sim *sim, uint8_t *out, size_t n);
+virs_status virs_get_wall_materials(const virs_sim *sim, uint8_t *out, size_t n);
 virs_status virs_get_normals(const virs_sim *sim, uint8_t *out, size_t n);
 virs_status virs_get_boundary_indices(const virs_sim *sim, uint32_t *out, size_t n);
 /* per boundary voxel (list order): material index and sponge weight */

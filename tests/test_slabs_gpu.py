@@ -1,0 +1,121 @@
+"""z-slabs on one GPU: a grid split into slab handles whose ghost planes are
+refreshed from their neighbours before every step advances exactly as the
+whole grid, bit for bit: classification of the owned planes (flags,
+normals, boundary list, materials, weights), receiver samples and fields.
+
+The exchange here is `slabs.exchange_local` (device copies on the current
+stream between handles of one process); across processes the same planes
+go through torch.distributed (`slabs.exchange`, covered on CPU by
+test_slabs.py)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from virs_b200 import capi, scenes, slabs
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(steps):
+    # boxes, 4 materials, 3-section cascades; sponge 6 so the classification
+    # halo of the slabs matters; a soft source and receivers spread in z
+    sc = scenes.furnished_room(steps=steps)
+    return dataclasses.replace(sc, cell_size=1 / 32, sponge_width=6)
+
+
+def _run_slabs(parts, steps):
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(steps):
+        slabs.exchange_local([p[0] for p in parts])
+        for s, *_ in parts:
+            s.run(1, stream=stream)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_slabs_match_whole_grid_f32(nparts):
+    sc = _scene(240)
+    whole, meta = scenes.build_simulation(sc)
+    nx, ny, nz = meta["shape"]
+    plane = nx * ny
+    wf, wn, wb = whole.flags(), whole.normals(), whole.boundary_indices()
+    wm, ww = whole.boundary_materials()
+    parts, pmeta = scenes.build_slabs(sc, nparts)
+    assert pmeta["shape"] == meta["shape"]
+    got_b, got_m, got_w = [], [], []
+    for s, z_lo, z_hi, _ in parts:
+        assert s.shape == (nx, ny, z_hi - z_lo + 2)
+        own = slice(plane, (z_hi - z_lo + 1) * plane)       # local planes 1 .. nz_local-2
+        gown = slice(z_lo * plane, z_hi * plane)
+        assert np.array_equal(s.flags()[own], wf[gown])
+        assert np.array_equal(s.normals()[own], wn[gown])
+        b = s.boundary_indices().astype(np.int64) + (z_lo - 1) * plane
+        m, w = s.boundary_materials()
+        got_b.append(b)
+        got_m.append(m)
+        got_w.append(w)
+    # the slabs' boundary lists, in slab order, are the whole grid's list
+    assert np.array_equal(np.concatenate(got_b), wb.astype(np.int64))
+    assert np.array_equal(np.concatenate(got_m), wm)
+    assert np.array_equal(np.concatenate(got_w).view(np.uint32), ww.view(np.uint32))
+
+    whole.run(sc.steps)
+    want_ir = whole.ir()
+    want_p, want_pp = whole.pressure(prev=True)
+    _run_slabs(parts, sc.steps)
+    ir = np.zeros_like(want_ir)
+    for s, z_lo, z_hi, own_r in parts:
+        if own_r.any():
+            ir[own_r] = s.ir()
+        p, pp = s.pressure(prev=True)
+        gown = slice(z_lo * plane, z_hi * plane)
+        assert np.array_equal(p[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_p[gown].view(np.uint32))
+        assert np.array_equal(pp[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_pp[gown].view(np.uint32))
+    assert sum(int(o.sum()) for *_, o in parts) == want_ir.shape[0]
+    assert np.abs(want_ir).max() > 0
+    assert np.array_equal(ir.view(np.uint32), want_ir.view(np.uint32))
+    for s, *_ in parts:
+        s.close()
+    whole.close()
+
+
+def test_slabs_match_whole_grid_bf16():
+    """16-bit storage with the same explicit scale on every handle."""
+    sc = _scene(160)
+    scale = 64.0
+    whole, meta = scenes.build_simulation(sc, storage=capi.STORAGE_BF16, storage_scale=scale)
+    parts, _ = scenes.build_slabs(sc, 2, storage=capi.STORAGE_BF16, storage_scale=scale)
+    whole.run(sc.steps)
+    want_ir = whole.ir()
+    _run_slabs(parts, sc.steps)
+    ir = np.zeros_like(want_ir)
+    for s, _, _, own_r in parts:
+        if own_r.any():
+            ir[own_r] = s.ir()
+    assert np.abs(want_ir).max() > 0
+    assert np.array_equal(ir.view(np.uint32), want_ir.view(np.uint32))
+    for s, *_ in parts:
+        s.close()
+    whole.close()
+
+
+def test_slab_arguments_checked():
+    sc = _scene(10)
+    with capi.Simulation(capi.default_params(sponge_width=6)) as s:
+        flags = np.zeros((40, 8, 8), np.uint8)
+        # owned planes outside 1 .. nz-2
+        with pytest.raises(capi.VirsError):
+            s.set_grid_slab((8, 8, 40), 0.1, 0, 10, flags)
+        # flags that miss the classification halo (W + 1 = 7 planes beyond the ghost)
+        with pytest.raises(capi.VirsError):
+            s.set_grid_slab((8, 8, 40), 0.1, 20, 30, flags[12:32], z_first=12)
+        s.set_grid_slab((8, 8, 40), 0.1, 20, 30, flags[12:38], z_first=12)
+        assert s.shape == (8, 8, 12)
+        first, last, glo, ghi, nb = s.slab_planes()
+        assert nb == 32 * 8 * 4 and first - glo == nb and ghi - last == nb
+    with capi.Simulation(capi.default_params(storage=capi.STORAGE_BF16)) as s:
+        with pytest.raises(capi.VirsError):  # 16-bit slabs need an explicit scale
+            s.set_grid_slab((8, 8, 40), 0.1, 1, 20, np.zeros((40, 8, 8), np.uint8))
+    del sc

@@ -66,9 +66,14 @@ _SIGS = {
     "virs_set_mesh": ([_P, _P, C.c_size_t, _P, _P, C.c_size_t], C.c_int),
     "virs_set_grid": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, _P, _P], C.c_int),
     "virs_get_grid_info": ([_P, _P], C.c_int),
+    "virs_set_grid_slab": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_uint64, C.c_uint64, _P, _P,
+                            C.c_uint64, C.c_uint64], C.c_int),
+    "virs_slab_planes": ([_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                          C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)], C.c_int),
     "virs_classify": ([_P], C.c_int),
     "virs_get_flags": ([_P, _P, C.c_size_t], C.c_int),
     "virs_get_normals": ([_P, _P, C.c_size_t], C.c_int),
+    "virs_get_wall_materials": ([_P, _P, C.c_size_t], C.c_int),
     "virs_get_boundary_indices": ([_P, _P, C.c_size_t], C.c_int),
     "virs_get_boundary_materials": ([_P, _P, _P, C.c_size_t], C.c_int),
     "virs_set_filters": ([_P, C.c_uint32, C.c_uint32, _P], C.c_int),
@@ -246,6 +251,28 @@ class Simulation:
         w = None if wall_material is None else _c(wall_material, np.uint8)
         check(lib().virs_set_grid(self._h, nx, ny, nz, cell_size, _ptr(f), _ptr(w)))
 
+    def set_grid_slab(self, shape, cell_size, z_lo, z_hi, flags, wall_material=None, z_first=0):
+        """One z-slab of the grid `shape` owning global planes [z_lo, z_hi);
+        flags / wall_material hold global planes z_first.. (their first axis
+        is z)."""
+        nx, ny, nz = shape
+        f = _c(flags, np.uint8).reshape(-1)
+        nz_ext = f.size // (nx * ny)
+        if nz_ext * nx * ny != f.size:
+            raise ValueError("flags must hold whole planes of nx*ny voxels")
+        w = None if wall_material is None else _c(wall_material, np.uint8).reshape(-1)
+        if w is not None and w.size != f.size:
+            raise ValueError("wall_material must match flags")
+        check(lib().virs_set_grid_slab(self._h, nx, ny, nz, cell_size, z_lo, z_hi, _ptr(f), _ptr(w), z_first, nz_ext))
+
+    def slab_planes(self):
+        """(first, last, ghost_lo, ghost_hi, plane_bytes): device addresses of
+        the planes of p^n a slab exchanges before its next step."""
+        v = [C.c_void_p() for _ in range(4)]
+        nb = C.c_size_t()
+        check(lib().virs_slab_planes(self._h, *[C.byref(x) for x in v], C.byref(nb)))
+        return tuple(int(x.value or 0) for x in v) + (int(nb.value),)
+
     def info(self) -> GridInfo:
         g = GridInfo()
         check(lib().virs_get_grid_info(self._h, C.byref(g)))
@@ -267,6 +294,11 @@ class Simulation:
     def flags(self) -> np.ndarray:
         out = np.empty(self.nvox, np.uint8)
         check(lib().virs_get_flags(self._h, _ptr(out), out.size))
+        return out
+
+    def wall_materials(self) -> np.ndarray:
+        out = np.empty(self.nvox, np.uint8)
+        check(lib().virs_get_wall_materials(self._h, _ptr(out), out.size))
         return out
 
     def normals(self) -> np.ndarray:

@@ -85,6 +85,13 @@ struct virs_sim {
     DevBuf field[2];
     int cur = 0;
 
+    // z-slab of a larger grid (virs_set_grid_slab): flags_raw / wall_mat
+    // hold ext_nz planes, classified together; the grid kept (nz planes,
+    // the owned planes and a ghost plane each side) starts slab_drop planes
+    // into them.  For a whole grid ext_nz == nz and slab_drop == 0.
+    bool slab = false;
+    uint32_t ext_nz = 0, slab_drop = 0;
+
     // boundary
     uint64_t nb = 0;
     DevBuf bidx, bpos, bcode, bnrm, bmat, bw, state;
@@ -251,10 +258,10 @@ bool interior(const virs_sim *s, uint64_t ref)
 
 // pitched copies between the reference layout (rows of nx) and the device
 // layout (rows of px)
-virs_status h2d_rows(void *dst, const void *src, size_t elem, const virs_sim *s)
+virs_status h2d_rows(void *dst, const void *src, size_t elem, const virs_sim *s, size_t planes = 0)
 {
     VIRS_CUDA(cudaMemcpy2D(dst, (size_t)s->px * elem, src, (size_t)s->nx * elem, (size_t)s->nx * elem,
-                           (size_t)s->ny * s->nz, cudaMemcpyHostToDevice));
+                           (size_t)s->ny * (planes ? planes : s->nz), cudaMemcpyHostToDevice));
     return VIRS_OK;
 }
 
@@ -271,11 +278,14 @@ virs_status wait_done(const virs_sim *s)
     return VIRS_OK;
 }
 
-// allocate the grid-sized buffers and upload flags / wall materials
+// allocate the grid-sized buffers and upload flags / wall materials.  For a
+// slab (keep > 0) the nz planes uploaded are classified together and the
+// grid kept is `keep` planes from `drop` on.
 virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h, const uint8_t *flags,
-                         const uint8_t *wmat)
+                         const uint8_t *wmat, uint64_t keep = 0, uint64_t drop = 0)
 {
     if (nx < 3 || ny < 3 || nz < 3) return fail(VIRS_E_ARG, "grid must be at least 3 voxels along each axis");
+    if (keep && (keep < 3 || drop + keep > nz)) return fail(VIRS_E_ARG, "slab planes outside the uploaded range");
     if (nx > (1u << 30) || ny > (1u << 30) || nz > (1u << 30) || ((nx + 31) / 32 * 32) * ny * nz >= (1ull << 32))
         return fail(VIRS_E_ARG, "grid too large: voxel positions are 32-bit (nx rounded up to 32, times ny*nz, < 2^32)");
     if (!finite_pos(h)) return fail(VIRS_E_ARG, "cell size must be finite and positive");
@@ -288,6 +298,10 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
         for (size_t i = 0; i < n; ++i) mx = std::max(mx, wmat[i]);
     s->drop_graphs();
     s->has_grid = s->classified = false;
+    s->slab = keep != 0;
+    s->ext_nz = (uint32_t)nz;
+    s->slab_drop = (uint32_t)drop;
+    if (keep) nz = keep;
     s->nx = (uint32_t)nx;
     s->ny = (uint32_t)ny;
     s->nz = (uint32_t)nz;
@@ -296,7 +310,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     // array are 16-byte aligned for the TMA
     s->spr = ((s->px + SEG - 1) / SEG + 3) / 4 * 4;
     s->nvox = (size_t)s->px * ny * nz;
-    s->nref = n;
+    s->nref = (size_t)nx * ny * nz;
     s->h = h;
     s->max_wall_mat = mx;
     compute_constants(s);
@@ -304,10 +318,11 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
                       &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
         b->release();
-    VIRS_TRY(s->flags_raw.alloc(s->nvox, "flags"));
-    VIRS_TRY(s->wall_mat.alloc(s->nvox, "wall materials"));
-    if (flags) VIRS_TRY(h2d_rows(s->flags_raw.ptr, flags, 1, s));
-    if (wmat) VIRS_TRY(h2d_rows(s->wall_mat.ptr, wmat, 1, s));
+    const size_t ext = (size_t)s->px * ny * s->ext_nz;
+    VIRS_TRY(s->flags_raw.alloc(ext, "flags"));
+    VIRS_TRY(s->wall_mat.alloc(ext, "wall materials"));
+    if (flags) VIRS_TRY(h2d_rows(s->flags_raw.ptr, flags, 1, s, s->ext_nz));
+    if (wmat) VIRS_TRY(h2d_rows(s->wall_mat.ptr, wmat, 1, s, s->ext_nz));
     VIRS_TRY(s->flags.alloc(s->nvox, "classified flags"));
     VIRS_TRY(s->field[0].alloc(s->nvox * s->storage_bytes(), "pressure field"));
     VIRS_TRY(s->field[1].alloc(s->nvox * s->storage_bytes(), "pressure field"));
@@ -742,6 +757,49 @@ VIRS_EXPORT virs_status virs_set_grid(virs_sim *s, uint64_t nx, uint64_t ny, uin
     return VIRS_OK;
 }
 
+// planes of flags a slab needs on each side of its own grid for the sponge
+// classification of its planes: the ghost plane is classified too, and a
+// voxel's class depends on the walls within W planes
+static uint64_t slab_halo(const virs_sim *s) { return (uint64_t)s->prm.sponge_width + 1; }
+
+VIRS_EXPORT virs_status virs_set_grid_slab(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h, uint64_t z_lo,
+                                           uint64_t z_hi, const uint8_t *flags, const uint8_t *wmat, uint64_t z_first,
+                                           uint64_t nz_ext)
+{
+    if (!s || !flags) return fail(VIRS_E_ARG, "virs_set_grid_slab: null argument");
+    if (nz < 3 || z_lo < 1 || z_hi <= z_lo || z_hi > nz - 1)
+        return fail(VIRS_E_ARG, "virs_set_grid_slab: owned planes must satisfy 1 <= z_lo < z_hi <= nz - 1");
+    const uint64_t H = slab_halo(s);
+    const uint64_t need_lo = z_lo - 1 >= H ? z_lo - 1 - H : 0;
+    const uint64_t need_hi = std::min<uint64_t>(nz, z_hi + 1 + H);
+    if (z_first > need_lo || z_first + nz_ext < need_hi || z_first + nz_ext > nz)
+        return fail(VIRS_E_ARG, "virs_set_grid_slab: flags must cover planes " + std::to_string(need_lo) + ".." +
+                                    std::to_string(need_hi - 1) + " (the slab, its ghost planes and sponge width + 1 "
+                                    "planes beyond) and stay inside the grid");
+    if (s->prm.storage != VIRS_STORAGE_F32 && !(s->prm.storage_scale > 0.f))
+        return fail(VIRS_E_ARG, "virs_set_grid_slab: 16-bit storage needs an explicit storage_scale, the same on every slab");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(install_grid(s, nx, ny, nz_ext, h, flags, wmat, z_hi - z_lo + 2, z_lo - 1 - z_first));
+    s->bmin[0] = s->bmin[1] = s->bmin[2] = 0.f;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_slab_planes(const virs_sim *s, void **first, void **last, void **ghost_lo,
+                                         void **ghost_hi, size_t *plane_bytes)
+{
+    if (!s || !first || !last || !ghost_lo || !ghost_hi || !plane_bytes)
+        return fail(VIRS_E_ARG, "virs_slab_planes: null argument");
+    if (!s->slab) return fail(VIRS_E_STATE, "virs_slab_planes: not a slab (virs_set_grid_slab)");
+    const size_t pb = (size_t)s->px * s->ny * s->storage_bytes();
+    char *p = s->field[s->cur].as<char>(); // p^n: the state the next step reads
+    *ghost_lo = p;
+    *first = p + pb;
+    *last = p + (size_t)(s->nz - 2) * pb;
+    *ghost_hi = p + (size_t)(s->nz - 1) * pb;
+    *plane_bytes = pb;
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_get_grid_info(const virs_sim *s, virs_grid_info *o)
 {
     if (!s || !o) return fail(VIRS_E_ARG, "virs_get_grid_info: null argument");
@@ -769,27 +827,47 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
     cudaStream_t st = s->stream;
     const int W = s->prm.sponge_width;
     {
-        DevBuf k1, k2, bmat_full, bd2_full, segcnt_tmp, scan_tmp, total, wtab;
-        VIRS_TRY(k1.alloc(s->nvox * 4, "sponge scratch"));
-        VIRS_TRY(k2.alloc(s->nvox * 4, "sponge scratch"));
-        VIRS_TRY(bmat_full.alloc(s->nvox, "sponge scratch"));
-        VIRS_TRY(bd2_full.alloc(s->nvox * 2, "sponge scratch"));
+        // the sponge layer over every uploaded plane (for a slab, its halo
+        // planes too), then only the kept planes
+        const size_t nvc = (size_t)s->px * s->ny * s->ext_nz;
+        DevBuf k1, k2, bmat_full, bd2_full, segcnt_tmp, scan_tmp, total, wtab, flags_ext;
+        VIRS_TRY(k1.alloc(nvc * 4, "sponge scratch"));
+        VIRS_TRY(k2.alloc(nvc * 4, "sponge scratch"));
+        VIRS_TRY(bmat_full.alloc(nvc, "sponge scratch"));
+        VIRS_TRY(bd2_full.alloc(nvc * 2, "sponge scratch"));
+        if (s->slab) VIRS_TRY(flags_ext.alloc(nvc, "sponge scratch"));
         ClassifyArgs ca{};
         ca.flags_in = s->flags_raw.as<uint8_t>();
         ca.wall_mat = s->wall_mat.as<uint8_t>();
-        ca.flags_out = s->flags.as<uint8_t>();
+        ca.flags_out = (s->slab ? flags_ext : s->flags).as<uint8_t>();
         ca.bmat_full = bmat_full.as<uint8_t>();
         ca.bd2_full = bd2_full.as<uint16_t>();
         ca.k1 = k1.as<uint32_t>();
         ca.k2 = k2.as<uint32_t>();
         ca.nx = s->nx;
         ca.ny = s->ny;
-        ca.nz = s->nz;
+        ca.nz = s->ext_nz;
         ca.px = s->px;
         ca.W = W;
         VIRS_CUDA(launch_sponge(ca, st));
         k1.release();
         k2.release();
+        if (s->slab) {
+            // planes are contiguous: one copy per array
+            const size_t off = (size_t)s->slab_drop * s->px * s->ny;
+            DevBuf bm, bd;
+            VIRS_TRY(bm.alloc(s->nvox, "sponge scratch"));
+            VIRS_TRY(bd.alloc(s->nvox * 2, "sponge scratch"));
+            VIRS_CUDA(cudaMemcpyAsync(s->flags.ptr, flags_ext.as<uint8_t>() + off, s->nvox, cudaMemcpyDeviceToDevice, st));
+            VIRS_CUDA(cudaMemcpyAsync(bm.ptr, bmat_full.as<uint8_t>() + off, s->nvox, cudaMemcpyDeviceToDevice, st));
+            VIRS_CUDA(cudaMemcpyAsync(bd.ptr, bd2_full.as<uint16_t>() + off, s->nvox * 2, cudaMemcpyDeviceToDevice, st));
+            VIRS_CUDA(cudaStreamSynchronize(st));
+            std::swap(bmat_full.ptr, bm.ptr);
+            std::swap(bmat_full.bytes, bm.bytes);
+            std::swap(bd2_full.ptr, bd.ptr);
+            std::swap(bd2_full.bytes, bd.bytes);
+            flags_ext.release();
+        }
 
         const size_t nseg = (size_t)s->spr * s->ny * s->nz;
         VIRS_TRY(s->code.alloc(s->nvox, "cell codes"));
@@ -876,7 +954,19 @@ VIRS_EXPORT virs_status virs_get_flags(const virs_sim *s, uint8_t *out, size_t n
     if (n < s->nref) return fail(VIRS_E_ARG, "virs_get_flags: buffer smaller than nx*ny*nz");
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
-    return d2h_rows(out, (s->classified ? s->flags : s->flags_raw).ptr, 1, s);
+    if (s->classified) return d2h_rows(out, s->flags.ptr, 1, s);
+    // a slab's kept planes of the uploaded flags
+    return d2h_rows(out, s->flags_raw.as<uint8_t>() + (size_t)s->slab_drop * s->px * s->ny, 1, s);
+}
+
+VIRS_EXPORT virs_status virs_get_wall_materials(const virs_sim *s, uint8_t *out, size_t n)
+{
+    if (!s || !out) return fail(VIRS_E_ARG, "virs_get_wall_materials: null argument");
+    if (!s->has_grid) return fail(VIRS_E_STATE, "no grid");
+    if (n < s->nref) return fail(VIRS_E_ARG, "virs_get_wall_materials: buffer smaller than nx*ny*nz");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    return d2h_rows(out, s->wall_mat.as<uint8_t>() + (size_t)s->slab_drop * s->px * s->ny, 1, s);
 }
 
 VIRS_EXPORT virs_status virs_get_normals(const virs_sim *s, uint8_t *out, size_t n)

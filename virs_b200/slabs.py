@@ -1,0 +1,138 @@
+"""z-slabs: one grid split along z over several GPUs, one process per GPU.
+
+The step is a 7-point stencil, so a split along z needs one exchange per
+step: every slab sends its first and last owned planes of p^n to the slabs
+below and above and receives theirs into its two ghost planes
+(`virs_set_grid_slab`, `virs_slab_planes` in include/virs.h).  Boundary
+lists, filter states, sources and receivers partition with their voxels;
+nothing else crosses between slabs.  The reference runs one grid on one GPU
+(src/simulator/simulator_gpu.cu:184-332); with the ghost planes exchanged
+before every step the slabs advance exactly as that grid.
+
+Exchanges go through torch.distributed point-to-point operations
+(`batch_isend_irecv`): NCCL over NVLink between GPUs, gloo between CPU
+processes.  The planes are plain device buffers of the library, wrapped as
+uint8 tensors without copies.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def split_planes(nz: int, parts: int) -> list[tuple[int, int]]:
+    """The interior planes 1 .. nz-2 of a grid split into `parts` contiguous
+    ranges [z_lo, z_hi) of sizes differing by at most one."""
+    inner = nz - 2
+    if parts < 1 or inner < parts:
+        raise ValueError(f"cannot split {inner} interior planes into {parts} slabs")
+    base, extra = divmod(inner, parts)
+    out, z = [], 1
+    for r in range(parts):
+        n = base + (1 if r < extra else 0)
+        out.append((z, z + n))
+        z += n
+    return out
+
+
+def flag_range(nz: int, z_lo: int, z_hi: int, sponge_width: int) -> tuple[int, int]:
+    """(z_first, nz_ext): the global planes of flags a slab owning
+    [z_lo, z_hi) needs: its ghost planes and sponge_width + 1 planes beyond,
+    for the classification of its planes."""
+    h = sponge_width + 1
+    lo = max(0, z_lo - 1 - h)
+    hi = min(nz, z_hi + 1 + h)
+    return lo, hi - lo
+
+
+def local_index(idx, shape, z_lo: int, z_hi: int):
+    """Global voxel indices -> (mask of those owned by the slab [z_lo, z_hi),
+    their indices in the slab's own grid, whose plane 0 is z_lo - 1)."""
+    nx, ny, _ = shape
+    idx = np.asarray(idx, np.uint64).reshape(-1)
+    z = idx // np.uint64(nx * ny)
+    own = (z >= z_lo) & (z < z_hi)
+    loc = idx[own] - np.uint64((z_lo - 1) * nx * ny)
+    return own, loc
+
+
+class _DeviceBytes:
+    """`n` bytes of device memory at `ptr`, for torch.as_tensor."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def device_bytes(ptr: int, n: int):
+    """A uint8 CUDA tensor viewing `n` bytes at device address `ptr`."""
+    import torch
+    return torch.as_tensor(_DeviceBytes(ptr, n), device="cuda")
+
+
+def exchange(first, last, ghost_lo, ghost_hi, rank: int, world: int, group=None) -> None:
+    """One halo exchange between neighbouring slabs: `first` goes to rank-1
+    (into its `ghost_hi`), `last` to rank+1 (into its `ghost_lo`); this rank's
+    ghost planes are filled from theirs.  All ranks call it at every step;
+    the end ranks have one neighbour.  Tensors may be CPU (gloo) or CUDA
+    (NCCL); the call returns when the receives are complete (on the current
+    stream for NCCL)."""
+    import torch.distributed as dist
+    ops = []
+    if rank > 0:
+        ops.append(dist.P2POp(dist.isend, first, rank - 1, group))
+        ops.append(dist.P2POp(dist.irecv, ghost_lo, rank - 1, group))
+    if rank < world - 1:
+        ops.append(dist.P2POp(dist.isend, last, rank + 1, group))
+        ops.append(dist.P2POp(dist.irecv, ghost_hi, rank + 1, group))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+
+
+def exchange_local(sims) -> None:
+    """The same exchange between slab handles of one process (one GPU or
+    several), as copies on the current torch stream: sims[r] owns the r-th
+    range from the bottom."""
+    planes = [s.slab_planes() for s in sims]
+    for r in range(len(sims)):
+        nb = planes[r][4]
+        if r > 0:
+            device_bytes(planes[r][2], nb).copy_(device_bytes(planes[r - 1][1], planes[r - 1][4]))
+        if r + 1 < len(sims):
+            device_bytes(planes[r][3], nb).copy_(device_bytes(planes[r + 1][0], planes[r + 1][4]))
+
+
+class SlabRun:
+    """Drives one slab of a distributed grid: per step, the halo exchange
+    with the neighbouring ranks, then the step on the current torch stream.
+
+    `sim` is a capi.Simulation set up with `setup_slab`, classified,
+    configured and started; every rank runs the same number of steps."""
+
+    def __init__(self, sim, rank: int, world: int, group=None):
+        self.sim, self.rank, self.world, self.group = sim, rank, world, group
+
+    def run(self, steps: int) -> None:
+        import torch
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(steps):
+            first, last, glo, ghi, nb = self.sim.slab_planes()
+            exchange(device_bytes(first, nb), device_bytes(last, nb), device_bytes(glo, nb), device_bytes(ghi, nb),
+                     self.rank, self.world, self.group)
+            self.sim.run(1, stream=stream)
+
+
+def setup_slab(sim, shape, cell_size: float, flags, wall_material, rank: int, world: int, sponge_width: int):
+    """Install this rank's slab of the global grid `shape` from the global
+    flags / wall materials ([nz][ny][nx] or flat, host arrays); returns its
+    owned planes (z_lo, z_hi)."""
+    nx, ny, nz = shape
+    z_lo, z_hi = split_planes(nz, world)[rank]
+    z_first, n_ext = flag_range(nz, z_lo, z_hi, sponge_width)
+    plane = nx * ny
+    f = np.ascontiguousarray(flags, np.uint8).reshape(-1)[z_first * plane:(z_first + n_ext) * plane]
+    w = None
+    if wall_material is not None:
+        w = np.ascontiguousarray(wall_material, np.uint8).reshape(-1)[z_first * plane:(z_first + n_ext) * plane]
+    sim.set_grid_slab(shape, cell_size, z_lo, z_hi, f, w, z_first)
+    return z_lo, z_hi
