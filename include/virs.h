@@ -153,6 +153,21 @@ virs_status virs_set_grid_slab(virs_sim *sim, uint64_t nx, uint64_t ny, uint64_t
                                uint64_t z_hi, const uint8_t *flags, const uint8_t *wall_material, uint64_t z_first,
                                uint64_t nz_ext);
 
+/* The same from a mesh, for slab `part` of `parts` (0 <= part < parts): the
+ * whole grid is sized from the mesh as virs_set_mesh / virs_load_obj size
+ * it, its interior planes are split into `parts` ranges whose sizes differ
+ * by at most one (lower ranges first), and only this slab's uploaded planes
+ * are voxelised, with the whole grid's origin, so every flag equals the
+ * whole grid's.  No handle ever holds the whole grid.  bbox_min in
+ * virs_get_grid_info is the whole grid's origin. */
+virs_status virs_set_mesh_slab(virs_sim *sim, const float *verts, size_t nverts, const uint32_t *tris,
+                               const int32_t *tri_material, size_t ntris, uint32_t part, uint32_t parts);
+virs_status virs_load_obj_slab(virs_sim *sim, const char *path, uint32_t part, uint32_t parts);
+
+/* Owned planes [*z_lo, *z_hi) of a slab and the planes *nz of its whole
+ * grid; VIRS_E_STATE for a handle that is not a slab. */
+virs_status virs_get_slab_info(const virs_sim *sim, uint64_t *z_lo, uint64_t *z_hi, uint64_t *nz);
+
 /* Device addresses of the planes of p^n (the state the next step reads)
  * that a slab exchanges before that step, each plane_bytes long (rows of nx
  * rounded up to 32 voxels, in the storage type): first / last = its first

@@ -12,6 +12,7 @@ import dataclasses
 import numpy as np
 import pytest
 
+import oracle
 from virs_b200 import capi, scenes, slabs
 
 pytestmark = pytest.mark.gpu
@@ -24,6 +25,37 @@ def _scene(steps):
     return dataclasses.replace(sc, cell_size=1 / 32, sponge_width=6)
 
 
+def test_mesh_slab_flags_equal_whole_grid():
+    """Each slab voxelises only its planes of the mesh (global origin and
+    sizes): its flags and wall materials equal the whole grid's planes."""
+    sc = _scene(10)
+    p = capi.default_params(courant=sc.courant, cell_size=sc.cell_size, bbox_nudge=sc.nudge,
+                            sponge_width=sc.sponge_width)
+    with capi.Simulation(p) as whole:
+        whole.set_material_roles(sc.roles)
+        whole.set_mesh(sc.verts, sc.tris, sc.tri_mat)
+        wf, wm = whole.flags(), whole.wall_materials()
+        nx, ny, nz = whole.shape
+        bmin = list(whole.info().bbox_min)
+    # the whole grid's voxelisation is the oracle's
+    lo, _ = oracle.bbox(sc.verts, sc.nudge)
+    of, ow = oracle.voxelize(sc.verts[sc.tris].reshape(-1, 9), sc.tri_mat, sc.roles, float(np.float32(sc.cell_size)),
+                             lo, (nx, ny, nz))
+    assert np.array_equal(wf, of) and np.array_equal(wm, ow)
+    plane = nx * ny
+    for part in range(3):
+        with capi.Simulation(p) as s:
+            s.set_material_roles(sc.roles)
+            s.set_mesh_slab(sc.verts, sc.tris, sc.tri_mat, part, 3)
+            z_lo, z_hi, n = s.slab_info()
+            assert (n, (z_lo, z_hi)) == (nz, slabs.split_planes(nz, 3)[part])
+            assert s.shape == (nx, ny, z_hi - z_lo + 2)
+            assert list(s.info().bbox_min) == bmin
+            keep = slice((z_lo - 1) * plane, (z_hi + 1) * plane)
+            assert np.array_equal(s.flags(), wf[keep])
+            assert np.array_equal(s.wall_materials(), wm[keep])
+
+
 def _run_slabs(parts, steps):
     import torch
     stream = torch.cuda.current_stream().cuda_stream
@@ -34,15 +66,15 @@ def _run_slabs(parts, steps):
     torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("nparts", [2, 3])
-def test_slabs_match_whole_grid_f32(nparts):
+@pytest.mark.parametrize("nparts,voxelise", [(2, "whole"), (3, "slab")])
+def test_slabs_match_whole_grid_f32(nparts, voxelise):
     sc = _scene(240)
     whole, meta = scenes.build_simulation(sc)
     nx, ny, nz = meta["shape"]
     plane = nx * ny
     wf, wn, wb = whole.flags(), whole.normals(), whole.boundary_indices()
     wm, ww = whole.boundary_materials()
-    parts, pmeta = scenes.build_slabs(sc, nparts)
+    parts, pmeta = scenes.build_slabs(sc, nparts, voxelise=voxelise)
     assert pmeta["shape"] == meta["shape"]
     got_b, got_m, got_w = [], [], []
     for s, z_lo, z_hi, _ in parts:

@@ -70,6 +70,9 @@ _SIGS = {
                             C.c_uint64, C.c_uint64], C.c_int),
     "virs_slab_planes": ([_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                           C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)], C.c_int),
+    "virs_set_mesh_slab": ([_P, _P, C.c_size_t, _P, _P, C.c_size_t, C.c_uint32, C.c_uint32], C.c_int),
+    "virs_load_obj_slab": ([_P, C.c_char_p, C.c_uint32, C.c_uint32], C.c_int),
+    "virs_get_slab_info": ([_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
     "virs_classify": ([_P], C.c_int),
     "virs_get_flags": ([_P, _P, C.c_size_t], C.c_int),
     "virs_get_normals": ([_P, _P, C.c_size_t], C.c_int),
@@ -264,6 +267,23 @@ class Simulation:
         if w is not None and w.size != f.size:
             raise ValueError("wall_material must match flags")
         check(lib().virs_set_grid_slab(self._h, nx, ny, nz, cell_size, z_lo, z_hi, _ptr(f), _ptr(w), z_first, nz_ext))
+
+    def set_mesh_slab(self, verts, tris, tri_material, part: int, parts: int):
+        """Slab `part` of `parts` of the grid sized from the mesh; only its
+        planes are voxelised."""
+        v = _c(verts, np.float32).reshape(-1, 3)
+        t = _c(tris, np.uint32).reshape(-1, 3)
+        m = _c(tri_material, np.int32)
+        check(lib().virs_set_mesh_slab(self._h, _ptr(v), v.shape[0], _ptr(t), _ptr(m), t.shape[0], part, parts))
+
+    def load_obj_slab(self, path, part: int, parts: int):
+        check(lib().virs_load_obj_slab(self._h, str(path).encode(), part, parts))
+
+    def slab_info(self):
+        """(z_lo, z_hi, nz): owned global planes and the whole grid's planes."""
+        a, b, n = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(lib().virs_get_slab_info(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return int(a.value), int(b.value), int(n.value)
 
     def slab_planes(self):
         """(first, last, ghost_lo, ghost_hi, plane_bytes): device addresses of

@@ -91,6 +91,7 @@ struct virs_sim {
     // into them.  For a whole grid ext_nz == nz and slab_drop == 0.
     bool slab = false;
     uint32_t ext_nz = 0, slab_drop = 0;
+    uint64_t slab_lo = 0, slab_hi = 0, global_nz = 0; // owned global planes and the global grid's planes
 
     // boundary
     uint64_t nb = 0;
@@ -340,7 +341,24 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
 
 // mesh -> grid: bounding box and sizing on the host, the triangle sweep on
 // the GPU (kernels_voxelize.cu) straight into the padded flag arrays
-virs_status install_mesh(virs_sim *s, const Mesh &m)
+// the interior planes 1..nz-2 split into `parts` contiguous ranges whose
+// sizes differ by at most one; range `part` (virs_b200/slabs.py:split_planes)
+void split_planes(uint64_t nz, uint32_t part, uint32_t parts, uint64_t *z_lo, uint64_t *z_hi)
+{
+    const uint64_t inner = nz - 2, base = inner / parts, extra = inner % parts;
+    *z_lo = 1 + part * base + std::min<uint64_t>(part, extra);
+    *z_hi = *z_lo + base + (part < extra ? 1 : 0);
+}
+
+// planes of flags a slab needs on each side of its own grid for the sponge
+// classification of its planes: the ghost plane is classified too, and a
+// voxel's class depends on the walls within W planes
+uint64_t slab_halo(const virs_sim *s) { return (uint64_t)s->prm.sponge_width + 1; }
+
+// parts == 0: the whole grid; otherwise slab `part` of `parts`, whose
+// uploaded planes (its own, the ghost planes and the classification halo)
+// alone are voxelised, with the whole grid's origin and sizes
+virs_status install_mesh(virs_sim *s, const Mesh &m, uint32_t part = 0, uint32_t parts = 0)
 {
     float bmin[3], bmax[3];
     mesh_bbox(m, s->prm.bbox_nudge, bmin, bmax);
@@ -348,30 +366,51 @@ virs_status install_mesh(virs_sim *s, const Mesh &m)
     uint64_t d[3];
     grid_dims(bmin, bmax, h, d);
     if (d[0] < 3 || d[1] < 3 || d[2] < 3) return fail(VIRS_E_ARG, "mesh bounding box gives a grid below 3 voxels per axis");
-    if (d[0] * d[1] * d[2] >= (1ull << 32)) return fail(VIRS_E_ARG, "mesh gives a grid of 2^32 voxels or more");
+    if (!parts && d[0] * d[1] * d[2] >= (1ull << 32)) return fail(VIRS_E_ARG, "mesh gives a grid of 2^32 voxels or more");
+    uint64_t z_lo = 0, z_hi = 0, z_first = 0, nz_ext = d[2];
+    if (parts) {
+        if (part >= parts || d[2] - 2 < parts)
+            return fail(VIRS_E_ARG, "slab " + std::to_string(part) + " of " + std::to_string(parts) + ": the grid has " +
+                                        std::to_string(d[2] - 2) + " interior planes");
+        if (s->prm.storage != VIRS_STORAGE_F32 && !(s->prm.storage_scale > 0.f))
+            return fail(VIRS_E_ARG, "slabs with 16-bit storage need an explicit storage_scale, the same on every slab");
+        split_planes(d[2], part, parts, &z_lo, &z_hi);
+        const uint64_t H = slab_halo(s);
+        z_first = z_lo - 1 >= H ? z_lo - 1 - H : 0;
+        nz_ext = std::min<uint64_t>(d[2], z_hi + 1 + H) - z_first;
+    }
     const uint64_t ntri = m.tri_mat.size();
     if (ntri >= 0xffffffffull) return fail(VIRS_E_ARG, "too many triangles");
     for (uint32_t v : m.tris)
         if ((uint64_t)v * 3 + 2 >= m.verts.size()) return fail(VIRS_E_ARG, "triangle vertex index out of range");
     VIRS_TRY(use_device(s));
-    VIRS_TRY(install_grid(s, d[0], d[1], d[2], h, nullptr, nullptr));
+    if (parts) {
+        VIRS_TRY(install_grid(s, d[0], d[1], nz_ext, h, nullptr, nullptr, z_hi - z_lo + 2, z_lo - 1 - z_first));
+        s->slab_lo = z_lo;
+        s->slab_hi = z_hi;
+        s->global_nz = d[2];
+    } else {
+        VIRS_TRY(install_grid(s, d[0], d[1], d[2], h, nullptr, nullptr));
+    }
     std::memcpy(s->bmin, bmin, sizeof(bmin));
     if (ntri) {
+        const size_t nvx = (size_t)s->px * s->ny * s->ext_nz; // the uploaded planes
         DevBuf dv, dt, dm, dr, tri, la, lw, mx;
         VIRS_TRY(dv.alloc(m.verts.size() * sizeof(float), "mesh vertices"));
         VIRS_TRY(dt.alloc(m.tris.size() * sizeof(uint32_t), "mesh triangles"));
         VIRS_TRY(dm.alloc(ntri * sizeof(int32_t), "triangle materials"));
         VIRS_TRY(dr.alloc(std::max<size_t>(s->roles.size(), 1), "material roles"));
         VIRS_TRY(tri.alloc(ntri * voxelize_tri_bytes(), "triangle table"));
-        VIRS_TRY(la.alloc(s->nvox * sizeof(uint32_t), "voxelisation marks"));
-        VIRS_TRY(lw.alloc(s->nvox * sizeof(uint32_t), "voxelisation marks"));
+        VIRS_TRY(la.alloc(nvx * sizeof(uint32_t), "voxelisation marks"));
+        VIRS_TRY(lw.alloc(nvx * sizeof(uint32_t), "voxelisation marks"));
         VIRS_TRY(mx.alloc(sizeof(uint32_t), "wall material maximum"));
         VIRS_CUDA(cudaMemcpy(dv.ptr, m.verts.data(), dv.bytes, cudaMemcpyHostToDevice));
         VIRS_CUDA(cudaMemcpy(dt.ptr, m.tris.data(), dt.bytes, cudaMemcpyHostToDevice));
         VIRS_CUDA(cudaMemcpy(dm.ptr, m.tri_mat.data(), dm.bytes, cudaMemcpyHostToDevice));
         if (!s->roles.empty()) VIRS_CUDA(cudaMemcpy(dr.ptr, s->roles.data(), s->roles.size(), cudaMemcpyHostToDevice));
         VIRS_CUDA(launch_voxelize(dv.as<float>(), dt.as<uint32_t>(), dm.as<int32_t>(), ntri, dr.as<uint8_t>(),
-                                  (uint32_t)s->roles.size(), h, bmin, s->nx, s->ny, s->nz, s->px, tri.ptr,
+                                  (uint32_t)s->roles.size(), h, bmin, s->nx, s->ny, (uint32_t)d[2], (uint32_t)z_first,
+                                  s->ext_nz, s->px, tri.ptr,
                                   la.as<uint32_t>(), lw.as<uint32_t>(), s->flags_raw.as<uint8_t>(),
                                   s->wall_mat.as<uint8_t>(), mx.as<uint32_t>(), s->stream));
         uint32_t mxh = 0;
@@ -730,8 +769,8 @@ VIRS_EXPORT virs_status virs_load_obj(virs_sim *s, const char *path)
     return install_mesh(s, m);
 }
 
-VIRS_EXPORT virs_status virs_set_mesh(virs_sim *s, const float *verts, size_t nverts, const uint32_t *tris,
-                                      const int32_t *tri_material, size_t ntris)
+static virs_status set_mesh(virs_sim *s, const float *verts, size_t nverts, const uint32_t *tris,
+                            const int32_t *tri_material, size_t ntris, uint32_t part, uint32_t parts)
 {
     if (!s || !verts || !tris || !tri_material || !nverts || !ntris)
         return fail(VIRS_E_ARG, "virs_set_mesh: null or empty argument");
@@ -744,7 +783,40 @@ VIRS_EXPORT virs_status virs_set_mesh(virs_sim *s, const float *verts, size_t nv
         if (v >= nverts) return fail(VIRS_E_ARG, "virs_set_mesh: triangle vertex index out of range");
     for (float v : m.verts)
         if (!std::isfinite(v)) return fail(VIRS_E_ARG, "virs_set_mesh: non-finite vertex coordinate");
-    return install_mesh(s, m);
+    return install_mesh(s, m, part, parts);
+}
+
+VIRS_EXPORT virs_status virs_set_mesh(virs_sim *s, const float *verts, size_t nverts, const uint32_t *tris,
+                                      const int32_t *tri_material, size_t ntris)
+{
+    return set_mesh(s, verts, nverts, tris, tri_material, ntris, 0, 0);
+}
+
+VIRS_EXPORT virs_status virs_set_mesh_slab(virs_sim *s, const float *verts, size_t nverts, const uint32_t *tris,
+                                           const int32_t *tri_material, size_t ntris, uint32_t part, uint32_t parts)
+{
+    if (!parts) return fail(VIRS_E_ARG, "virs_set_mesh_slab: parts must be at least 1");
+    return set_mesh(s, verts, nverts, tris, tri_material, ntris, part, parts);
+}
+
+VIRS_EXPORT virs_status virs_load_obj_slab(virs_sim *s, const char *path, uint32_t part, uint32_t parts)
+{
+    if (!s || !path) return fail(VIRS_E_ARG, "virs_load_obj_slab: null argument");
+    if (!parts) return fail(VIRS_E_ARG, "virs_load_obj_slab: parts must be at least 1");
+    VIRS_TRY(use_device(s));
+    Mesh m;
+    VIRS_TRY(load_obj(path, m));
+    return install_mesh(s, m, part, parts);
+}
+
+VIRS_EXPORT virs_status virs_get_slab_info(const virs_sim *s, uint64_t *z_lo, uint64_t *z_hi, uint64_t *nz)
+{
+    if (!s || !z_lo || !z_hi || !nz) return fail(VIRS_E_ARG, "virs_get_slab_info: null argument");
+    if (!s->slab) return fail(VIRS_E_STATE, "virs_get_slab_info: not a slab");
+    *z_lo = s->slab_lo;
+    *z_hi = s->slab_hi;
+    *nz = s->global_nz;
+    return VIRS_OK;
 }
 
 VIRS_EXPORT virs_status virs_set_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h,
@@ -756,11 +828,6 @@ VIRS_EXPORT virs_status virs_set_grid(virs_sim *s, uint64_t nx, uint64_t ny, uin
     s->bmin[0] = s->bmin[1] = s->bmin[2] = 0.f;
     return VIRS_OK;
 }
-
-// planes of flags a slab needs on each side of its own grid for the sponge
-// classification of its planes: the ghost plane is classified too, and a
-// voxel's class depends on the walls within W planes
-static uint64_t slab_halo(const virs_sim *s) { return (uint64_t)s->prm.sponge_width + 1; }
 
 VIRS_EXPORT virs_status virs_set_grid_slab(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, float h, uint64_t z_lo,
                                            uint64_t z_hi, const uint8_t *flags, const uint8_t *wmat, uint64_t z_first,
@@ -780,6 +847,9 @@ VIRS_EXPORT virs_status virs_set_grid_slab(virs_sim *s, uint64_t nx, uint64_t ny
         return fail(VIRS_E_ARG, "virs_set_grid_slab: 16-bit storage needs an explicit storage_scale, the same on every slab");
     VIRS_TRY(use_device(s));
     VIRS_TRY(install_grid(s, nx, ny, nz_ext, h, flags, wmat, z_hi - z_lo + 2, z_lo - 1 - z_first));
+    s->slab_lo = z_lo;
+    s->slab_hi = z_hi;
+    s->global_nz = nz;
     s->bmin[0] = s->bmin[1] = s->bmin[2] = 0.f;
     return VIRS_OK;
 }

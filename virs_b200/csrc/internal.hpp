@@ -210,9 +210,9 @@ cudaError_t launch_zero_at(float *f, const uint32_t *pos, uint32_t n, cudaStream
 size_t voxelize_tri_bytes();
 cudaError_t launch_voxelize(const float *verts, const uint32_t *tris, const int32_t *tri_mat, uint64_t ntri,
                             const uint8_t *roles, uint32_t nroles, float h, const float bmin[3], uint32_t nx,
-                            uint32_t ny, uint32_t nz, uint32_t px, void *tri_buf, uint32_t *last_any,
-                            uint32_t *last_wall, uint8_t *flags, uint8_t *wall_mat, uint32_t *max_mat,
-                            cudaStream_t s);
+                            uint32_t ny, uint32_t nz, uint32_t zw, uint32_t nzl, uint32_t px, void *tri_buf,
+                            uint32_t *last_any, uint32_t *last_wall, uint8_t *flags, uint8_t *wall_mat,
+                            uint32_t *max_mat, cudaStream_t s);
 
 // IR post-processing (kernels_ir.cu)
 cudaError_t launch_ir_sos(const float *in, uint64_t in_stride, uint64_t len, const double *sos, int ns, float *out,

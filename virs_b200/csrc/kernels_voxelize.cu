@@ -9,6 +9,10 @@
 //                 a hit raises the voxel's "last triangle" marks with an
 //                 atomic maximum of the triangle number
 //   k_resolve     marks -> flags and wall materials
+// The grid may be a window of planes [zw, zw + nzl) of a taller grid (a
+// z-slab): voxel coordinates and the cell tests stay global, so every hit
+// is the whole grid's, and only the boxes and the stored index are cut to
+// the window.
 // The reference's sweep runs the triangles in order and a later triangle
 // overwrites a voxel's flag (wall 1 or source 3), while a source triangle
 // leaves the wall material alone.  So the flag comes from the last wall or
@@ -97,8 +101,8 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? l
 
 __global__ void k_tri_prep(const float *__restrict verts, const uint32_t *__restrict tris,
                            const int32_t *__restrict tri_mat, uint64_t ntri, const uint8_t *__restrict roles,
-                           uint32_t nroles, float h, float bx, float by, float bz, int nx, int ny, int nz,
-                           Tri *__restrict out)
+                           uint32_t nroles, float h, float bx, float by, float bz, int nx, int ny, int nz, int zw,
+                           int nzl, Tri *__restrict out)
 {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntri) return;
@@ -116,13 +120,17 @@ __global__ void k_tri_prep(const float *__restrict verts, const uint32_t *__rest
         T.box[a] = clampi((int)floorf(mn3(T.g[a], T.g[3 + a], T.g[6 + a])), 0, n[a] - 1);
         T.box[3 + a] = clampi((int)ceilf(mx3(T.g[a], T.g[3 + a], T.g[6 + a])), 0, n[a] - 1);
     }
+    // the window of planes held
+    T.box[2] = T.box[2] > zw ? T.box[2] : zw;
+    T.box[5] = T.box[5] < zw + nzl - 1 ? T.box[5] : zw + nzl - 1;
+    if (T.box[2] > T.box[5]) T.role = VIRS_ROLE_IGNORE;
     out[t] = T;
 }
 
 // blocks stride over the triangles (x) and over the cells of a triangle's
 // box (y and the threads)
 __global__ void __launch_bounds__(256) k_tri_sweep(const Tri *__restrict tris, uint64_t ntri, uint32_t px,
-                                                   uint32_t ny, uint32_t *__restrict last_any,
+                                                   uint32_t ny, int zw, uint32_t *__restrict last_any,
                                                    uint32_t *__restrict last_wall)
 {
     for (uint64_t t = blockIdx.x; t < ntri; t += gridDim.x) {
@@ -138,7 +146,7 @@ __global__ void __launch_bounds__(256) k_tri_sweep(const Tri *__restrict tris, u
              q += (uint64_t)gridDim.y * blockDim.x) {
             const int i = x0 + (int)(q % sx), j = y0 + (int)((q / sx) % sy), k = z0 + (int)(q / (sx * sy));
             if (!overlap(g, (float)i, (float)j, (float)k)) continue;
-            const size_t idx = ((size_t)k * ny + (size_t)j) * px + (size_t)i;
+            const size_t idx = ((size_t)(k - zw) * ny + (size_t)j) * px + (size_t)i;
             atomicMax(last_any + idx, (uint32_t)(t + 1));
             if (role != VIRS_ROLE_SOURCE) atomicMax(last_wall + idx, (uint32_t)(t + 1));
         }
@@ -168,21 +176,22 @@ size_t voxelize_tri_bytes() { return sizeof(Tri); }
 
 cudaError_t launch_voxelize(const float *verts, const uint32_t *tris, const int32_t *tri_mat, uint64_t ntri,
                             const uint8_t *roles, uint32_t nroles, float h, const float bmin[3], uint32_t nx,
-                            uint32_t ny, uint32_t nz, uint32_t px, void *tri_buf, uint32_t *last_any,
-                            uint32_t *last_wall, uint8_t *flags, uint8_t *wall_mat, uint32_t *max_mat,
-                            cudaStream_t s)
+                            uint32_t ny, uint32_t nz, uint32_t zw, uint32_t nzl, uint32_t px, void *tri_buf,
+                            uint32_t *last_any, uint32_t *last_wall, uint8_t *flags, uint8_t *wall_mat,
+                            uint32_t *max_mat, cudaStream_t s)
 {
     if (ntri == 0) return cudaSuccess;
     Tri *T = static_cast<Tri *>(tri_buf);
     k_tri_prep<<<(unsigned)((ntri + 127) / 128), 128, 0, s>>>(verts, tris, tri_mat, ntri, roles, nroles, h, bmin[0],
-                                                              bmin[1], bmin[2], (int)nx, (int)ny, (int)nz, T);
+                                                              bmin[1], bmin[2], (int)nx, (int)ny, (int)nz, (int)zw,
+                                                              (int)nzl, T);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const unsigned gx = (unsigned)(ntri < 4096 ? ntri : 4096);
     const unsigned gy = ntri < 64 ? 256u : (ntri < 1024 ? 16u : 1u);
-    k_tri_sweep<<<dim3(gx, gy), 256, 0, s>>>(T, ntri, px, ny, last_any, last_wall);
+    k_tri_sweep<<<dim3(gx, gy), 256, 0, s>>>(T, ntri, px, ny, (int)zw, last_any, last_wall);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const uint64_t n = (uint64_t)px * ny * nz;
+    const uint64_t n = (uint64_t)px * ny * nzl;
     k_resolve<<<1184, 256, 0, s>>>(T, last_any, last_wall, n, flags, wall_mat, max_mat);
     return cudaGetLastError();
 }

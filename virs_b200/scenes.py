@@ -307,28 +307,43 @@ def build_simulation(sc: Scene, *, storage: int = 0, device: int = 0, boundary_k
 
 
 def build_slabs(sc: Scene, parts: int, *, storage: int = 0, device: int = 0, storage_scale: float = 0.0,
-                steps: int | None = None, form: int | None = None):
+                steps: int | None = None, form: int | None = None, voxelise: str = "slab"):
     """The scene's grid split into `parts` z-slabs, one handle each on
-    `device` (virs_set_grid_slab), each configured like build_simulation with
-    the sources and receivers it owns.  The mesh is voxelised once on the
-    GPU; every slab gets its planes of the flags and wall materials.
-    Returns ([(sim, z_lo, z_hi, receivers_owned_mask)], info dict)."""
+    `device`, each configured like build_simulation with the sources and
+    receivers it owns.  voxelise="slab": every slab voxelises its own planes
+    of the mesh (virs_set_mesh_slab); "whole": the mesh is voxelised once
+    and every slab gets its planes of the flags and wall materials
+    (virs_set_grid_slab).  Returns ([(sim, z_lo, z_hi,
+    receivers_owned_mask)], info dict)."""
     from . import capi, slabs
     p = capi.default_params(device=device, courant=sc.courant, cell_size=sc.cell_size, bbox_nudge=sc.nudge,
                             sponge_width=sc.sponge_width, storage=storage, storage_scale=storage_scale,
                             boundary_form=boundary_form(sc) if form is None else form)
-    with capi.Simulation(p) as whole:
-        whole.set_material_roles(sc.roles)
-        whole.set_mesh(sc.verts, sc.tris, sc.tri_mat)
-        flags, wmat, g = whole.flags(), whole.wall_materials(), whole.info()
-    shape = (int(g.nx), int(g.ny), int(g.nz))
+    sims = []
+    if voxelise == "whole":
+        with capi.Simulation(p) as whole:
+            whole.set_material_roles(sc.roles)
+            whole.set_mesh(sc.verts, sc.tris, sc.tri_mat)
+            flags, wmat, g = whole.flags(), whole.wall_materials(), whole.info()
+        shape = (int(g.nx), int(g.ny), int(g.nz))
+        for r in range(parts):
+            s = capi.Simulation(p)
+            slabs.setup_slab(s, shape, g.cell_size, flags, wmat, r, parts, sc.sponge_width)
+            sims.append(s)
+    else:
+        for r in range(parts):
+            s = capi.Simulation(p)
+            s.set_material_roles(sc.roles)
+            s.set_mesh_slab(sc.verts, sc.tris, sc.tri_mat, r, parts)
+            sims.append(s)
+        g = sims[0].info()
+        shape = (int(g.nx), int(g.ny), sims[0].slab_info()[2])
     bmin = np.array(list(g.bbox_min), np.float32)
     src = voxel_index(sc.src_pos, bmin, g.cell_size, shape) if len(sc.src_pos) else np.zeros(0, np.uint64)
     rcv = voxel_index(sc.rcv_pos, bmin, g.cell_size, shape) if len(sc.rcv_pos) else np.zeros(0, np.uint64)
     out = []
-    for r in range(parts):
-        s = capi.Simulation(p)
-        z_lo, z_hi = slabs.setup_slab(s, shape, g.cell_size, flags, wmat, r, parts, sc.sponge_width)
+    for s in sims:
+        z_lo, z_hi, _ = s.slab_info()
         s.classify()
         if sc.coef64 is not None:
             s.set_filters(sc.coef64.astype(np.float32), n_sections=sc.n_sections)
