@@ -68,6 +68,37 @@ public:
     {
         check(virs_set_mesh(h_, verts.data(), verts.size() / 3, tris.data(), tri_material.data(), tris.size() / 3));
     }
+    /* one z-slab of a grid split over several GPUs: slab `part` of `parts`
+     * from a mesh, or owned planes [z_lo, z_hi) from the whole grid's flags
+     * (planes [z_first, z_first + flags.size()/(nx*ny))) */
+    void set_mesh_slab(const std::vector<float> &verts, const std::vector<uint32_t> &tris,
+                       const std::vector<int32_t> &tri_material, uint32_t part, uint32_t parts)
+    {
+        check(virs_set_mesh_slab(h_, verts.data(), verts.size() / 3, tris.data(), tri_material.data(),
+                                 tris.size() / 3, part, parts));
+    }
+    void load_obj_slab(const std::string &path, uint32_t part, uint32_t parts)
+    {
+        check(virs_load_obj_slab(h_, path.c_str(), part, parts));
+    }
+    void set_grid_slab(uint64_t nx, uint64_t ny, uint64_t nz, float cell_size, uint64_t z_lo, uint64_t z_hi,
+                       const std::vector<uint8_t> &flags, const std::vector<uint8_t> &wall_material, uint64_t z_first)
+    {
+        check(virs_set_grid_slab(h_, nx, ny, nz, cell_size, z_lo, z_hi, flags.data(),
+                                 wall_material.empty() ? nullptr : wall_material.data(), z_first,
+                                 flags.size() / (nx * ny)));
+    }
+    struct SlabPlanes {
+        void *first, *last, *ghost_lo, *ghost_hi;
+        size_t bytes;
+    };
+    /* the planes of p^n to exchange before the next step */
+    SlabPlanes slab_planes() const
+    {
+        SlabPlanes p{};
+        check(virs_slab_planes(h_, &p.first, &p.last, &p.ghost_lo, &p.ghost_hi, &p.bytes));
+        return p;
+    }
     /* sponge layer, normals, boundary list: the rest of loadObj (:469-610) */
     void classify() { check(virs_classify(h_)); }
     virs_grid_info info() const
@@ -86,6 +117,12 @@ public:
         std::vector<uint8_t> f(voxels());
         check(virs_get_flags(h_, f.data(), f.size()));
         return f;
+    }
+    std::vector<uint8_t> wall_materials() const
+    {
+        std::vector<uint8_t> w(voxels());
+        check(virs_get_wall_materials(h_, w.data(), w.size()));
+        return w;
     }
     std::vector<uint32_t> boundary_indices() const
     {

@@ -78,7 +78,7 @@ struct StepArgs {
     const uint8_t *bnrm;    // [nb] air-neighbour mask of each slot's voxel (rigid-wall update)
     const uint8_t *bmat;
     const float *bw;
-    float *state;           // [S][4][nb]
+    float *state;           // [2(S+1)][nb]: X_q[n-1], X_q[n-2] of the cascade's input and section outputs
     const float *coef;      // [M][S][5]
     const float *hard;      // per-step hard source values (scaled)
     const uint32_t *ctr;    // device step counter

@@ -1,4 +1,6 @@
-// The FDTD step on the GPU: one fused kernel per time step.
+// The FDTD step on the GPU: the register-streaming stencil (the variant
+// with pipeline depth 0; the TMA-staged default is kernels_step_tma.cu), the
+// boundary pass and the per-step source / receiver kernel.
 //
 // Semantics follow the reference step (src/simulator/simulator_gpu.cu):
 //   interior leapfrog with the wall mirror rule       :38-103
@@ -19,7 +21,7 @@
 //     and updated by k_boundary, one thread per entry of the compacted,
 //     ascending boundary list: the leapfrog and the biquad correction
 //     together, with no divergence in the stencil kernel; the filter states
-//     are stored [section][4][slot] so a warp touches consecutive words.
+//     are stored [2(S+1)][slot] so a warp touches consecutive words.
 //
 // Arithmetic order is fixed with _rn intrinsics so that the result is
 // bit-identical to the CPU oracle: the reference CUDA build contracts
