@@ -16,6 +16,7 @@
 #include <tuple>
 #include <new>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -82,6 +83,7 @@ struct virs_sim {
     uint8_t max_wall_mat = 0;
 
     DevBuf flags_raw, wall_mat, flags, code, normals, bseg;
+    DevBuf segnz;                  // [nseg] 1 if a 128-voxel row segment holds a non-zero code
     DevBuf field[2];
     int cur = 0;
 
@@ -133,6 +135,10 @@ struct virs_sim {
     CUtensorMap tmP[2], tmQ[2], tmC;
     DevBuf side;                   // {free, p, p^{n-1}} per boundary slot (TMA kernel -> boundary pass)
     int maps_rows = 0;             // tile rows the maps were built for (0 = none)
+    // per stencil tile, the stages whose codes are all zero (not copied);
+    // built for zm_rows x zm_zc tiles (0 = none)
+    DevBuf zmask;
+    int zm_rows = 0, zm_zc = 0;
     DevBuf err;                    // device error flag of bounded waits
 
     // CUDA graphs for GRAPH_STEPS steps, one per parity of `cur`
@@ -316,7 +322,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->max_wall_mat = mx;
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
-    for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->field[0],
+    for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->segnz, &s->field[0],
                       &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
         b->release();
     const size_t ext = (size_t)s->px * ny * s->ext_nz;
@@ -331,6 +337,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->nb = 0;
     s->steps_done = 0;
     s->maps_rows = 0;
+    s->zm_rows = s->zm_zc = 0;
     // sources and receivers refer to voxel indices of the previous grid
     s->nsrc = s->nrcv = 0;
     s->src_ref.clear();
@@ -505,6 +512,32 @@ virs_status check_err(virs_sim *s)
     return VIRS_OK;
 }
 
+int eff_planes(const virs_sim *s) { return s->zc > 0 ? s->zc : default_planes(s->nz); }
+
+// per tile of a rows x zc tiling of the TMA stencil, the stages whose codes
+// are all zero (kernels_classify.cu::k_tile_zero_mask)
+virs_status build_zero_masks(const virs_sim *s, int rows, int zc, DevBuf &mask)
+{
+    const uint32_t gx = (s->px + (uint32_t)tma_tile_x() - 1) / (uint32_t)tma_tile_x();
+    const uint32_t gy = (s->ny + (uint32_t)rows - 1) / (uint32_t)rows;
+    const uint32_t gz = (s->nz - 2 + (uint32_t)zc - 1) / (uint32_t)zc;
+    VIRS_TRY(mask.alloc((size_t)gx * gy * gz * 8, "zero-code masks"));
+    VIRS_CUDA(launch_tile_zero_masks(s->segnz.as<uint8_t>(), s->ny, s->nz, s->spr, (uint32_t)rows, (uint32_t)zc, gx,
+                                     gy, gz, mask.as<uint64_t>(), s->stream));
+    VIRS_CUDA(cudaStreamSynchronize(s->stream));
+    return VIRS_OK;
+}
+
+// The first and last tile columns hold the grid's border (code CODE_NONE),
+// so only grids at least three tiles wide have planes of a tile with all
+// codes zero; for the others the masks would cost their tests for nothing.
+bool zero_masks_useful(const virs_sim *s) { return s->px > 2u * (uint32_t)tma_tile_x(); }
+
+bool zero_masks_ready(const virs_sim *s)
+{
+    return s->depth > 0 && zero_masks_useful(s) && s->zm_rows == s->tile_rows && s->zm_zc == eff_planes(s);
+}
+
 virs_status ready_to_run(virs_sim *s)
 {
     if (!s->has_grid) return fail(VIRS_E_STATE, "no grid: call virs_load_obj, virs_set_mesh or virs_set_grid");
@@ -516,6 +549,13 @@ virs_status ready_to_run(virs_sim *s)
     if (!s->state.ptr) VIRS_TRY(alloc_states(s));
     if (!s->ctr.ptr) VIRS_TRY(s->ctr.alloc(sizeof(uint32_t), "step counter"));
     if (s->depth > 0 && s->maps_rows != s->tile_rows) VIRS_TRY(build_maps(s));
+    if (s->depth > 0 && zero_masks_useful(s) && !zero_masks_ready(s)) {
+        s->zm_rows = s->zm_zc = 0;
+        VIRS_TRY(build_zero_masks(s, s->tile_rows, eff_planes(s), s->zmask));
+        s->zm_rows = s->tile_rows;
+        s->zm_zc = eff_planes(s);
+        s->drop_graphs();
+    }
     return VIRS_OK;
 }
 
@@ -553,6 +593,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.mix_d = s->prm.mix_direct;
     a.gain = (double)s->prm.boundary_gain;
     a.form = s->prm.boundary_form;
+    if (zero_masks_ready(s)) a.tzmask = s->zmask.as<uint64_t>();
     return a;
 }
 
@@ -943,11 +984,13 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(s->code.alloc(s->nvox, "cell codes"));
         VIRS_TRY(s->normals.alloc(s->nvox, "normals"));
         VIRS_TRY(s->bseg.alloc(nseg * 4, "boundary prefix"));
+        VIRS_TRY(s->segnz.alloc(nseg, "segment code flags"));
         CodesArgs co{};
         co.flags = s->flags.as<uint8_t>();
         co.code = s->code.as<uint8_t>();
         co.normals = s->normals.as<uint8_t>();
         co.segcnt = s->bseg.as<uint32_t>();
+        co.segnz = s->segnz.as<uint8_t>();
         co.nx = s->nx;
         co.ny = s->ny;
         co.nz = s->nz;
@@ -1012,6 +1055,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
     s->state.release();
     if (s->filters_set) VIRS_TRY(alloc_states(s));
     s->maps_rows = 0;
+    s->zm_rows = s->zm_zc = 0;
     s->classified = true;
     VIRS_CUDA(cudaEventRecord(s->done, st));
     return VIRS_OK;
@@ -1737,6 +1781,8 @@ struct virs_batch {
     uint64_t ntiles = 0, nbnd = 0;
     uint32_t max_sections = 0;
     DevBuf desc, err;
+    // each member's zero-code masks for the batch's tiling
+    std::deque<DevBuf> zmasks;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1776,6 +1822,7 @@ virs_status batch_check(const virs_batch *b)
 virs_status batch_build(virs_batch *b)
 {
     b->drop_graphs();
+    b->zmasks.clear();
     std::vector<BatchMember> h(b->mem.size());
     uint64_t tiles = 0, bnd = 0;
     b->max_sections = 0;
@@ -1794,9 +1841,16 @@ virs_status batch_build(virs_batch *b)
         }
         VIRS_TRY(encode(&m.mapC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)tma_tile_x(), b->rows));
         const int zc = b->planes > 0 ? b->planes : (s->zc > 0 ? s->zc : default_planes(s->nz));
+        const uint64_t *zm = nullptr;
+        if (zero_masks_useful(s)) {
+            b->zmasks.emplace_back();
+            VIRS_TRY(build_zero_masks(s, b->rows, zc, b->zmasks.back()));
+            zm = b->zmasks.back().as<uint64_t>();
+        }
         for (int par = 0; par < 2; ++par) {
             m.step[par] = step_args(s, par);
             m.step[par].zc = zc;
+            m.step[par].tzmask = zm; // the batch's tiling, not the member's own
             m.post[par] = post_args(s, par);
         }
         m.bidx = s->bidx.as<uint32_t>();

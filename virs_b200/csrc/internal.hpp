@@ -69,6 +69,7 @@ constexpr int SEG = 128;              // voxels per boundary-prefix segment
 
 struct StepArgs {
     float4 *side;           // per boundary slot {free, p, p^{n-1}, 0}, kept by the boundary pass for the adjoint
+    const uint64_t *tzmask; // TMA stencil, per tile: bit j = the codes of stage j are all zero (nullptr: none)
     const void *p;          // p^n (storage type)
     void *q;                // in p^{n-1}, out p^{n+1}
     const uint8_t *code;
@@ -167,6 +168,7 @@ struct CodesArgs {
     uint8_t *code;             // padded
     uint8_t *normals;          // padded
     uint32_t *segcnt;          // [nseg]
+    uint8_t *segnz;            // [nseg] 1 if the segment holds a non-zero code
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_codes(const CodesArgs &a, cudaStream_t s);
@@ -190,6 +192,10 @@ struct CompactArgs {
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);
+// per tile of a rows x zc tiling of the TMA stencil: bit j set when the codes
+// of the plane in stage j are all zero (kernels_classify.cu)
+cudaError_t launch_tile_zero_masks(const uint8_t *segnz, uint32_t ny, uint32_t nz, uint32_t spr, uint32_t rows,
+                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint64_t *mask, cudaStream_t s);
 cudaError_t launch_hard_list(const uint8_t *code, uint64_t n, uint32_t *count, uint32_t *out, uint32_t cap,
                              cudaStream_t s);
 

@@ -107,14 +107,15 @@ __global__ void k_edt_z(const ClassifyArgs a)
     a.bd2_full[i] = (uint16_t)(best >> 18);
 }
 
-// cell code, normals and per-segment boundary counts; one block of SEG
-// threads per 128-voxel row segment
+// cell code, normals, per-segment boundary counts and whether a segment
+// holds any non-zero code; one block of SEG threads per 128-voxel row
+// segment
 __global__ void k_codes(const CodesArgs a)
 {
     const int x = blockIdx.x * SEG + threadIdx.x;
     const int y = blockIdx.y, z = blockIdx.z;
     const int nx = a.nx, ny = a.ny, nz = a.nz, px = a.px;
-    bool bnd = false;
+    bool bnd = false, nonzero = false;
     if (x < px) {
         const size_t sy = px, sz = (size_t)px * ny;
         const size_t i = (size_t)z * sz + (size_t)y * sy + x;
@@ -145,9 +146,14 @@ __global__ void k_codes(const CodesArgs a)
         }
         a.code[i] = code;
         a.normals[i] = nrm;
+        nonzero = code != 0;
     }
     const int cnt = __syncthreads_count(bnd);
-    if (threadIdx.x == 0) a.segcnt[((size_t)z * ny + y) * a.spr + blockIdx.x] = (uint32_t)cnt;
+    const int any = __syncthreads_or(nonzero);
+    if (threadIdx.x == 0) {
+        a.segcnt[((size_t)z * ny + y) * a.spr + blockIdx.x] = (uint32_t)cnt;
+        a.segnz[((size_t)z * ny + y) * a.spr + blockIdx.x] = any ? 1 : 0;
+    }
 }
 
 // boundary voxels of one segment get consecutive slots after bseg[segment]
@@ -309,6 +315,46 @@ cudaError_t launch_hard_list(const uint8_t *code, uint64_t n, uint32_t *count, u
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s)
 {
     k_compact<<<dim3(a.spr, a.ny, a.nz), dim3(SEG), 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+
+// ---- planes of a stencil tile whose codes are all zero ---------------------------
+//
+// For a rows x zc tiling, bit j of a tile's mask is set when the codes of
+// the plane staged in stage j (plane z0 - 1 + j, j < 64, one of the tile's
+// own planes) are all zero over the tile's 128 x rows voxels: the stencil
+// then skips their copy and treats every voxel as plain air.  From the
+// per-segment flags of k_codes (a tile row is one segment).
+namespace {
+__global__ void __launch_bounds__(64) k_tile_zero_mask(const uint8_t *__restrict segnz, uint32_t ny, uint32_t nz,
+                                                       uint32_t spr, uint32_t rows, uint32_t zc, uint32_t gx,
+                                                       uint32_t gy, uint64_t *__restrict mask)
+{
+    __shared__ unsigned w[2];
+    const uint32_t t = blockIdx.x, j = threadIdx.x;
+    const uint32_t bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
+    const uint32_t z0 = 1 + bz * zc, z1 = min(z0 + zc, nz - 1);
+    const uint32_t k = z0 - 1 + j;
+    bool zero = false;
+    if (k >= z0 && k < z1) {
+        zero = true;
+        const uint32_t y1 = min(by * rows + rows, ny);
+        for (uint32_t y = by * rows; y < y1 && zero; ++y) zero = segnz[((size_t)k * ny + y) * spr + bx] == 0;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, zero);
+    if ((j & 31) == 0) w[j >> 5] = b;
+    __syncthreads();
+    if (j == 0) mask[t] = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+}
+} // namespace
+
+cudaError_t launch_tile_zero_masks(const uint8_t *segnz, uint32_t ny, uint32_t nz, uint32_t spr, uint32_t rows,
+                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint64_t *mask, cudaStream_t s)
+{
+    const uint64_t ntiles = (uint64_t)gx * gy * gz;
+    if (ntiles == 0) return cudaSuccess;
+    k_tile_zero_mask<<<(unsigned)ntiles, 64, 0, s>>>(segnz, ny, nz, spr, rows, zc, gx, gy, mask);
     return cudaGetLastError();
 }
 

@@ -8,7 +8,11 @@
 //                        a 16-byte halo in x      (TY+2) x (TX+2*PAD)
 //                  Q(k)  p^{n-1} of the tile       TY x TX
 //                  C(k)  the cell codes of the tile TY x TX bytes
-// for plane k = z0 - 1 + j.  Each thread updates the V voxels of one
+// for plane k = z0 - 1 + j.  A plane of a tile whose codes are all zero
+// (plain air: most of a large room's interior) is marked in the tile's
+// 64-bit mask (a.tzmask, built per tiling at set-up); its codes are not
+// copied and every voxel takes the air update.  Each thread updates the V
+// voxels of one
 // 16-byte vector; the centres of P(z-1) and P(z) stay in its registers, so
 // the ring has D = L + 2 stages: planes z and z+1 are in use while L more
 // are in flight, each stage guarded by one mbarrier that the TMA completes
@@ -120,6 +124,7 @@ __device__ __forceinline__ uint32_t mirror_bytes(uint32_t w)
 template <> struct Codes<4> {
     uint32_t w;
     __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint32_t *>(p); }
+    __device__ void clear() { w = 0u; }
     __device__ bool any() const { return w != 0u; }
     __device__ uint32_t get(int k) const { return (w >> (8 * k)) & 0xffu; }
     __device__ uint32_t mirror() const { return mirror_bytes(w); }
@@ -128,6 +133,7 @@ template <> struct Codes<4> {
 template <> struct Codes<8> {
     uint2 w;
     __device__ void load(const unsigned char *p) { w = *reinterpret_cast<const uint2 *>(p); }
+    __device__ void clear() { w = make_uint2(0u, 0u); }
     __device__ bool any() const { return (w.x | w.y) != 0u; }
     __device__ uint32_t get(int k) const { return ((k < 4 ? w.x : w.y) >> (8 * (k & 3))) & 0xffu; }
     // the mirror bytes of the two words folded into one: bit 7 of byte k
@@ -165,6 +171,10 @@ template <typename T, int TY, int L> struct Tile {
     bool act, leader;
     float2 c2dt2, inv_h2;
     size_t plane;
+    uint64_t zmask; // bit j: the codes of stage j are all zero (not copied)
+
+    // the codes of stage j are all zero and not copied
+    __device__ __forceinline__ bool codes_zero(int j) const { return j < 64 && ((zmask >> j) & 1ull); }
 
     static constexpr int D = L + 2;
     using S = Stage<T, TY>;
@@ -178,12 +188,11 @@ template <typename T, int TY, int L> struct Tile {
         unsigned char *st = smem + (g % D) * S::SB;
         uint64_t *b = bars + (g % D);
         const bool full = j >= 1 && j <= nst - 2;
-        mbar_expect_tx(b, S::PB + (full ? S::QB + S::CB : 0u));
+        const bool codes = full && !codes_zero(j);
+        mbar_expect_tx(b, S::PB + (full ? S::QB : 0u) + (codes ? S::CB : 0u));
         tma_load_3d(st, mP, b, x0 - PAD, y0 - 1, k);
-        if (full) {
-            tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
-            tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
-        }
+        if (full) tma_load_3d(st + S::PBa, mQ, b, x0, y0, k);
+        if (codes) tma_load_3d(st + S::PBa + S::QBa, mC, b, x0, y0, k);
     }
 
     // Plane z = z0 + i: zm and cc hold the centres of P(z-1) and P(z); the
@@ -210,8 +219,9 @@ template <typename T, int TY, int L> struct Tile {
         IO::ld(Ph + c0 - PW, ym);
         IO::ld(Ph + c0 + PW, yp);
         IO::ld(reinterpret_cast<const T *>(s0 + S::PBa) + t0, qv);
-        Codes<V> code;
-        code.load(s0 + S::PBa + S::QBa + t0);
+        Codes<V> code; // stage i + 1 holds plane z
+        if (codes_zero(i + 1)) code.clear();
+        else code.load(s0 + S::PBa + S::QBa + t0);
         float left = __shfl_up_sync(FULL, cc[V - 1], 1, LPR);
         float right = __shfl_down_sync(FULL, cc[0], 1, LPR);
         if (sl == 0) left = IO::ld1(Ph + c0 - 1);
@@ -310,6 +320,10 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
     t.inv_h2 = make_float2(a.inv_h2, a.inv_h2);
     t.plane = (size_t)a.px * a.ny;
+    {
+        const uint32_t gx = (a.px + TX - 1) / TX, gy = (a.ny + TY - 1) / TY;
+        t.zmask = a.tzmask ? __ldg(a.tzmask + ((size_t)bz * gy + (size_t)by) * gx + (size_t)bx) : 0ull;
+    }
 
     if (t.leader)
         for (int j = 0; j < D && j < t.nst; ++j) t.issue(j);
