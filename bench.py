@@ -344,6 +344,7 @@ def run_virs(args):
         return
     peak, peak_kind = peaks()
     value = nvox * args.steps / (r32["ms"] * 1e-3) / 1e9 * world
+    interior = int(np.prod([d - 2 for d in args.size]))
     kernel_ms = r32.get("kernel_ms")
     achieved = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
     line = {
@@ -364,6 +365,10 @@ def run_virs(args):
                         "8 receivers, Courant 1/sqrt(3), centered boundary form"
                         % (*args.size, STORAGE_NAMES[args.storage]),
             "voxels": nvox,
+            # the count above is every cell the stencil streams; the interior
+            # (border planes excluded) alongside, with its own rate
+            "interior_voxels": interior,
+            "interior_value": round(interior * args.steps / (r32["ms"] * 1e-3) / 1e9 * world, 3),
             "boundary_voxels": int(r32["meta"]["info"].boundary_count),
             "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * (bpv - 1) / 3 / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
