@@ -257,6 +257,22 @@ virs_status virs_start_simulation(virs_sim *sim, uint64_t steps);
  * *keep_going (may be NULL). */
 virs_status virs_step(virs_sim *sim, uint32_t step, int *keep_going, float *sample);
 
+/* The reference's stop rule (simulator_gpu.cu:303-330, applied on the host
+ * after every step; virs_step keeps that form) evaluated on the device, so
+ * that graph-launched runs can stop too: with enable = 1, after every step
+ * of virs_run / virs_run_host past step 3000 the post kernel takes the RMS
+ * of receiver 0's last 100 samples through the reference's slow filter, and
+ * once it is below 0.0009 every later kernel of the run returns at once.
+ * The run then ends after the step that fired the rule: virs_run /
+ * virs_run_host synchronise when the rule is on, steps_done
+ * (virs_get_grid_info) is that step + 1, the fields and samples are those
+ * of that step, and further runs do nothing until virs_start_simulation.
+ * Off by default (benchmarks run every step).  virs_step, the adjoint and
+ * batches refuse or ignore it: they run every step. */
+virs_status virs_set_stop_rule(virs_sim *sim, int enable);
+/* whether the rule fired, and at which step */
+virs_status virs_get_stop(const virs_sim *sim, int *stopped, uint64_t *stop_step);
+
 /* Run `steps` steps on `stream` (a cudaStream_t, NULL = the handle's own
  * stream) with no host traffic; the step loop is a CUDA graph.  Returns
  * when the work is queued. */

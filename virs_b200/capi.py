@@ -98,6 +98,8 @@ _SIGS = {
     "virs_run_host": ([_P, C.c_uint64, _P, _P, _P], C.c_int),
     "virs_synchronize": ([_P], C.c_int),
     "virs_get_ir": ([_P, C.c_uint64, C.c_uint64, _P], C.c_int),
+    "virs_set_stop_rule": ([_P, C.c_int], C.c_int),
+    "virs_get_stop": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_uint64)], C.c_int),
     "virs_get_pressure": ([_P, _P, _P, C.c_size_t], C.c_int),
     "virs_set_pressure": ([_P, _P, _P, C.c_size_t], C.c_int),
     "virs_init_pressure_sphere": ([_P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_int], C.c_int),
@@ -397,6 +399,16 @@ class Simulation:
 
     def synchronize(self):
         check(lib().virs_synchronize(self._h))
+
+    def set_stop_rule(self, enable: bool):
+        """The reference's RMS stop rule evaluated on the device in run()."""
+        check(lib().virs_set_stop_rule(self._h, int(bool(enable))))
+
+    def stop_state(self):
+        """(stopped, stop_step)."""
+        a, b = C.c_int(), C.c_uint64()
+        check(lib().virs_get_stop(self._h, C.byref(a), C.byref(b)))
+        return bool(a.value), int(b.value)
 
     def ir(self, first: int = 0, steps: int | None = None) -> np.ndarray:
         if steps is None:

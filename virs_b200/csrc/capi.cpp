@@ -155,6 +155,11 @@ struct virs_sim {
     // virs_step's RMS rule (simulator_gpu.cu:303-330)
     std::vector<float> out0;
     float rms_state = 0.f;
+    // the same rule on the device for virs_run / virs_run_host
+    // (virs_set_stop_rule): {stopped, stop step, filter state}
+    DevBuf stopbuf;
+    bool stop_rule = false, stopped = false;
+    uint64_t stop_step = 0;
 
     DevBuf energy_partial;
 
@@ -570,6 +575,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.bpos = s->bpos.as<uint32_t>();
     a.l2 = s->l2;
     a.rigid = s->prm.rigid_walls ? 1 : 0;
+    if (s->stop_rule) a.stop = s->stopbuf.as<uint32_t>();
     a.bmat = s->bmat.as<uint8_t>();
     a.bcode = s->bcode.as<uint8_t>();
     a.bnrm = s->bnrm.as<uint8_t>();
@@ -601,6 +607,7 @@ PostArgs post_args(const virs_sim *s, int parity)
 {
     PostArgs a{};
     a.q = s->field[parity ^ 1].ptr;
+    if (s->stop_rule) a.stop = s->stopbuf.as<uint32_t>();
     a.src = s->src.as<uint64_t>();
     a.sig = s->sig.as<float>();
     a.rcv = s->rcv.as<uint64_t>();
@@ -658,6 +665,7 @@ virs_status build_graphs(virs_sim *s, cudaStream_t st)
 
 virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
 {
+    if (s->stop_rule && s->stopped) return VIRS_OK; // nothing runs after the rule fired, until a new start
     if (!s->fields_valid) return fail(VIRS_E_STATE, "the fields were consumed by virs_adjoint: start the simulation again");
     VIRS_TRY(ready_to_run(s));
     VIRS_TRY(ensure_ir(s, s->steps_done + n));
@@ -704,9 +712,24 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
             if (e != cudaSuccess) return cuda_fail(e, "step launch");
         }
     }
+    const int cur0 = s->cur;
+    const uint64_t done0 = s->steps_done;
     s->cur ^= (int)(n & 1);
     s->steps_done += n;
     VIRS_CUDA(cudaEventRecord(s->done, st));
+    if (s->stop_rule) {
+        // how many of the n steps ran before the rule fired
+        uint32_t sb[2] = {0, 0};
+        VIRS_CUDA(cudaMemcpyAsync(sb, s->stopbuf.ptr, sizeof(sb), cudaMemcpyDeviceToHost, st));
+        VIRS_CUDA(cudaStreamSynchronize(st));
+        if (sb[0]) {
+            const uint64_t ran = (uint64_t)sb[1] + 1 - done0;
+            s->cur = cur0 ^ (int)(ran & 1);
+            s->steps_done = (uint64_t)sb[1] + 1;
+            s->stopped = true;
+            s->stop_step = sb[1];
+        }
+    }
     return VIRS_OK;
 }
 
@@ -1323,6 +1346,8 @@ VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
     VIRS_CUDA(cudaMemset(s->field[1].ptr, 0, s->field[1].bytes));
     VIRS_CUDA(cudaMemset(s->state.ptr, 0, s->state.bytes));
     VIRS_CUDA(cudaMemset(s->ctr.ptr, 0, 4));
+    if (s->stopbuf.ptr) VIRS_CUDA(cudaMemset(s->stopbuf.ptr, 0, s->stopbuf.bytes));
+    s->stopped = false;
     s->cur = 0;
     s->steps_done = 0;
     s->out0.clear();
@@ -1393,6 +1418,8 @@ VIRS_EXPORT virs_status virs_run_host(virs_sim *s, uint64_t steps, const float *
 VIRS_EXPORT virs_status virs_step(virs_sim *s, uint32_t step, int *keep_going, float *sample)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_step: null");
+    if (s->stop_rule)
+        return fail(VIRS_E_STATE, "virs_step applies the stop rule on the host: disable the device rule (virs_set_stop_rule)");
     if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
@@ -1432,6 +1459,29 @@ VIRS_EXPORT virs_status virs_step(virs_sim *s, uint32_t step, int *keep_going, f
         if (rms < 0.0009f) go = false;
     }
     if (keep_going) *keep_going = go ? 1 : 0;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_set_stop_rule(virs_sim *s, int enable)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_set_stop_rule: null");
+    if (enable != 0 && enable != 1) return fail(VIRS_E_ARG, "virs_set_stop_rule: enable must be 0 or 1");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    if (enable && !s->stopbuf.ptr) VIRS_TRY(s->stopbuf.alloc(4 * sizeof(uint32_t), "stop rule state"));
+    if (s->stopbuf.ptr) VIRS_CUDA(cudaMemset(s->stopbuf.ptr, 0, s->stopbuf.bytes));
+    s->stop_rule = enable != 0;
+    s->stopped = false;
+    s->drop_graphs();
+    ++s->gen;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_stop(const virs_sim *s, int *stopped, uint64_t *stop_step)
+{
+    if (!s || !stopped || !stop_step) return fail(VIRS_E_ARG, "virs_get_stop: null argument");
+    *stopped = s->stopped ? 1 : 0;
+    *stop_step = s->stopped ? s->stop_step : 0;
     return VIRS_OK;
 }
 
@@ -1642,6 +1692,8 @@ virs_status reset_state(virs_sim *s)
     VIRS_CUDA(cudaMemsetAsync(s->field[1].ptr, 0, s->field[1].bytes, s->stream));
     VIRS_CUDA(cudaMemsetAsync(s->state.ptr, 0, s->state.bytes, s->stream));
     VIRS_CUDA(cudaMemsetAsync(s->ctr.ptr, 0, 4, s->stream));
+    if (s->stopbuf.ptr) VIRS_CUDA(cudaMemsetAsync(s->stopbuf.ptr, 0, s->stopbuf.bytes, s->stream));
+    s->stopped = false;
     if (s->ir.ptr) VIRS_CUDA(cudaMemsetAsync(s->ir.ptr, 0, s->ir.bytes, s->stream));
     VIRS_CUDA(cudaStreamSynchronize(s->stream));
     s->cur = 0;
@@ -1850,8 +1902,10 @@ virs_status batch_build(virs_batch *b)
         for (int par = 0; par < 2; ++par) {
             m.step[par] = step_args(s, par);
             m.step[par].zc = zc;
+            m.step[par].stop = nullptr; // batches run every step
             m.step[par].tzmask = zm; // the batch's tiling, not the member's own
             m.post[par] = post_args(s, par);
+            m.post[par].stop = nullptr;
         }
         m.bidx = s->bidx.as<uint32_t>();
         m.gx = (s->px + tma_tile_x() - 1) / tma_tile_x();
@@ -2085,6 +2139,7 @@ VIRS_EXPORT virs_status virs_forward_checkpointed(virs_sim *s, uint64_t steps, u
     if (s->depth == 0) return fail(VIRS_E_STATE, "the adjoint needs the TMA kernel (pipeline depth 1..3)");
     if (s->prm.rigid_walls)
         return fail(VIRS_E_STATE, "the adjoint assumes the mirrored update at boundary voxels, not rigid_walls");
+    if (s->stop_rule) return fail(VIRS_E_STATE, "the adjoint runs every step: disable the stop rule (virs_set_stop_rule)");
     VIRS_TRY(virs_start_simulation(s, steps));
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     auto &A = s->adj;

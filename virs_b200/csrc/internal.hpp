@@ -69,6 +69,7 @@ constexpr int SEG = 128;              // voxels per boundary-prefix segment
 
 struct StepArgs {
     float4 *side;           // per boundary slot {free, p, p^{n-1}, 0}, kept by the boundary pass for the adjoint
+    const uint32_t *stop;   // nonzero *stop: the RMS stop rule has fired, the step does nothing (nullptr: off)
     const uint64_t *tzmask; // TMA stencil, per tile: bit j = the codes of stage j are all zero (nullptr: none)
     const void *p;          // p^n (storage type)
     void *q;                // in p^{n-1}, out p^{n+1}
@@ -109,6 +110,7 @@ struct PostArgs {
     uint32_t nhpos;
     uint32_t nhard;         // per-step hard-source values (scaled) in `hard`
     const float *hard;
+    uint32_t *stop;         // the RMS stop rule on the device (nullptr: off): {stopped, stop step, filter state}
 };
 
 // one member of a batched run (device-resident descriptor)

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
     const int x = x0 + lane * VEC;
     const int y0 = blockIdx.y * TY;
     const int y = y0 + ty;
+    if (a.stop && *a.stop) return; // the stop rule fired at an earlier step
     const int z0 = 1 + blockIdx.z * a.zc;
     const int z1 = min(z0 + a.zc, (int)a.nz - 1);
     if (z0 >= z1) return; // uniform over the block
@@ -240,6 +241,7 @@ constexpr int BT = 256;
 template <typename T, int MODE, int MAXS>
 __global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArgs a)
 {
+    if (a.stop && *a.stop) return; // the stop rule fired at an earlier step
     const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
     const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
     BVox<T, MAXS> v0, v1;
@@ -276,10 +278,38 @@ __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__res
     bvox_update<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
 }
 
+// The reference's stop rule (simulator_gpu.cu:303-330) on receiver 0's
+// samples of the steps before step sn, in the host rule's float operations
+// and order: after step 3000 the RMS of the last 100 samples, through a
+// slow first-order filter from step 3002 on; below 0.0009 the run stops.
+__device__ __forceinline__ void stop_rule(const PostArgs &a, uint32_t sn)
+{
+    constexpr uint32_t RMS_SIZE = 100, MIN_RMS_CHECK_STEP = 3000;
+    if (sn <= MIN_RMS_CHECK_STEP) return;
+    float sum = 0.f;
+    for (uint32_t i = sn - RMS_SIZE; i < sn; ++i) sum = __fadd_rn(sum, __fmul_rn(a.ir[i], a.ir[i]));
+    float rms = __fsqrt_rn(__fdiv_rn(sum, (float)RMS_SIZE));
+    float state = __uint_as_float(a.stop[2]);
+    if (sn == MIN_RMS_CHECK_STEP + 1) {
+        state = rms;
+    } else {
+        const float g = 0.00008f;
+        const float vout = __fdiv_rn(__fadd_rn(__fmul_rn(g, rms), state), __fadd_rn(g, 1.f));
+        state = __fsub_rn(__fmul_rn(2.f, vout), state);
+        rms = vout;
+    }
+    a.stop[2] = __float_as_uint(state);
+    if (rms < 0.0009f) {
+        a.stop[1] = sn;
+        a.stop[0] = 1u;
+    }
+}
+
 template <typename T> __device__ __forceinline__ void post_body(const PostArgs &a)
 {
     using IO = Io<T>;
     T *Q = static_cast<T *>(a.q);
+    if (a.stop && a.stop[0]) return; // the stop rule fired at an earlier step
     const uint32_t sn = *a.ctr;
     // hard-source voxels (flag 3, simulator_gpu.cu:59-63): the stencils leave
     // them alone; their value of this step is written here, before the soft
@@ -299,7 +329,10 @@ template <typename T> __device__ __forceinline__ void post_body(const PostArgs &
         for (uint32_t r = threadIdx.x; r < a.nrcv; r += blockDim.x)
             a.ir[(uint64_t)r * a.cap + sn] = __fmul_rn(IO::get(Q[a.rcv[r]]), a.inv_scale);
     __syncthreads();
-    if (threadIdx.x == 0) *a.ctr = sn + 1;
+    if (threadIdx.x == 0) {
+        if (a.stop && a.nrcv && sn < a.cap) stop_rule(a, sn);
+        *a.ctr = sn + 1;
+    }
 }
 
 template <typename T> __global__ void k_post(const __grid_constant__ PostArgs a) { post_body<T>(a); }

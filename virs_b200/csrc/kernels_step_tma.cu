@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k
                                                                         const __grid_constant__ CUtensorMap mC, int *err)
 {
     constexpr int D = L + 2;
+    if (a.stop && *a.stop) return; // the stop rule fired at an earlier step (uniform over the block)
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
