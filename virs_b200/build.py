@@ -21,6 +21,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "libvirs_b200.so"
+CLI_SRC = PKG / "cli" / "virs_simulate.cpp"
+CLI = PKG / "virs_simulate"
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -79,7 +81,21 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_cli(force)
     return LIB
+
+
+def build_cli(force: bool = False) -> Path:
+    """The command-line program over the library (next to it, found through
+    its rpath)."""
+    deps = [CLI_SRC, LIB, ROOT / "include" / "virs.h", ROOT / "include" / "virs.hpp"]
+    if force or not CLI.exists() or any(d.stat().st_mtime > CLI.stat().st_mtime for d in deps):
+        cmd = [CXX, "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{ROOT / 'include'}", str(CLI_SRC), f"-L{PKG}",
+               "-lvirs_b200", "-Wl,-rpath,$ORIGIN", "-o", str(CLI)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CLI build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return CLI
 
 
 def main() -> None:
