@@ -67,6 +67,32 @@ def test_configuration_errors(cli, tmp_path):
         assert r.returncode == 2 and word in r.stderr, (cfg, r.stderr)
 
 
+def test_material_configuration_errors(cli, tmp_path):
+    base = {"files": {"meshfile": "a.obj", "audiofile": "a.wav"}, "simulation": {"num_simulation_steps": 10}}
+    for extra, word in [({"materials": {"index": 0}}, "array"),
+                        ({"materials": [{"type": "wall"}]}, "'index'"),
+                        ({"materials": [{"index": 0, "type": "glass"}]}, "unknown material type"),
+                        ({"materials": [{"index": 0, "type": "wall", "absorber": 2}],
+                          "absorbers": [{"reflection": 0.9, "cutoff": 500}]}, "does not define"),
+                        ({"materials": [{"index": 0, "type": "wall", "absorber": 1}]}, "'absorbers' is missing"),
+                        ({"absorbers": [{"reflection": 0.9}]}, "each absorber"),
+                        ({"absorbers": [{"alpha": [0.1, 0.2]}]}, "each absorber"),
+                        ({"source": {"audio": True}}, "cannot open")]:
+        (tmp_path / "c.json").write_text(json.dumps({**base, **extra}))
+        r = _run(cli, "simulate", "-i", tmp_path / "c.json", cwd=tmp_path)
+        assert r.returncode == 2 and word in r.stderr, (extra, r.stderr)
+
+
+def _write_wav(path, x, rate, channels=2):
+    """32-bit float WAV, the signal in channel 1 and its negative in 0."""
+    x = np.asarray(x, np.float32)
+    frames = np.stack([-x, x] if channels == 2 else [x], axis=1).reshape(-1)
+    data = frames.tobytes()
+    hdr = b"RIFF" + struct.pack("<I", 4 + 24 + 8 + len(data)) + b"WAVE"
+    hdr += b"fmt " + struct.pack("<IHHIIHH", 16, 3, channels, rate, rate * 4 * channels, 4 * channels, 32)
+    Path(path).write_bytes(hdr + b"data" + struct.pack("<I", len(data)) + data)
+
+
 def _write_room(tmp_path, sc):
     """The scene as an OBJ with an mtllib: walls (material 0) and a speaker
     box (material 1), one quad per two triangles."""
@@ -134,3 +160,55 @@ def test_cli_wav_equals_python_run(cli, tmp_path):
     # the reference's receiver voxel lies outside this small grid
     r = _run(cli, "simulate", "-i", cfg, "-o", out)
     assert r.returncode == 2 and "outside" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_materials_absorbers_and_audio_source(cli, tmp_path):
+    """Material indexing (walls with two absorbers: a first-order design and
+    a three-band cascade), and the speaker voxels playing channel 1 of a WAV
+    file: the same samples as the Python binding given the same roles,
+    filters and audio."""
+    sc = scenes.reference_room(size=(8, 6, 5))
+    _write_room(tmp_path, sc)
+    steps = 300
+    t = np.arange(2000) / 48000.0
+    sig = (np.sin(2 * np.pi * 700 * t) * np.exp(-t * 400)).astype(np.float32)
+    _write_wav(tmp_path / "in.wav", sig, 48000)
+    roles = np.array([1, 0xFE], np.uint8)                  # walls take absorber 1, material 1 is the speaker
+    sim = capi.Simulation(capi.default_params())
+    sim.set_material_roles(roles)
+    sim.load_obj(tmp_path / "room.obj")
+    sim.classify()
+    g = sim.info()
+    fs = float(g.sample_rate)
+    des = [capi.design_first_order(fs, 0.85, 800.0), capi.design_octave_cascade(fs, [0.2, 0.4, 0.6])]
+    coef = np.zeros((2, 3, 5), np.float32)
+    coef[0, :, 0] = 1.0
+    coef[0, 0] = des[0].astype(np.float32).reshape(5)
+    coef[1] = des[1].astype(np.float32).reshape(3, 5)
+    sim.set_filters(coef, n_sections=3)
+    sim.set_hard_source_audio(sig, 48000.0, steps)
+    shape = (int(g.nx), int(g.ny), int(g.nz))
+    L = np.array([8, 6, 5], np.float32) * np.float32(0.05)
+    idx = int(scenes.voxel_index(0.85 * L, np.array(list(g.bbox_min), np.float32), g.cell_size, shape)[0])
+    x, y, z = idx % shape[0], (idx // shape[0]) % shape[1], idx // (shape[0] * shape[1])
+    sim.set_receivers([idx])
+    sim.start(steps)
+    sim.run(steps)
+    sos = capi.design_chebyshev_lowpass(fs, 0.45 * 48000, 0.5 * 48000, 0.5, 90.0)
+    want = sim.postprocess_ir(48000.0, sos, True)[0]
+    sim.close()
+
+    cfg = _config(tmp_path, materials=[{"index": 0, "type": "wall", "absorber": 1}, {"index": 1, "type": "source"}],
+                  absorbers=[{"reflection": 0.85, "cutoff": 800.0}, {"alpha": [0.2, 0.4, 0.6]}],
+                  source={"audio": True, "channel": 1})
+    cfg_d = json.loads(cfg.read_text())
+    cfg_d["files"]["audiofile"] = str(tmp_path / "in.wav")
+    cfg_d["simulation"]["num_simulation_steps"] = steps
+    cfg.write_text(json.dumps(cfg_d))
+    out = tmp_path / "out.wav"
+    r = _run(cli, "simulate", "-i", cfg, "-o", out, "--receiver", f"{x},{y},{z}")
+    assert r.returncode == 0, r.stderr
+    _, data = _read_wav(out)
+    assert np.abs(want).max() == 1.0
+    assert np.array_equal(data.view(np.uint32), want.view(np.uint32))

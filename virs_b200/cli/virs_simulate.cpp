@@ -6,10 +6,23 @@
 //
 // The configuration is the reference's JSON file (Simulator::loadConfig,
 // src/simulator/simulator.cpp:165-260): files.meshfile (the OBJ, opened
-// relative to the working directory), files.audiofile (required, as there,
-// and not used: the reference's step drives its speaker voxels with the
-// fixed hard-source pulse) and simulation.num_simulation_steps.  Then, as
-// Simulator::simulate (simulator.cpp:933-1100): the mesh is voxelised and
+// relative to the working directory), files.audiofile (required, as there)
+// and simulation.num_simulation_steps.  Three optional keys carry the
+// material indexing and audio sources that the reference's TODO.md plans
+// ("Material indexing", "Audio file implementation"):
+//   "materials": [{"index": i, "type": "wall" | "source" | "ignore",
+//                  "absorber": a}]   OBJ material i (the order of newmtl
+//                                    declarations) and its role; default
+//                                    the reference's: 0 wall, 1 source
+//   "absorbers": [{"reflection": R, "cutoff": fc} | {"alpha": [a, b, c]}]
+//                                    filter a: a first-order absorber or a
+//                                    three-band cascade (FP64 designs);
+//                                    default the reference's high-pass
+//   "source": {"audio": true, "channel": k}
+//                                    the speaker voxels play channel k of
+//                                    files.audiofile (a WAV file) instead
+//                                    of the reference's fixed pulse
+// Then, as Simulator::simulate (simulator.cpp:933-1100): the mesh is voxelised and
 // classified with the reference's defaults, the receiver is the voxel
 // (334, 225, 270) unless --receiver names another, the steps run with the
 // reference's RMS stop rule (here on the device), and the receiver trace is
@@ -20,6 +33,7 @@
 //
 // Exit status: 0 on success, 2 for a usage or configuration error, 3 when
 // the library reports an error (its message is printed).
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdint>
@@ -27,6 +41,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iterator>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -169,6 +184,63 @@ struct Parser {
     }
 };
 
+// ---- WAV input: one channel of PCM 16/24/32-bit or 32-bit float, as float -----
+
+bool read_wav(const std::string &path, int channel, std::vector<float> &out, float &rate, std::string &err)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f) { err = "cannot open " + path; return false; }
+    std::vector<unsigned char> b((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    auto u16 = [&](size_t i) { return (uint32_t)b[i] | ((uint32_t)b[i + 1] << 8); };
+    auto u32 = [&](size_t i) { return u16(i) | (u16(i + 2) << 16); };
+    if (b.size() < 12 || std::memcmp(b.data(), "RIFF", 4) || std::memcmp(b.data() + 8, "WAVE", 4)) {
+        err = path + ": not a RIFF/WAVE file";
+        return false;
+    }
+    uint32_t fmt = 0, nch = 0, sr = 0, bits = 0;
+    size_t data = 0, dlen = 0;
+    for (size_t i = 12; i + 8 <= b.size();) {
+        const uint32_t n = u32(i + 4);
+        if (!std::memcmp(b.data() + i, "fmt ", 4) && n >= 16 && i + 8 + n <= b.size()) {
+            fmt = u16(i + 8);
+            nch = u16(i + 10);
+            sr = u32(i + 12);
+            bits = u16(i + 22);
+            if (fmt == 0xFFFE && n >= 26) fmt = u16(i + 32); // WAVE_FORMAT_EXTENSIBLE: the sub-format
+        } else if (!std::memcmp(b.data() + i, "data", 4)) {
+            data = i + 8;
+            dlen = std::min<size_t>(n, b.size() - data);
+        }
+        i += 8 + (size_t)n + (n & 1);
+    }
+    const bool ok = nch > 0 && sr > 0 && data &&
+                    ((fmt == 1 && (bits == 16 || bits == 24 || bits == 32)) || (fmt == 3 && bits == 32));
+    if (!ok) { err = path + ": unsupported WAV format (PCM 16/24/32-bit or 32-bit float)"; return false; }
+    if (channel < 0 || (uint32_t)channel >= nch) {
+        err = path + ": no channel " + std::to_string(channel) + " (" + std::to_string(nch) + " channels)";
+        return false;
+    }
+    const size_t bps = bits / 8, frame = bps * nch, frames = dlen / frame;
+    out.resize(frames);
+    for (size_t k = 0; k < frames; ++k) {
+        const unsigned char *p = b.data() + data + k * frame + (size_t)channel * bps;
+        if (fmt == 3) {
+            std::memcpy(&out[k], p, 4);
+        } else if (bits == 16) {
+            out[k] = (float)(int16_t)((uint16_t)p[0] | ((uint16_t)p[1] << 8)) / 32768.f;
+        } else if (bits == 24) {
+            int32_t v = (int32_t)((uint32_t)p[0] << 8 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 24) >> 8;
+            out[k] = (float)v / 8388608.f;
+        } else {
+            int32_t v;
+            std::memcpy(&v, p, 4);
+            out[k] = (float)((double)v / 2147483648.0);
+        }
+    }
+    rate = (float)sr;
+    return true;
+}
+
 // ---- a 32-bit float mono WAV file (RIFF, format 3) -----------------------------
 
 bool write_wav(const std::string &path, const std::vector<float> &x, uint32_t rate)
@@ -276,13 +348,115 @@ int main(int argc, char **argv)
         return usage("configuration has no positive integer 'num_simulation_steps'");
     const uint64_t steps = steps_override > 0 ? (uint64_t)steps_override : (uint64_t)nsteps->num;
 
+    // material indexing: OBJ material id -> role (virs_set_material_roles)
+    std::vector<uint8_t> roles;
+    uint32_t max_absorber = 0;
+    bool any_wall_role = false;
+    if (const Json *mats = cfg.get("materials")) {
+        if (mats->kind != Json::ARR) return usage("'materials' must be an array");
+        for (const Json &m : mats->arr) {
+            const Json *ix = m.get("index"), *ty = m.get("type");
+            if (!ix || ix->kind != Json::NUM || ix->num < 0 || ix->num > 255 || ix->num != std::floor(ix->num))
+                return usage("each material needs an integer 'index' in 0..255");
+            if (!ty || ty->kind != Json::STR) return usage("each material needs a 'type' (wall, source or ignore)");
+            const size_t i = (size_t)ix->num;
+            if (roles.size() <= i) roles.resize(i + 1, VIRS_ROLE_IGNORE);
+            if (ty->str == "wall") {
+                const Json *ab = m.get("absorber");
+                double a = 0;
+                if (ab) {
+                    if (ab->kind != Json::NUM || ab->num < 0 || ab->num > 63 || ab->num != std::floor(ab->num))
+                        return usage("a wall's 'absorber' must be an integer in 0..63");
+                    a = ab->num;
+                }
+                roles[i] = (uint8_t)a;
+                max_absorber = std::max(max_absorber, (uint32_t)a);
+                any_wall_role = true;
+            } else if (ty->str == "source") {
+                roles[i] = VIRS_ROLE_SOURCE;
+            } else if (ty->str == "ignore") {
+                roles[i] = VIRS_ROLE_IGNORE;
+            } else {
+                return usage(("unknown material type '" + ty->str + "'").c_str());
+            }
+        }
+    }
+    // absorbers: one filter cascade per absorber index
+    const Json *absorbers = cfg.get("absorbers");
+    if (absorbers && (absorbers->kind != Json::ARR || absorbers->arr.empty()))
+        return usage("'absorbers' must be a non-empty array");
+    if (absorbers && any_wall_role && max_absorber >= absorbers->arr.size())
+        return usage("a material names an absorber that 'absorbers' does not define");
+    if (!absorbers && any_wall_role && max_absorber > 0)
+        return usage("materials name absorbers beyond 0 but 'absorbers' is missing");
+    if (absorbers)
+        for (const Json &a : absorbers->arr) {
+            const Json *r = a.get("reflection"), *fc = a.get("cutoff"), *al = a.get("alpha");
+            const bool first = r && fc && r->kind == Json::NUM && fc->kind == Json::NUM;
+            const bool bands = al && al->kind == Json::ARR && al->arr.size() == 3;
+            if (first == bands) return usage("each absorber is {reflection, cutoff} or {alpha: [3 values]}");
+            if (bands)
+                for (const Json &v : al->arr)
+                    if (v.kind != Json::NUM) return usage("'alpha' values must be numbers");
+        }
+    // the speaker voxels: the reference's pulse, or a channel of the audio file
+    int audio_channel = -1;
+    if (const Json *src = cfg.get("source")) {
+        const Json *au = src->get("audio"), *ch = src->get("channel");
+        if (au && au->kind == Json::BOOL && au->b) {
+            audio_channel = 0;
+            if (ch) {
+                if (ch->kind != Json::NUM || ch->num < 0 || ch->num != std::floor(ch->num))
+                    return usage("'channel' must be a non-negative integer");
+                audio_channel = (int)ch->num;
+            }
+        }
+    }
+    std::vector<float> audio_samples;
+    float audio_rate = 0.f;
+    if (audio_channel >= 0) {
+        std::string err;
+        if (!read_wav(audio->str, audio_channel, audio_samples, audio_rate, err)) return usage(err.c_str());
+        if (audio_samples.empty()) return usage("the audio file has no samples");
+    }
+
     try {
         virs_params p = virs::default_params();
         p.storage = storage == "bf16" ? VIRS_STORAGE_BF16 : storage == "f16" ? VIRS_STORAGE_F16 : VIRS_STORAGE_F32;
         virs::Simulator sim(p);
+        if (!roles.empty()) sim.set_material_roles(roles);
         sim.load_obj(mesh->str);
         sim.classify();
         const virs_grid_info g = sim.info();
+        if (absorbers) {
+            // FP64 designs at the simulation rate; shorter cascades padded
+            // with pass-through sections {1, 0, 0, 0, 0}
+            std::vector<std::vector<double>> des;
+            uint32_t ns = 1;
+            for (const Json &a : absorbers->arr) {
+                std::vector<double> c;
+                if (const Json *al = a.get("alpha")) {
+                    const double alpha[3] = {al->arr[0].num, al->arr[1].num, al->arr[2].num};
+                    c.resize(15);
+                    virs::check(virs_design_octave_cascade(g.sample_rate, alpha, nullptr, c.data()));
+                } else {
+                    c.resize(5);
+                    virs::check(virs_design_first_order(g.sample_rate, a.get("reflection")->num, a.get("cutoff")->num,
+                                                        c.data()));
+                }
+                ns = std::max<uint32_t>(ns, (uint32_t)(c.size() / 5));
+                des.push_back(std::move(c));
+            }
+            std::vector<float> coef;
+            for (const auto &c : des)
+                for (uint32_t q = 0; q < ns; ++q)
+                    for (int k = 0; k < 5; ++k)
+                        coef.push_back(q * 5 < c.size() ? (float)c[q * 5 + k] : (k == 0 ? 1.f : 0.f));
+            sim.set_filters((uint32_t)des.size(), ns, coef);
+        }
+        if (audio_channel >= 0)
+            virs::check(virs_set_hard_source_audio(sim.handle(), audio_samples.data(), audio_samples.size(), audio_rate,
+                                                   steps));
         if (rx < 0 || ry < 0 || rz < 0 || (uint64_t)rx >= g.nx || (uint64_t)ry >= g.ny || (uint64_t)rz >= g.nz) {
             std::fprintf(stderr, "virs_simulate: receiver (%lld, %lld, %lld) is outside the %llux%llux%llu grid; "
                                  "pass --receiver X,Y,Z\n",
