@@ -266,7 +266,9 @@ virs_status virs_step(virs_sim *sim, uint32_t step, int *keep_going, float *samp
  * The run then ends after the step that fired the rule: virs_run /
  * virs_run_host synchronise when the rule is on, steps_done
  * (virs_get_grid_info) is that step + 1, the fields and samples are those
- * of that step, and further runs do nothing until virs_start_simulation.
+ * of that step (virs_run_host still copies the samples it was asked for:
+ * those of steps that did not run are 0), and further runs do nothing
+ * until virs_start_simulation.
  * Off by default (benchmarks run every step).  virs_step, the adjoint and
  * batches refuse or ignore it: they run every step. */
 virs_status virs_set_stop_rule(virs_sim *sim, int enable);
