@@ -77,7 +77,10 @@ def test_material_configuration_errors(cli, tmp_path):
                         ({"materials": [{"index": 0, "type": "wall", "absorber": 1}]}, "'absorbers' is missing"),
                         ({"absorbers": [{"reflection": 0.9}]}, "each absorber"),
                         ({"absorbers": [{"alpha": [0.1, 0.2]}]}, "each absorber"),
-                        ({"source": {"audio": True}}, "cannot open")]:
+                        ({"source": {"audio": True}}, "cannot open"),
+                        ({"sources": [{"position": [0.1, 0.2]}]}, "'position'"),
+                        ({"sources": [{"position": [0.1, 0.2, 0.3], "channel": -1}]}, "'channel'"),
+                        ({"sources": [{"position": [0.1, 0.2, 0.3]}]}, "cannot open")]:
         (tmp_path / "c.json").write_text(json.dumps({**base, **extra}))
         r = _run(cli, "simulate", "-i", tmp_path / "c.json", cwd=tmp_path)
         assert r.returncode == 2 and word in r.stderr, (extra, r.stderr)
@@ -211,4 +214,47 @@ def test_cli_materials_absorbers_and_audio_source(cli, tmp_path):
     assert r.returncode == 0, r.stderr
     _, data = _read_wav(out)
     assert np.abs(want).max() == 1.0
+    assert np.array_equal(data.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_cli_point_sources_play_audio_channels(cli, tmp_path):
+    """Two point sources (metres), each playing one channel of a stereo WAV
+    file, the speaker box left to the reference's pulse: the same samples
+    as the Python binding given the same voxels and signals."""
+    sc = scenes.reference_room(size=(8, 6, 5))
+    _write_room(tmp_path, sc)
+    steps = 300
+    t = np.arange(3000) / 44100.0
+    sig = (np.sin(2 * np.pi * 500 * t) * np.exp(-t * 300)).astype(np.float32)
+    _write_wav(tmp_path / "in.wav", sig, 44100)               # channel 0: -sig, channel 1: sig
+    pos = np.array([[0.05, 0.25, 0.05], [0.35, 0.05, 0.20]], np.float32)      # near two corners, in the air
+    sim = capi.Simulation(capi.default_params())
+    sim.load_obj(tmp_path / "room.obj")
+    sim.classify()
+    g = sim.info()
+    shape = (int(g.nx), int(g.ny), int(g.nz))
+    bmin = np.array(list(g.bbox_min), np.float32)
+    src = scenes.voxel_index(pos, bmin, g.cell_size, shape)
+    sim.set_sources_audio(src, np.stack([-sig, sig]), 44100.0, steps)
+    L = np.array([8, 6, 5], np.float32) * np.float32(0.05)
+    idx = int(scenes.voxel_index(0.85 * L, bmin, g.cell_size, shape)[0])
+    x, y, z = idx % shape[0], (idx // shape[0]) % shape[1], idx // (shape[0] * shape[1])
+    sim.set_receivers([idx])
+    sim.start(steps)
+    sim.run(steps)
+    sos = capi.design_chebyshev_lowpass(float(g.sample_rate), 0.45 * 48000, 0.5 * 48000, 0.5, 90.0)
+    want = sim.postprocess_ir(48000.0, sos, True)[0]
+    sim.close()
+
+    cfg = _config(tmp_path, sources=[{"position": pos[0].tolist(), "channel": 0},
+                                     {"position": pos[1].tolist(), "channel": 1}])
+    cfg_d = json.loads(cfg.read_text())
+    cfg_d["files"]["audiofile"] = str(tmp_path / "in.wav")
+    cfg_d["simulation"]["num_simulation_steps"] = steps
+    cfg.write_text(json.dumps(cfg_d))
+    out = tmp_path / "out.wav"
+    r = _run(cli, "simulate", "-i", cfg, "-o", out, "--receiver", f"{x},{y},{z}")
+    assert r.returncode == 0, r.stderr
+    _, data = _read_wav(out)
     assert np.array_equal(data.view(np.uint32), want.view(np.uint32))

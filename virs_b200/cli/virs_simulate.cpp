@@ -22,6 +22,11 @@
 //                                    the speaker voxels play channel k of
 //                                    files.audiofile (a WAV file) instead
 //                                    of the reference's fixed pulse
+//   "sources": [{"position": [x, y, z], "channel": k}]
+//                                    point sources in metres (the voxel by
+//                                    toVoxel and truncation, simulator.h:
+//                                    32-45), each playing its channel of
+//                                    files.audiofile, added to the field
 // Then, as Simulator::simulate (simulator.cpp:933-1100): the mesh is voxelised and
 // classified with the reference's defaults, the receiver is the voxel
 // (334, 225, 270) unless --receiver names another, the steps run with the
@@ -419,6 +424,34 @@ int main(int argc, char **argv)
         if (!read_wav(audio->str, audio_channel, audio_samples, audio_rate, err)) return usage(err.c_str());
         if (audio_samples.empty()) return usage("the audio file has no samples");
     }
+    // point sources playing channels of the audio file
+    struct PointSource {
+        float pos[3];
+        std::vector<float> samples;
+    };
+    std::vector<PointSource> points;
+    float points_rate = 0.f;
+    if (const Json *ps = cfg.get("sources")) {
+        if (ps->kind != Json::ARR) return usage("'sources' must be an array");
+        for (const Json &e : ps->arr) {
+            const Json *pos = e.get("position"), *ch = e.get("channel");
+            if (!pos || pos->kind != Json::ARR || pos->arr.size() != 3 || pos->arr[0].kind != Json::NUM ||
+                pos->arr[1].kind != Json::NUM || pos->arr[2].kind != Json::NUM)
+                return usage("each source needs a 'position' [x, y, z] in metres");
+            int c = 0;
+            if (ch) {
+                if (ch->kind != Json::NUM || ch->num < 0 || ch->num != std::floor(ch->num))
+                    return usage("a source's 'channel' must be a non-negative integer");
+                c = (int)ch->num;
+            }
+            PointSource p;
+            for (int k = 0; k < 3; ++k) p.pos[k] = (float)pos->arr[k].num;
+            std::string err;
+            if (!read_wav(audio->str, c, p.samples, points_rate, err)) return usage(err.c_str());
+            if (p.samples.empty()) return usage("the audio file has no samples");
+            points.push_back(std::move(p));
+        }
+    }
 
     try {
         virs_params p = virs::default_params();
@@ -457,6 +490,29 @@ int main(int argc, char **argv)
         if (audio_channel >= 0)
             virs::check(virs_set_hard_source_audio(sim.handle(), audio_samples.data(), audio_samples.size(), audio_rate,
                                                    steps));
+        if (!points.empty()) {
+            // toVoxel, then truncation (Simulator::getGridIdxFromVecPos)
+            std::vector<uint64_t> idx;
+            const size_t len = points[0].samples.size(); // every channel of one file has the same length
+            std::vector<float> chans;
+            for (const PointSource &p : points) {
+                uint64_t v[3];
+                const uint64_t dim[3] = {g.nx, g.ny, g.nz};
+                for (int k = 0; k < 3; ++k) {
+                    const float t = (p.pos[k] - g.bbox_min[k]) / g.cell_size;
+                    if (!(t >= 0.f) || (uint64_t)t >= dim[k]) {
+                        std::fprintf(stderr, "virs_simulate: source at (%g, %g, %g) m is outside the grid\n",
+                                     (double)p.pos[0], (double)p.pos[1], (double)p.pos[2]);
+                        return 2;
+                    }
+                    v[k] = (uint64_t)t;
+                }
+                idx.push_back((v[2] * g.ny + v[1]) * g.nx + v[0]);
+                chans.insert(chans.end(), p.samples.begin(), p.samples.end());
+            }
+            virs::check(virs_set_sources_audio(sim.handle(), (uint32_t)idx.size(), idx.data(), chans.data(), len,
+                                               points_rate, steps));
+        }
         if (rx < 0 || ry < 0 || rz < 0 || (uint64_t)rx >= g.nx || (uint64_t)ry >= g.ny || (uint64_t)rz >= g.nz) {
             std::fprintf(stderr, "virs_simulate: receiver (%lld, %lld, %lld) is outside the %llux%llux%llu grid; "
                                  "pass --receiver X,Y,Z\n",
