@@ -450,16 +450,18 @@ virs_status ensure_ir(virs_sim *s, uint64_t need)
     return VIRS_OK;
 }
 
+// looked up once, in a static initialiser (thread-safe: handles may be
+// created and retiled from several host threads)
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return nullptr;
+    }();
     return fn;
 }
 
