@@ -1,8 +1,9 @@
 """Edge cases of the step through the C ABI, against the oracle bit for bit:
 a grid with no boundary voxels (an empty boundary list: the pass is not
 launched, alone or in a batch), the smallest grid (3 x 3 x 3: one interior
-voxel), 16-bit storage on an empty list, and sizes beyond the 32-bit
-voxel positions rejected before any input is read."""
+voxel), 16-bit storage on an empty list, sizes beyond the 32-bit voxel
+positions rejected before any input is read, and two handles driven from
+two host threads at once."""
 import numpy as np
 import pytest
 
@@ -132,3 +133,36 @@ def test_grid_beyond_32_bit_positions_rejected():
             sim.set_grid((4096, 4096, 300), 0.05, np.zeros(8, np.uint8))
         assert e.value.status == capi.E_ARG
         assert "too large" in str(e.value)
+
+
+def test_two_handles_on_two_host_threads():
+    """Handles share no state but the autotuner's cache (locked) and the
+    tensor-map encoder (looked up once): two simulations driven from two
+    host threads at the same time give the results they give one after the
+    other."""
+    import threading
+    shape = (70, 36, 30)
+    flags, src, sig, rcv = _air_room(shape)
+    nx, ny, nz = shape
+    walls = flags.reshape(nz, ny, nx).copy()
+    walls[1:-1, 1:-1, 1] = walls[1:-1, 1:-1, -2] = 1
+    steps = 120
+
+    def run(f, out, k):
+        s = _sim(shape, f, src, sig, rcv, steps)
+        s.set_tiling(8, 0, 2)
+        s.run(steps)
+        out[k] = s.ir()
+        s.close()
+
+    alone = {}
+    run(flags, alone, 0)
+    run(walls.reshape(-1), alone, 1)
+    both = {}
+    th = [threading.Thread(target=run, args=(f, both, k)) for k, f in enumerate([flags, walls.reshape(-1)])]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for k in (0, 1):
+        assert np.array_equal(both[k].view(np.uint32), alone[k].view(np.uint32))
