@@ -53,6 +53,10 @@ sys.path.insert(0, str(ROOT))
 GRAPH_WARMUP = 64  # warm-up steps at least: both step graphs (32 steps per parity) built and launched once
 BYTES_F32 = 13.0   # per voxel update: p 4 + p^{n-1} 4 + p^{n+1} 4 + code 1
 BYTES_16 = 7.0     # 16-bit storage: 2 + 2 + 2 + 1
+# two steps per pass (time blocking), per voxel and launch: p^n, p^{n-1} in,
+# the code, p^{n+1}, p^{n+2} out
+PAIR_F32 = 17.0    # 4 + 4 + 1 + 4 + 4
+PAIR_16 = 9.0      # 2 + 2 + 1 + 2 + 2
 METRIC = "Gvoxel-updates/s"
 STORAGE_NAMES = {"f32": "FP32", "bf16": "BF16 storage (FP32 update)", "f16": "FP16 storage (FP32 update)"}
 KERNEL_TYPES = {"f32": "float", "bf16": "__nv_bfloat16", "f16": "__half"}
@@ -85,6 +89,20 @@ def measured_traffic(path: Path, storage: str, nvox: int):
                 src += f", captured on {n} voxels and scaled by {nvox / n:.3f}"
             return {"bytes": round(b * nvox / n), "source": src}
     return None
+
+
+def stencil_roofline(r, storage: str):
+    """(algorithmic bytes per voxel and launch, steps per launch, kernel name,
+    traffic file) of the run's dominant kernel: the two-step kernel when the
+    autotuner chose time blocking, else the single-step stencil."""
+    f32 = storage == "f32"
+    if r.get("time_blocking", {}).get("active"):
+        return (PAIR_F32 if f32 else PAIR_16, 2, "k_pair_tma<%s> (two steps per pass; then the boundary passes, "
+                "post kernels and the fix-up of the voxels next to boundary voxels and sources)" % KERNEL_TYPES[storage],
+                ROOT / "profiles" / "k_pair_tma_dram_traffic.txt")
+    return (BYTES_F32 if f32 else BYTES_16, 1,
+            "k_step_tma<%s> (stencil; boundary voxels in a separate list pass)" % KERNEL_TYPES[storage],
+            ROOT / "profiles" / "k_step_tma_dram_traffic.txt")
 
 
 def host_threads():
@@ -191,6 +209,13 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     total = warm + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
     sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
     tiling = sim.autotune(args.tune_steps) if args.tune_steps else sim.tiling()
+    if args.steps_per_pass:
+        # forced: single steps, or two steps per pass with the autotuner's
+        # two-step tiling when it chose one, else --pair-tiling
+        tb = sim.time_blocking()
+        rows, planes = (tb["rows"], tb["planes"]) if tb["active"] and not args.pair_tiling else \
+            tuple(args.pair_tiling or (16, 64))
+        sim.set_time_blocking(args.steps_per_pass, rows, planes)
     sim.run(warm, stream.cuda_stream)
     torch.cuda.synchronize()
     if dist:
@@ -200,7 +225,8 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     ms = max_over_ranks(ms, dist, f"cuda:{dev}")
     out = {"ms": ms, "clocks": clk.summary(), "meta": meta,
            "tiling": {"tile_rows": tiling.tile_rows, "planes_per_block": tiling.planes_per_block,
-                      "pipeline_depth": tiling.pipeline_depth}}
+                      "pipeline_depth": tiling.pipeline_depth},
+           "time_blocking": sim.time_blocking()}
     # per-kernel events over K' steps (no graph; events around each stencil launch)
     if args.kernel_steps:
         sim.set_timing(True)
@@ -208,8 +234,11 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         sim.synchronize()
         t = sim.timing()
         sim.set_timing(False)
+        # per launch of the dominant kernel (two steps with time blocking);
+        # the boundary pass per step
         out["kernel_ms"] = t.step_kernel_ms / max(t.step_launches, 1)
-        out["boundary_ms"] = t.boundary_kernel_ms / max(t.step_launches, 1)
+        per = 2 if out["time_blocking"]["active"] else 1
+        out["boundary_ms"] = t.boundary_kernel_ms / max(t.step_launches * per, 1)
     if want_e2e:
         nsrc, nrcv = len(sc.src_pos), len(sc.rcv_pos)
         first = int(sim.info().steps_done)
@@ -319,18 +348,21 @@ def run_virs(args):
     nvox = int(np.prod(args.size))
     stream = torch.cuda.Stream(device=dev)
     storage = {"f32": capi.STORAGE_F32, "bf16": capi.STORAGE_BF16, "f16": capi.STORAGE_F16}[args.storage]
-    bpv = BYTES_F32 if storage == capi.STORAGE_F32 else BYTES_16
+    fbytes = 4 if storage == capi.STORAGE_F32 else 2   # bytes of one field value
     r32 = bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e=True)
     variants = {}
     if args.variants and storage == capi.STORAGE_F32:
         rb = bench_storage(sc, capi.STORAGE_BF16, args, stream, dev, world, dist, want_e2e=False)
         gv = nvox * args.steps / (rb["ms"] * 1e-3) / 1e9 * world
         peak, _ = peaks()
+        bb, _, bkern, _ = stencil_roofline(rb, "bf16")
         variants["bf16_storage"] = {
             "value": gv, "ms_per_step": rb["ms"] / args.steps,
             "speedup_vs_f32": (r32["ms"] / rb["ms"]),
-            "roofline_frac": (nvox * BYTES_16 / (rb["kernel_ms"] * 1e-3) / 1e9) / peak if rb.get("kernel_ms") else None,
-            "bytes_per_voxel": BYTES_16,
+            "roofline_frac": (nvox * bb / (rb["kernel_ms"] * 1e-3) / 1e9) / peak if rb.get("kernel_ms") else None,
+            "bytes_per_voxel": bb,
+            "kernel": bkern.split(" ")[0],
+            "time_blocking": rb["time_blocking"],
         }
     if args.batch_steps:
         for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):
@@ -346,6 +378,7 @@ def run_virs(args):
     value = nvox * args.steps / (r32["ms"] * 1e-3) / 1e9 * world
     interior = int(np.prod([d - 2 for d in args.size]))
     kernel_ms = r32.get("kernel_ms")
+    bpv, steps_per_launch, kernel_name, traffic_file = stencil_roofline(r32, args.storage)
     achieved = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
     line = {
         "metric": METRIC,
@@ -370,10 +403,12 @@ def run_virs(args):
             "interior_voxels": interior,
             "interior_value": round(interior * args.steps / (r32["ms"] * 1e-3) / 1e9 * world, 3),
             "boundary_voxels": int(r32["meta"]["info"].boundary_count),
-            "l2": "inputs larger than L2 (2 x %.2f GB fields), no flush" % (nvox * (bpv - 1) / 3 / 1e9),
+            "l2": "inputs larger than L2 (%d x %.2f GB fields), no flush"
+                  % (4 if steps_per_launch == 2 else 2, nvox * fbytes / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
             "timing": "CUDA events on the launching stream around virs_run (CUDA graph), max over ranks",
             "tiling": r32["tiling"],
+            "time_blocking": r32["time_blocking"],
         },
         "roofline": {
             "bound": "hbm",
@@ -383,8 +418,9 @@ def run_virs(args):
             "frac": round(achieved / peak, 4) if achieved else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
             "traffic": None,
-            "kernel": "k_step_tma<%s> (stencil; boundary voxels in a separate list pass)" % KERNEL_TYPES[args.storage],
+            "kernel": kernel_name,
             "kernel_ms": kernel_ms,
+            "steps_per_launch": steps_per_launch,
             "bytes_per_voxel": bpv,
             "boundary_pass_ms": r32.get("boundary_ms"),
         },
@@ -402,7 +438,7 @@ def run_virs(args):
     }
     if "batched_bf16" in variants:
         variants["bf16_batched_vs_f32_plain"] = round(variants["batched_bf16"]["value"] / value, 3)
-    tr = measured_traffic(Path(args.traffic), args.storage, nvox)
+    tr = measured_traffic(Path(args.traffic) if args.traffic else traffic_file, args.storage, nvox)
     if tr:
         line["roofline"]["traffic"] = tr["bytes"]
         line["roofline"]["traffic_source"] = tr["source"]
@@ -494,7 +530,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--storage", choices=list(STORAGE_NAMES), default="f32",
                     help="field storage of the timed hall (f32 is the headline; bf16/f16 store 16-bit fields)")
-    ap.add_argument("--traffic", default=str(ROOT / "profiles" / "k_step_tma_dram_traffic.txt"),
+    ap.add_argument("--steps-per-pass", type=int, choices=[0, 1, 2], default=0,
+                    help="0: the autotuner's choice; 1: single steps; 2: two steps per pass (time blocking)")
+    ap.add_argument("--pair-tiling", type=int, nargs=2, default=None, metavar=("ROWS", "PLANES"),
+                    help="tile rows (16/32) and planes per block of the two-step kernel with --steps-per-pass 2")
+    ap.add_argument("--traffic", default=None,
                     help="ncu DRAM-traffic summary of the stencil kernel")
     args = ap.parse_args()
     if args.warmup < 3:

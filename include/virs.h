@@ -277,7 +277,9 @@ virs_status virs_get_stop(const virs_sim *sim, int *stopped, uint64_t *stop_step
 
 /* Run `steps` steps on `stream` (a cudaStream_t, NULL = the handle's own
  * stream) with no host traffic; the step loop is a CUDA graph.  Returns
- * when the work is queued. */
+ * when the work is queued.  The handle's own stream is a non-blocking
+ * stream: work on CUDA's legacy default stream is not ordered with it, so a
+ * caller that wants the legacy stream passes cudaStreamLegacy. */
 virs_status virs_run(virs_sim *sim, uint64_t steps, void *stream);
 
 /* End-to-end form for host callers: copies `signal` [n_src][steps] (or NULL
@@ -334,6 +336,20 @@ virs_status virs_get_timing(virs_sim *sim, virs_timing *out);
  * default (TMA, 2).  All variants give bit-identical results. */
 virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block, int pipeline_depth);
 
+/* Time blocking (no reference counterpart): with steps_per_pass = 2, virs_run
+ * and virs_run_host advance whole groups of four steps two at a time: one
+ * kernel reads p^n and p^{n-1} once and writes p^{n+1} and p^{n+2}, over two
+ * more field buffers allocated on first use (a grid for which they do not fit
+ * runs single steps).  The voxels next to boundary voxels and sources are
+ * recomputed after the first step is complete, so the results are
+ * bit-identical to single steps.  tile_rows 16 or 32 (0 = 16), planes per
+ * block 0 = all.  Off (1) by default; not used with the device stop rule or
+ * the register-streaming kernel (pipeline depth 0).  *active tells whether
+ * the current settings run two steps per pass. */
+virs_status virs_set_time_blocking(virs_sim *sim, int steps_per_pass, int tile_rows, int planes_per_block);
+virs_status virs_get_time_blocking(const virs_sim *sim, int *steps_per_pass, int *tile_rows, int *planes_per_block,
+                                   int *active);
+
 typedef struct virs_tiling {
     int32_t tile_rows;        /* 4, 8 or 16                                        */
     int32_t planes_per_block; /* z planes streamed by one block                    */
@@ -343,8 +359,11 @@ typedef struct virs_tiling {
 
 /* Autotuner (no reference counterpart): right after virs_start_simulation,
  * times `trial_steps` steps of each TMA variant (tile rows 4/8/16, depth
- * 1..3, 8..64 planes per block) on this handle's own grid and keeps the
- * fastest; the simulation is then back at rest.  Results are cached per
+ * 1..3, 8..64 planes per block) and then of the two-step variants (time
+ * blocking: tile rows 16/32, 32..128 planes per block, trial_steps rounded
+ * up to a multiple of four) on this handle's own grid and keeps the fastest:
+ * the tiling it returns, and the steps per pass that virs_get_time_blocking
+ * reports.  The simulation is then back at rest.  Results are cached per
  * device, storage and grid shape for the life of the process. */
 virs_status virs_autotune(virs_sim *sim, uint32_t trial_steps, virs_tiling *best);
 virs_status virs_get_tiling(const virs_sim *sim, virs_tiling *out);

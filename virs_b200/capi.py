@@ -108,6 +108,8 @@ _SIGS = {
     "virs_set_timing": ([_P, C.c_int], C.c_int),
     "virs_get_timing": ([_P, _P], C.c_int),
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "virs_set_time_blocking": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "virs_get_time_blocking": ([_P, _P, _P, _P, _P], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
     "virs_forward_checkpointed": ([_P, C.c_uint64, C.c_uint32, _P], C.c_int),
@@ -122,6 +124,19 @@ _SIGS = {
 }
 
 EXPORTED = tuple(_SIGS)
+
+# cudaStreamLegacy: the stream handle that names CUDA's legacy default stream
+_LEGACY_STREAM = 1
+
+
+def _stream(stream):
+    """A cudaStream_t given as an int (torch's `cuda_stream`): None is the
+    handle's own stream (NULL to the C API); 0, torch's default stream, is
+    CUDA's legacy default stream, passed as cudaStreamLegacy because NULL
+    would select the handle's stream."""
+    if stream is None:
+        return None
+    return _LEGACY_STREAM if int(stream) == 0 else int(stream)
 
 _lib = None
 
@@ -388,14 +403,14 @@ class Simulation:
         return bool(keep.value), float(v.value)
 
     def run(self, steps: int, stream: int | None = None):
-        check(lib().virs_run(self._h, steps, stream))
+        check(lib().virs_run(self._h, steps, _stream(stream)))
 
     def run_host(self, steps: int, signal=None, ir_out=None, stream: int | None = None):
         s = None if signal is None else _c(signal, np.float32)
-        check(lib().virs_run_host(self._h, steps, _ptr(s), _ptr(ir_out), stream))
+        check(lib().virs_run_host(self._h, steps, _ptr(s), _ptr(ir_out), _stream(stream)))
 
     def run_host_ptr(self, steps: int, signal_ptr, ir_ptr, stream: int | None = None):
-        check(lib().virs_run_host(self._h, steps, signal_ptr, ir_ptr, stream))
+        check(lib().virs_run_host(self._h, steps, signal_ptr, ir_ptr, _stream(stream)))
 
     def synchronize(self):
         check(lib().virs_synchronize(self._h))
@@ -452,7 +467,7 @@ class Simulation:
 
     def energy_noalloc(self, d_out_ptr: int, stream: int | None = None) -> None:
         """Enqueue the allocation-free energy into the device double at d_out_ptr."""
-        check(lib().virs_energy_noalloc(self._h, d_out_ptr, stream))
+        check(lib().virs_energy_noalloc(self._h, d_out_ptr, _stream(stream)))
 
     def set_timing(self, enable: bool):
         check(lib().virs_set_timing(self._h, int(enable)))
@@ -467,7 +482,7 @@ class Simulation:
         return int(lib().virs_check_bounded_wait(self._h, limit))
 
     def forward_checkpointed(self, steps: int, every: int = 64, stream: int | None = None):
-        check(lib().virs_forward_checkpointed(self._h, steps, every, stream))
+        check(lib().virs_forward_checkpointed(self._h, steps, every, _stream(stream)))
         self._adj_steps = steps
 
     def adjoint(self, dl_dir, n_materials: int, n_sections: int):
@@ -493,6 +508,15 @@ class Simulation:
     def set_tiling(self, rows: int = 0, planes: int = 0, depth: int = -1):
         check(lib().virs_set_tiling(self._h, rows, planes, depth))
 
+    def set_time_blocking(self, steps_per_pass: int = 2, rows: int = 0, planes: int = 0):
+        """Two steps per pass over the fields (bit-identical to single steps)."""
+        check(lib().virs_set_time_blocking(self._h, steps_per_pass, rows, planes))
+
+    def time_blocking(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        check(lib().virs_get_time_blocking(self._h, *[C.byref(x) for x in v]))
+        return {"steps_per_pass": v[0].value, "rows": v[1].value, "planes": v[2].value, "active": bool(v[3].value)}
+
 
 class Batch:
     """One virs_batch: many Simulations advanced together (3 launches per step)."""
@@ -504,7 +528,7 @@ class Batch:
         check(lib().virs_batch_create(arr, len(self.sims), C.byref(self._h)))
 
     def run(self, steps: int, stream: int | None = None):
-        check(lib().virs_batch_run(self._h, steps, stream))
+        check(lib().virs_batch_run(self._h, steps, _stream(stream)))
 
     def synchronize(self):
         check(lib().virs_batch_synchronize(self._h))

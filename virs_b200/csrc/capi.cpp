@@ -58,9 +58,34 @@ virs_status DevBuf::alloc(size_t n, const char *what)
                                     cudaGetErrorString(e));
     }
     bytes = n;
-    e = cudaMemset(ptr, 0, n);
+    e = cudaMemsetAsync(ptr, 0, n, cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
     return VIRS_OK;
+}
+
+// Every copy and memset of the library runs on the handle's own stream, a
+// non-blocking stream, and is complete when the call returns: nothing goes
+// to the legacy default stream, which would have to wait for (and would
+// break) a graph capture in progress on another handle's stream in another
+// host thread.
+cudaError_t copy_on(cudaStream_t st, void *dst, const void *src, size_t n, cudaMemcpyKind k)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, n, k, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+cudaError_t copy2d_on(cudaStream_t st, void *dst, size_t dpitch, const void *src, size_t spitch, size_t w, size_t h,
+                      cudaMemcpyKind k)
+{
+    cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, w, h, k, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+cudaError_t zero_on(cudaStream_t st, void *p, size_t n)
+{
+    cudaError_t e = cudaMemsetAsync(p, 0, n, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
 }
 
 } // namespace virs
@@ -140,6 +165,23 @@ struct virs_sim {
     DevBuf zmask;
     int zm_rows = 0, zm_zc = 0;
     DevBuf err;                    // device error flag of bounded waits
+
+    // two steps per pass (virs_set_time_blocking).  spare[k] is the partner
+    // of field[k] in a four-buffer rotation (four steps go field -> spare ->
+    // field); pmP / pmQ are the maps of field[0], field[1], spare[0],
+    // spare[1] (index 0..3) for pm_rows-row tiles, pmC the wider code box;
+    // plist holds the voxels whose second step is provisional (pl_ok: built
+    // for the current codes and sources)
+    int pair_steps = 1, pair_rows = 16, pair_zc = 0;
+    DevBuf spare[2];
+    CUtensorMap pmP[4], pmQ[4], pmC;
+    int pm_rows = 0;
+    DevBuf plist;
+    uint32_t nplist = 0;
+    bool pl_ok = false;
+    DevBuf pzmask;                 // zero-code masks of the two-step tiles (pm_rows x pzm_zc; -1 = none)
+    int pzm_zc = -1;
+    bool pair_nomem = false;       // the spare buffers did not fit: single steps
 
     // CUDA graphs for GRAPH_STEPS steps, one per parity of `cur`
     static constexpr int GRAPH_STEPS = 32;
@@ -224,7 +266,7 @@ virs_status upload_hard(virs_sim *s)
     std::vector<float> v(s->hard_host.size());
     for (size_t i = 0; i < v.size(); ++i) v[i] = s->hard_host[i] * s->scale;
     VIRS_TRY(s->hard.alloc(v.size() * sizeof(float), "hard source schedule"));
-    if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->hard.ptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (!v.empty()) VIRS_CUDA(copy_on(s->stream, s->hard.ptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
     s->nhard = (uint32_t)v.size();
     s->graph_dirty = true;
     ++s->gen;
@@ -240,7 +282,7 @@ virs_status default_filters(virs_sim *s)
     s->nmat = 1;
     s->nsec = 1;
     VIRS_TRY(s->coef.alloc(5 * sizeof(float), "filter coefficients"));
-    VIRS_CUDA(cudaMemcpy(s->coef.ptr, k, sizeof(k), cudaMemcpyHostToDevice));
+    VIRS_CUDA(copy_on(s->stream, s->coef.ptr, k, sizeof(k), cudaMemcpyHostToDevice));
     s->filters_set = true;
     return VIRS_OK;
 }
@@ -272,14 +314,14 @@ bool interior(const virs_sim *s, uint64_t ref)
 // layout (rows of px)
 virs_status h2d_rows(void *dst, const void *src, size_t elem, const virs_sim *s, size_t planes = 0)
 {
-    VIRS_CUDA(cudaMemcpy2D(dst, (size_t)s->px * elem, src, (size_t)s->nx * elem, (size_t)s->nx * elem,
+    VIRS_CUDA(copy2d_on(s->stream, dst, (size_t)s->px * elem, src, (size_t)s->nx * elem, (size_t)s->nx * elem,
                            (size_t)s->ny * (planes ? planes : s->nz), cudaMemcpyHostToDevice));
     return VIRS_OK;
 }
 
 virs_status d2h_rows(void *dst, const void *src, size_t elem, const virs_sim *s)
 {
-    VIRS_CUDA(cudaMemcpy2D(dst, (size_t)s->nx * elem, src, (size_t)s->px * elem, (size_t)s->nx * elem,
+    VIRS_CUDA(copy2d_on(s->stream, dst, (size_t)s->nx * elem, src, (size_t)s->px * elem, (size_t)s->nx * elem,
                            (size_t)s->ny * s->nz, cudaMemcpyDeviceToHost));
     return VIRS_OK;
 }
@@ -328,7 +370,8 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->segnz, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos})
+                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos,
+                      &s->spare[0], &s->spare[1], &s->plist, &s->pzmask})
         b->release();
     const size_t ext = (size_t)s->px * ny * s->ext_nz;
     VIRS_TRY(s->flags_raw.alloc(ext, "flags"));
@@ -343,6 +386,9 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->steps_done = 0;
     s->maps_rows = 0;
     s->zm_rows = s->zm_zc = 0;
+    s->pm_rows = 0;
+    s->pl_ok = false;
+    s->pair_nomem = false;
     // sources and receivers refer to voxel indices of the previous grid
     s->nsrc = s->nrcv = 0;
     s->src_ref.clear();
@@ -416,10 +462,10 @@ virs_status install_mesh(virs_sim *s, const Mesh &m, uint32_t part = 0, uint32_t
         VIRS_TRY(la.alloc(nvx * sizeof(uint32_t), "voxelisation marks"));
         VIRS_TRY(lw.alloc(nvx * sizeof(uint32_t), "voxelisation marks"));
         VIRS_TRY(mx.alloc(sizeof(uint32_t), "wall material maximum"));
-        VIRS_CUDA(cudaMemcpy(dv.ptr, m.verts.data(), dv.bytes, cudaMemcpyHostToDevice));
-        VIRS_CUDA(cudaMemcpy(dt.ptr, m.tris.data(), dt.bytes, cudaMemcpyHostToDevice));
-        VIRS_CUDA(cudaMemcpy(dm.ptr, m.tri_mat.data(), dm.bytes, cudaMemcpyHostToDevice));
-        if (!s->roles.empty()) VIRS_CUDA(cudaMemcpy(dr.ptr, s->roles.data(), s->roles.size(), cudaMemcpyHostToDevice));
+        VIRS_CUDA(copy_on(s->stream, dv.ptr, m.verts.data(), dv.bytes, cudaMemcpyHostToDevice));
+        VIRS_CUDA(copy_on(s->stream, dt.ptr, m.tris.data(), dt.bytes, cudaMemcpyHostToDevice));
+        VIRS_CUDA(copy_on(s->stream, dm.ptr, m.tri_mat.data(), dm.bytes, cudaMemcpyHostToDevice));
+        if (!s->roles.empty()) VIRS_CUDA(copy_on(s->stream, dr.ptr, s->roles.data(), s->roles.size(), cudaMemcpyHostToDevice));
         VIRS_CUDA(launch_voxelize(dv.as<float>(), dt.as<uint32_t>(), dm.as<int32_t>(), ntri, dr.as<uint8_t>(),
                                   (uint32_t)s->roles.size(), h, bmin, s->nx, s->ny, (uint32_t)d[2], (uint32_t)z_first,
                                   s->ext_nz, s->px, tri.ptr,
@@ -440,7 +486,7 @@ virs_status ensure_ir(virs_sim *s, uint64_t need)
     DevBuf nb;
     VIRS_TRY(nb.alloc(std::max<uint32_t>(s->nrcv, 1) * cap * sizeof(float), "receiver samples"));
     if (s->ircap && s->nrcv)
-        VIRS_CUDA(cudaMemcpy2D(nb.ptr, cap * sizeof(float), s->ir.ptr, s->ircap * sizeof(float),
+        VIRS_CUDA(copy2d_on(s->stream, nb.ptr, cap * sizeof(float), s->ir.ptr, s->ircap * sizeof(float),
                                s->ircap * sizeof(float), s->nrcv, cudaMemcpyDeviceToDevice));
     std::swap(s->ir.ptr, nb.ptr);
     std::swap(s->ir.bytes, nb.bytes);
@@ -511,9 +557,9 @@ virs_status check_err(virs_sim *s)
 {
     if (!s->err.ptr) return VIRS_OK;
     int e = 0;
-    VIRS_CUDA(cudaMemcpy(&e, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    VIRS_CUDA(copy_on(s->stream, &e, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
-        VIRS_CUDA(cudaMemset(s->err.ptr, 0, sizeof(int)));
+        VIRS_CUDA(zero_on(s->stream, s->err.ptr, sizeof(int)));
         return fail(VIRS_E_TIMEOUT, "a stencil block gave up waiting for its staged planes (bounded wait expired)");
     }
     return VIRS_OK;
@@ -643,6 +689,158 @@ cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
     return launch_post(s->prm.storage, post_args(s, parity), st);
 }
 
+// ---- two steps per pass -------------------------------------------------------
+
+// buffer k of the four-buffer rotation: field[0], field[1], spare[0], spare[1]
+void *buf_ptr(const virs_sim *s, int k) { return k < 2 ? s->field[k].ptr : s->spare[k - 2].ptr; }
+
+bool pair_on(const virs_sim *s)
+{
+    return s->pair_steps == 2 && !s->pair_nomem && s->depth > 0 && !s->stop_rule && s->nx >= 3 && s->ny >= 3 &&
+           s->nz >= 3;
+}
+
+// the voxels whose p^{n+2} the two-step kernel leaves provisional, for the
+// current codes, boundary list and sources (kernels_classify.cu)
+virs_status build_pair_list(virs_sim *s)
+{
+    cudaStream_t st = s->stream;
+    const size_t nseg = mark_segments(s->nvox);
+    DevBuf mark, cnt, tmp, total;
+    VIRS_TRY(mark.alloc(s->nvox, "provisional-voxel marks"));
+    VIRS_TRY(cnt.alloc(nseg * 4, "provisional-voxel counts"));
+    VIRS_TRY(tmp.alloc(scan_tmp_words(nseg) * 4, "scan scratch"));
+    VIRS_TRY(total.alloc(4, "provisional-voxel total"));
+    VIRS_CUDA(cudaMemsetAsync(mark.ptr, 0, s->nvox, st));
+    VIRS_CUDA(launch_pair_marks(s->code.as<uint8_t>(), s->px, s->ny, s->nz, s->bpos.as<uint32_t>(), s->nb,
+                                s->hpos.as<uint32_t>(), s->nhpos, s->src.as<uint64_t>(), s->nsrc, mark.as<uint8_t>(),
+                                cnt.as<uint32_t>(), st));
+    VIRS_CUDA(launch_scan(cnt.as<uint32_t>(), nseg, tmp.as<uint32_t>(), total.as<uint32_t>(), st));
+    uint32_t n = 0;
+    VIRS_CUDA(cudaMemcpyAsync(&n, total.ptr, 4, cudaMemcpyDeviceToHost, st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    VIRS_TRY(s->plist.alloc(std::max<uint32_t>(n, 1) * 4, "provisional-voxel list"));
+    if (n) VIRS_CUDA(launch_mark_list(mark.as<uint8_t>(), s->nvox, cnt.as<uint32_t>(), s->plist.as<uint32_t>(), st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    s->nplist = n;
+    s->pl_ok = true;
+    s->drop_graphs();
+    return VIRS_OK;
+}
+
+// spare buffers, maps and the provisional-voxel list; a grid whose spare
+// buffers do not fit in device memory runs single steps
+virs_status ready_pairs(virs_sim *s)
+{
+    const size_t fb = s->nvox * s->storage_bytes();
+    for (int k = 0; k < 2; ++k)
+        if (!s->spare[k].ptr && s->spare[k].alloc(fb, "pressure field (rotation)") != VIRS_OK) {
+            s->spare[0].release();
+            s->spare[1].release();
+            (void)cudaGetLastError();
+            s->pair_nomem = true;
+            s->drop_graphs();
+            return VIRS_OK;
+        }
+    if (s->pm_rows != s->pair_rows) {
+        const int rows = s->pair_rows;
+        const CUtensorMapDataType dt = s->prm.storage == VIRS_STORAGE_F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                       : s->prm.storage == VIRS_STORAGE_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                                            : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+        const size_t el = s->storage_bytes();
+        for (int b = 0; b < 4; ++b) {
+            VIRS_TRY(encode(&s->pmP[b], dt, el, buf_ptr(s, b), s, (uint32_t)tma_box_width(s->prm.storage), rows + 2));
+            VIRS_TRY(encode(&s->pmQ[b], dt, el, buf_ptr(s, b), s, (uint32_t)tma_tile_x(), rows));
+        }
+        VIRS_TRY(encode(&s->pmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->code.ptr, s, (uint32_t)pair_code_box(), rows));
+        if (!s->err.ptr) VIRS_TRY(s->err.alloc(sizeof(int), "error flag"));
+        s->pm_rows = rows;
+        s->pzm_zc = -1;
+        s->drop_graphs();
+    }
+    if (zero_masks_useful(s) && s->pzm_zc != s->pair_zc) {
+        const uint32_t ix = (uint32_t)pair_tile_x(s->prm.storage), v = (uint32_t)(16 / s->storage_bytes());
+        const uint32_t rows = (uint32_t)s->pair_rows, zc = s->pair_zc > 0 ? (uint32_t)s->pair_zc : s->nz - 2;
+        const uint32_t gx = (s->px + ix - 1) / ix, gy = (s->ny + rows - 3) / (rows - 2);
+        const uint32_t gz = (s->nz - 2 + zc - 1) / zc;
+        VIRS_TRY(s->pzmask.alloc((size_t)gx * gy * gz * 8, "two-step zero-code masks"));
+        VIRS_CUDA(launch_pair_zero_masks(s->segnz.as<uint8_t>(), s->px, s->ny, s->nz, s->spr, rows, zc, ix, v, gx, gy,
+                                         gz, s->pzmask.as<uint64_t>(), s->stream));
+        VIRS_CUDA(cudaStreamSynchronize(s->stream));
+        s->pzm_zc = s->pair_zc;
+        s->drop_graphs();
+    }
+    if (!s->pl_ok) VIRS_TRY(build_pair_list(s));
+    return VIRS_OK;
+}
+
+// The planes z = 0 and nz-1 keep their values (border codes) and no stencil
+// writes them: spare[k] takes those of field[k], its partner in the rotation.
+virs_status sync_border_planes(virs_sim *s, cudaStream_t st)
+{
+    const size_t pb = (size_t)s->px * s->ny * s->storage_bytes(), last = (size_t)(s->nz - 1) * pb;
+    for (int k = 0; k < 2; ++k) {
+        VIRS_CUDA(cudaMemcpyAsync(s->spare[k].ptr, s->field[k].ptr, pb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(s->spare[k].as<char>() + last, s->field[k].as<char>() + last, pb,
+                                  cudaMemcpyDeviceToDevice, st));
+    }
+    return VIRS_OK;
+}
+
+StepArgs step_args_bufs(const virs_sim *s, int p, int q)
+{
+    StepArgs a = step_args(s, 0);
+    a.p = buf_ptr(s, p);
+    a.q = buf_ptr(s, q);
+    a.tzmask = nullptr;
+    return a;
+}
+
+PostArgs post_args_buf(const virs_sim *s, int q)
+{
+    PostArgs a = post_args(s, 0);
+    a.q = buf_ptr(s, q);
+    return a;
+}
+
+// Two steps: p^n in buffer x, p^{n-1} in y; p^{n+1} to z, p^{n+2} to w.
+// After k_pair_tma the first step is completed (boundary pass, post kernel);
+// then one launch runs the second step's boundary pass and recomputes its
+// provisional voxels, and the second post kernel follows.
+cudaError_t enqueue_pair(const virs_sim *s, int x, int y, int z, int w, cudaStream_t st, cudaEvent_t *ev = nullptr)
+{
+    const int sto = s->prm.storage;
+    StepArgs a = step_args_bufs(s, x, y);
+    a.zc = s->pair_zc;
+    if (zero_masks_useful(s) && s->pzm_zc == s->pair_zc) a.tzmask = s->pzmask.as<uint64_t>();
+    const TmaMaps m{&s->pmP[x], &s->pmQ[y], &s->pmC};
+    if (ev) cudaEventRecord(ev[0], st);
+    cudaError_t e = launch_pair_tma(sto, s->pair_rows, a, m, buf_ptr(s, z), buf_ptr(s, w), s->err.as<int>(), st);
+    if (ev) cudaEventRecord(ev[1], st);
+    if (e == cudaSuccess) e = launch_boundary(sto, step_args_bufs(s, x, z), BND_UPDATE, st);
+    if (ev) cudaEventRecord(ev[2], st);
+    if (e == cudaSuccess) e = launch_post(sto, post_args_buf(s, z), st);
+    if (ev) cudaEventRecord(ev[3], st);
+    if (e == cudaSuccess)
+        e = launch_boundary_fix(sto, step_args_bufs(s, z, w), buf_ptr(s, x), s->plist.as<uint32_t>(), s->nplist, st);
+    if (ev) cudaEventRecord(ev[4], st);
+    if (e == cudaSuccess) e = launch_post(sto, post_args_buf(s, w), st);
+    return e;
+}
+
+// four steps from parity par, field -> spare -> field: the state is back in
+// field[par] (p^n) and field[par ^ 1] (p^{n-1}) afterwards
+cudaError_t enqueue_quad(const virs_sim *s, int par, cudaStream_t st, cudaEvent_t *ev = nullptr)
+{
+    cudaError_t e = enqueue_pair(s, par, par ^ 1, 2 + (par ^ 1), 2 + par, st, ev);
+    if (e == cudaSuccess) e = enqueue_pair(s, 2 + par, 2 + (par ^ 1), par ^ 1, par, st, ev ? ev + 5 : nullptr);
+    return e;
+}
+
+// kernels per pair: the two-step kernel, two post kernels, the first
+// boundary pass, and the second one together with the fix-up
+uint64_t pair_launches(const virs_sim *s) { return 3 + (s->nb ? 1 : 0) + (s->nb || s->nplist ? 1 : 0); }
+
 virs_status build_graphs(virs_sim *s, cudaStream_t st)
 {
     s->drop_graphs();
@@ -650,7 +848,10 @@ virs_status build_graphs(virs_sim *s, cudaStream_t st)
         cudaGraph_t g = nullptr;
         VIRS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
-        for (int i = 0; i < virs_sim::GRAPH_STEPS && e == cudaSuccess; ++i) e = enqueue_step(s, par ^ (i & 1), st);
+        if (pair_on(s))
+            for (int i = 0; i < virs_sim::GRAPH_STEPS / 4 && e == cudaSuccess; ++i) e = enqueue_quad(s, par, st);
+        else
+            for (int i = 0; i < virs_sim::GRAPH_STEPS && e == cudaSuccess; ++i) e = enqueue_step(s, par ^ (i & 1), st);
         cudaError_t e2 = cudaStreamEndCapture(st, &g);
         if (e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
@@ -671,46 +872,88 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
     if (!s->fields_valid) return fail(VIRS_E_STATE, "the fields were consumed by virs_adjoint: start the simulation again");
     VIRS_TRY(ready_to_run(s));
     VIRS_TRY(ensure_ir(s, s->steps_done + n));
+    // with two steps per pass, whole groups of four steps go through the
+    // spare buffers and back; the remaining n % 4 are single steps
+    uint64_t quads = 0;
+    if (pair_on(s) && n >= 4) {
+        VIRS_TRY(ready_pairs(s));
+        if (pair_on(s)) {
+            quads = n / 4;
+            VIRS_TRY(sync_border_planes(s, st));
+        }
+    }
+    const uint64_t n1 = n - 4 * quads; // single steps, after the quads (which keep the parity)
     if (s->timing) {
-        std::vector<cudaEvent_t> ev(2 * n);
-        for (auto &e : ev) VIRS_CUDA(cudaEventCreate(&e));
         cudaError_t err = cudaSuccess;
-        ev.resize(3 * n);
-        for (size_t k = 2 * n; k < ev.size(); ++k) VIRS_CUDA(cudaEventCreate(&ev[k]));
-        for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
-            const int par = s->cur ^ (int)(i & 1);
-            cudaEventRecord(ev[2 * i], st);
-            err = launch_stencil(s, par, st);
-            cudaEventRecord(ev[2 * i + 1], st);
-            if (err == cudaSuccess)
-                err = launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, st);
-            cudaEventRecord(ev[2 * n + i], st);
-            if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
+        if (quads) {
+            std::vector<cudaEvent_t> ev(10 * quads);
+            for (auto &e : ev) VIRS_CUDA(cudaEventCreate(&e));
+            for (uint64_t q = 0; q < quads && err == cudaSuccess; ++q) err = enqueue_quad(s, s->cur, st, &ev[10 * q]);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            double ms = 0, bms = 0;
+            for (uint64_t p = 0; p < 2 * quads && err == cudaSuccess; ++p) {
+                float t = 0, b1 = 0, b2 = 0;
+                err = cudaEventElapsedTime(&t, ev[5 * p], ev[5 * p + 1]);
+                if (err == cudaSuccess) err = cudaEventElapsedTime(&b1, ev[5 * p + 1], ev[5 * p + 2]);
+                if (err == cudaSuccess) err = cudaEventElapsedTime(&b2, ev[5 * p + 3], ev[5 * p + 4]);
+                ms += t;
+                bms += (double)b1 + b2;
+            }
+            for (auto &e : ev) cudaEventDestroy(e);
+            if (err != cudaSuccess) return cuda_fail(err, "timed two-step loop");
+            s->t_ms += ms;
+            s->t_bms += bms;
+            s->t_steps += 2 * quads;
+            s->t_launch += 2 * quads * pair_launches(s);
         }
-        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
-        double ms = 0, bms = 0;
-        for (uint64_t i = 0; i < n && err == cudaSuccess; ++i) {
-            float t = 0, tb = 0;
-            err = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
-            if (err == cudaSuccess) err = cudaEventElapsedTime(&tb, ev[2 * i + 1], ev[2 * n + i]);
-            ms += t;
-            bms += tb;
+        if (n1) {
+            std::vector<cudaEvent_t> ev(3 * n1);
+            for (auto &e : ev) VIRS_CUDA(cudaEventCreate(&e));
+            for (uint64_t i = 0; i < n1 && err == cudaSuccess; ++i) {
+                const int par = s->cur ^ (int)(i & 1);
+                cudaEventRecord(ev[2 * i], st);
+                err = launch_stencil(s, par, st);
+                cudaEventRecord(ev[2 * i + 1], st);
+                if (err == cudaSuccess) err = launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, st);
+                cudaEventRecord(ev[2 * n1 + i], st);
+                if (err == cudaSuccess) err = launch_post(s->prm.storage, post_args(s, par), st);
+            }
+            if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            double ms = 0, bms = 0;
+            for (uint64_t i = 0; i < n1 && err == cudaSuccess; ++i) {
+                float t = 0, tb = 0;
+                err = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+                if (err == cudaSuccess) err = cudaEventElapsedTime(&tb, ev[2 * i + 1], ev[2 * n1 + i]);
+                ms += t;
+                bms += tb;
+            }
+            for (auto &e : ev) cudaEventDestroy(e);
+            if (err != cudaSuccess) return cuda_fail(err, "timed step loop");
+            s->t_ms += ms;
+            s->t_bms += bms;
+            s->t_steps += n1;
+            s->t_launch += (s->nb ? 3 : 2) * n1;
         }
-        s->t_bms += bms;
-        for (auto &e : ev) cudaEventDestroy(e);
-        if (err != cudaSuccess) return cuda_fail(err, "timed step loop");
-        s->t_ms += ms;
-        s->t_steps += n;
-        s->t_launch += (s->nb ? 3 : 2) * n;
     } else {
         uint64_t i = 0;
-        if (n >= (uint64_t)virs_sim::GRAPH_STEPS) {
+        if (quads) {
+            constexpr uint64_t GQ = virs_sim::GRAPH_STEPS / 4;
+            uint64_t q = 0;
+            if (quads >= GQ) {
+                if (s->graph_dirty) VIRS_TRY(build_graphs(s, st));
+                for (; q + GQ <= quads; q += GQ) VIRS_CUDA(cudaGraphLaunch(s->graph[s->cur], st));
+            }
+            for (; q < quads; ++q) {
+                cudaError_t e = enqueue_quad(s, s->cur, st);
+                if (e != cudaSuccess) return cuda_fail(e, "two-step launch");
+            }
+        } else if (n >= (uint64_t)virs_sim::GRAPH_STEPS) {
             if (s->graph_dirty) VIRS_TRY(build_graphs(s, st));
             for (; i + virs_sim::GRAPH_STEPS <= n; i += virs_sim::GRAPH_STEPS)
                 VIRS_CUDA(cudaGraphLaunch(s->graph[s->cur ^ (int)(i & 1)], st));
         }
-        for (; i < n; ++i) {
-            cudaError_t e = enqueue_step(s, s->cur ^ (int)(i & 1), st);
+        for (uint64_t k = 0; k < n1 - i; ++k) {
+            cudaError_t e = enqueue_step(s, s->cur ^ (int)((i + k) & 1), st);
             if (e != cudaSuccess) return cuda_fail(e, "step launch");
         }
     }
@@ -795,7 +1038,7 @@ VIRS_EXPORT virs_status virs_create(const virs_params *p, virs_sim **out)
     VIRS_TRY(use_device(s.get()));
     // a blocking stream: it orders after the synchronous copies and memsets
     // of the setup calls, which run on the legacy default stream
-    VIRS_CUDA(cudaStreamCreate(&s->stream));
+    VIRS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     VIRS_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
     VIRS_CUDA(cudaEventRecord(s->done, s->stream));
     s->roles.assign(2, VIRS_ROLE_IGNORE);
@@ -1047,7 +1290,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         std::vector<float> wt((size_t)W * W + 1);
         for (int d = 0; d <= W * W; ++d) wt[d] = sponge_weight(W, d);
         VIRS_TRY(wtab.alloc(wt.size() * 4, "sponge weights"));
-        VIRS_CUDA(cudaMemcpy(wtab.ptr, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice));
+        VIRS_CUDA(copy_on(s->stream, wtab.ptr, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice));
         VIRS_TRY(s->bidx.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary indices"));
         VIRS_TRY(s->bpos.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary positions"));
         VIRS_TRY(s->bmat.alloc(std::max<uint64_t>(nb, 1), "boundary materials"));
@@ -1081,6 +1324,9 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
     if (s->filters_set) VIRS_TRY(alloc_states(s));
     s->maps_rows = 0;
     s->zm_rows = s->zm_zc = 0;
+    s->pm_rows = 0;
+    s->pzm_zc = -1;
+    s->pl_ok = false;
     s->classified = true;
     VIRS_CUDA(cudaEventRecord(s->done, st));
     return VIRS_OK;
@@ -1125,7 +1371,7 @@ VIRS_EXPORT virs_status virs_get_boundary_indices(const virs_sim *s, uint32_t *o
     if (n < s->nb) return fail(VIRS_E_ARG, "virs_get_boundary_indices: buffer smaller than the boundary count");
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
-    if (s->nb) VIRS_CUDA(cudaMemcpy(out, s->bidx.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
+    if (s->nb) VIRS_CUDA(copy_on(s->stream, out, s->bidx.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
     return VIRS_OK;
 }
 
@@ -1136,8 +1382,8 @@ VIRS_EXPORT virs_status virs_get_boundary_materials(const virs_sim *s, uint8_t *
     if (n < s->nb) return fail(VIRS_E_ARG, "virs_get_boundary_materials: buffer smaller than the boundary count");
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
-    if (s->nb && mat) VIRS_CUDA(cudaMemcpy(mat, s->bmat.ptr, s->nb, cudaMemcpyDeviceToHost));
-    if (s->nb && w) VIRS_CUDA(cudaMemcpy(w, s->bw.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
+    if (s->nb && mat) VIRS_CUDA(copy_on(s->stream, mat, s->bmat.ptr, s->nb, cudaMemcpyDeviceToHost));
+    if (s->nb && w) VIRS_CUDA(copy_on(s->stream, w, s->bw.ptr, s->nb * 4, cudaMemcpyDeviceToHost));
     return VIRS_OK;
 }
 
@@ -1150,7 +1396,7 @@ VIRS_EXPORT virs_status virs_set_filters(virs_sim *s, uint32_t nm, uint32_t ns, 
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     VIRS_TRY(s->coef.alloc((size_t)nm * ns * 5 * 4, "filter coefficients"));
-    VIRS_CUDA(cudaMemcpy(s->coef.ptr, coeffs, (size_t)nm * ns * 5 * 4, cudaMemcpyHostToDevice));
+    VIRS_CUDA(copy_on(s->stream, s->coef.ptr, coeffs, (size_t)nm * ns * 5 * 4, cudaMemcpyHostToDevice));
     s->nmat = nm;
     s->nsec = ns;
     s->filters_set = true;
@@ -1287,11 +1533,12 @@ VIRS_EXPORT virs_status virs_set_sources(virs_sim *s, uint32_t n, const uint64_t
     s->sig_host.assign(sig, sig + (size_t)n * len);
     s->sig_peak = peak;
     VIRS_TRY(s->src.alloc(std::max<uint32_t>(n, 1) * 8, "source indices"));
-    if (n) VIRS_CUDA(cudaMemcpy(s->src.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
+    if (n) VIRS_CUDA(copy_on(s->stream, s->src.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
     s->nsrc = n;
     s->siglen = len;
     s->src_ref.assign(idx, idx + n);
     s->sig.release();
+    s->pl_ok = false;
     s->graph_dirty = true;
     ++s->gen;
     return VIRS_OK;
@@ -1309,7 +1556,7 @@ VIRS_EXPORT virs_status virs_set_receivers(virs_sim *s, uint32_t n, const uint64
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     VIRS_TRY(s->rcv.alloc(std::max<uint32_t>(n, 1) * 8, "receiver indices"));
-    if (n) VIRS_CUDA(cudaMemcpy(s->rcv.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
+    if (n) VIRS_CUDA(copy_on(s->stream, s->rcv.ptr, dev.data(), n * 8, cudaMemcpyHostToDevice));
     s->nrcv = n;
     s->rcv_ref.assign(idx, idx + n);
     s->ir.release();
@@ -1325,7 +1572,7 @@ virs_status upload_signals(virs_sim *s)
     std::vector<float> v(s->sig_host.size());
     for (size_t i = 0; i < v.size(); ++i) v[i] = s->sig_host[i] * s->scale;
     VIRS_TRY(s->sig.alloc(std::max<size_t>(v.size(), 1) * 4, "source signals"));
-    if (!v.empty()) VIRS_CUDA(cudaMemcpy(s->sig.ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+    if (!v.empty()) VIRS_CUDA(copy_on(s->stream, s->sig.ptr, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
     s->graph_dirty = true;
     ++s->gen;
     return VIRS_OK;
@@ -1344,11 +1591,11 @@ VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
     s->ir.release();
     s->ircap = 0;
     VIRS_TRY(ensure_ir(s, std::max<uint64_t>(steps, 1)));
-    VIRS_CUDA(cudaMemset(s->field[0].ptr, 0, s->field[0].bytes));
-    VIRS_CUDA(cudaMemset(s->field[1].ptr, 0, s->field[1].bytes));
-    VIRS_CUDA(cudaMemset(s->state.ptr, 0, s->state.bytes));
-    VIRS_CUDA(cudaMemset(s->ctr.ptr, 0, 4));
-    if (s->stopbuf.ptr) VIRS_CUDA(cudaMemset(s->stopbuf.ptr, 0, s->stopbuf.bytes));
+    VIRS_CUDA(zero_on(s->stream, s->field[0].ptr, s->field[0].bytes));
+    VIRS_CUDA(zero_on(s->stream, s->field[1].ptr, s->field[1].bytes));
+    VIRS_CUDA(zero_on(s->stream, s->state.ptr, s->state.bytes));
+    VIRS_CUDA(zero_on(s->stream, s->ctr.ptr, 4));
+    if (s->stopbuf.ptr) VIRS_CUDA(zero_on(s->stream, s->stopbuf.ptr, s->stopbuf.bytes));
     s->stopped = false;
     s->cur = 0;
     s->steps_done = 0;
@@ -1356,7 +1603,7 @@ VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
     s->rms_state = 0.f;
     s->fields_valid = true;
     s->drop_graphs();
-    VIRS_CUDA(cudaDeviceSynchronize());
+    VIRS_CUDA(cudaStreamSynchronize(s->stream));
     VIRS_CUDA(cudaEventRecord(s->done, s->stream));
     return VIRS_OK;
 }
@@ -1471,7 +1718,7 @@ VIRS_EXPORT virs_status virs_set_stop_rule(virs_sim *s, int enable)
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     if (enable && !s->stopbuf.ptr) VIRS_TRY(s->stopbuf.alloc(4 * sizeof(uint32_t), "stop rule state"));
-    if (s->stopbuf.ptr) VIRS_CUDA(cudaMemset(s->stopbuf.ptr, 0, s->stopbuf.bytes));
+    if (s->stopbuf.ptr) VIRS_CUDA(zero_on(s->stream, s->stopbuf.ptr, s->stopbuf.bytes));
     s->stop_rule = enable != 0;
     s->stopped = false;
     s->drop_graphs();
@@ -1495,7 +1742,7 @@ VIRS_EXPORT virs_status virs_get_ir(const virs_sim *s, uint64_t first, uint64_t 
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     VIRS_TRY(check_err(const_cast<virs_sim *>(s)));
-    VIRS_CUDA(cudaMemcpy2D(out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
+    VIRS_CUDA(copy2d_on(s->stream, out, steps * 4, s->ir.as<float>() + first, s->ircap * 4, steps * 4, s->nrcv,
                            cudaMemcpyDeviceToHost));
     return VIRS_OK;
 }
@@ -1573,7 +1820,7 @@ VIRS_EXPORT virs_status virs_set_pressure(virs_sim *s, const float *cur, const f
     for (int k = 0; k < 2; ++k) {
         DevBuf &f = s->field[s->cur ^ k];
         if (!ins[k]) {
-            VIRS_CUDA(cudaMemset(f.ptr, 0, f.bytes));
+            VIRS_CUDA(zero_on(s->stream, f.ptr, f.bytes));
             continue;
         }
         if (s->prm.storage == VIRS_STORAGE_F32) {
@@ -1581,7 +1828,7 @@ VIRS_EXPORT virs_status virs_set_pressure(virs_sim *s, const float *cur, const f
         } else {
             DevBuf tmp;
             VIRS_TRY(tmp.alloc(s->nref * 4, "pressure import"));
-            VIRS_CUDA(cudaMemcpy(tmp.ptr, ins[k], s->nref * 4, cudaMemcpyHostToDevice));
+            VIRS_CUDA(copy_on(s->stream, tmp.ptr, ins[k], s->nref * 4, cudaMemcpyHostToDevice));
             VIRS_CUDA(launch_unpack(s->prm.storage, tmp.as<float>(), f.ptr, s->nx, s->ny, s->nz, s->px, s->scale,
                                     s->stream));
             VIRS_CUDA(cudaStreamSynchronize(s->stream));
@@ -1662,6 +1909,42 @@ VIRS_EXPORT virs_status virs_set_tiling(virs_sim *s, int rows, int planes, int d
     return VIRS_OK;
 }
 
+VIRS_EXPORT virs_status virs_set_time_blocking(virs_sim *s, int steps_per_pass, int tile_rows, int planes)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_set_time_blocking: null");
+    if (steps_per_pass != 1 && steps_per_pass != 2) return fail(VIRS_E_ARG, "steps per pass must be 1 or 2");
+    if (tile_rows != 0 && tile_rows != 16 && tile_rows != 32)
+        return fail(VIRS_E_ARG, "two-step tile rows must be 16 or 32");
+    if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
+    VIRS_TRY(wait_done(s));
+    s->pair_steps = steps_per_pass;
+    s->pair_rows = tile_rows ? tile_rows : 16;
+    s->pair_zc = planes;
+    s->pm_rows = 0;
+    s->pair_nomem = false;
+    if (steps_per_pass == 1) {
+        s->spare[0].release();
+        s->spare[1].release();
+        s->plist.release();
+        s->nplist = 0;
+        s->pl_ok = false;
+    }
+    s->drop_graphs();
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_get_time_blocking(const virs_sim *s, int *steps_per_pass, int *tile_rows, int *planes,
+                                               int *active)
+{
+    if (!s || !steps_per_pass || !tile_rows || !planes || !active)
+        return fail(VIRS_E_ARG, "virs_get_time_blocking: null argument");
+    *steps_per_pass = s->pair_steps;
+    *tile_rows = s->pair_rows;
+    *planes = s->pair_zc;
+    *active = pair_on(s) ? 1 : 0;
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_check_bounded_wait(virs_sim *s, uint32_t limit)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_check_bounded_wait: null");
@@ -1685,8 +1968,13 @@ struct TuneKey {
         return std::tie(dev, storage, nx, ny, nz) < std::tie(o.dev, o.storage, o.nx, o.ny, o.nz);
     }
 };
+// the single-step tiling, and the two-step settings when those won
+struct TunePick {
+    virs_tiling t{};
+    int pair_steps = 1, pair_rows = 16, pair_zc = 0;
+};
 std::mutex g_tune_mu;
-std::map<TuneKey, virs_tiling> g_tune;
+std::map<TuneKey, TunePick> g_tune;
 
 virs_status reset_state(virs_sim *s)
 {
@@ -1716,7 +2004,7 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     const TuneKey key{s->prm.device, s->prm.storage, s->nx, s->ny, s->nz};
-    virs_tiling pick{};
+    TunePick pick{};
     bool cached = false;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
@@ -1727,7 +2015,9 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
         }
     }
     if (!cached) {
-        VIRS_TRY(ensure_ir(s, 2ull * trial_steps + 2));
+        const uint32_t quads = (trial_steps + 3) / 4;
+        VIRS_TRY(ensure_ir(s, std::max<uint64_t>(2ull * trial_steps, 4ull * quads + 4) + 2));
+        s->pair_steps = 1;
         cudaEvent_t e0, e1;
         VIRS_CUDA(cudaEventCreate(&e0));
         VIRS_CUDA(cudaEventCreate(&e1));
@@ -1760,27 +2050,76 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
                         break;
                     }
                     if ((st = check_err(s)) != VIRS_OK) break;
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        pick = {r, pl, d, ms / trial_steps};
+                    if (ms / trial_steps < best_ms) {
+                        best_ms = ms / trial_steps;
+                        pick.t = {r, pl, d, ms / trial_steps};
                     }
                     if ((st = reset_state(s)) != VIRS_OK) break;
                 }
+        // two steps per pass (groups of four steps), with the best single-step
+        // tiling for the steps that do not fill a group
+        if (st == VIRS_OK) {
+            s->tile_rows = pick.t.tile_rows;
+            s->depth = pick.t.pipeline_depth;
+            s->zc = pick.t.planes_per_block;
+            s->maps_rows = 0;
+            const int prow_c[] = {16, 32}, pplanes_c[] = {32, 51, 64, 102, 128};
+            for (int r : prow_c)
+                for (int pl : pplanes_c) {
+                    if (st != VIRS_OK) break;
+                    s->pair_steps = 2;
+                    s->pair_rows = r;
+                    s->pair_zc = pl;
+                    s->pm_rows = 0;
+                    if ((st = ready_to_run(s)) != VIRS_OK || (st = ready_pairs(s)) != VIRS_OK) break;
+                    if (!pair_on(s)) break; // no room for the spare buffers, or a grid too small
+                    if ((st = sync_border_planes(s, s->stream)) != VIRS_OK) break;
+                    cudaError_t e = enqueue_quad(s, s->cur, s->stream);
+                    cudaEventRecord(e0, s->stream);
+                    for (uint32_t k = 0; k < quads && e == cudaSuccess; ++k) e = enqueue_quad(s, s->cur, s->stream);
+                    cudaEventRecord(e1, s->stream);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float ms = 0;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                    if (e != cudaSuccess) {
+                        st = cuda_fail(e, "autotune trial (two steps per pass)");
+                        break;
+                    }
+                    if ((st = check_err(s)) != VIRS_OK) break;
+                    const float per = ms / (4.f * quads);
+                    if (per < best_ms) {
+                        best_ms = per;
+                        pick.t.ms_per_step = per;
+                        pick.pair_steps = 2;
+                        pick.pair_rows = r;
+                        pick.pair_zc = pl;
+                    }
+                    if ((st = reset_state(s)) != VIRS_OK) break;
+                }
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (st != VIRS_OK) return st;
         std::lock_guard<std::mutex> g(g_tune_mu);
         g_tune[key] = pick;
     }
-    s->tile_rows = pick.tile_rows;
-    s->zc = pick.planes_per_block;
-    s->depth = pick.pipeline_depth;
+    s->tile_rows = pick.t.tile_rows;
+    s->zc = pick.t.planes_per_block;
+    s->depth = pick.t.pipeline_depth;
     s->maps_rows = 0;
+    s->pair_steps = pick.pair_steps;
+    s->pair_rows = pick.pair_rows;
+    s->pair_zc = pick.pair_zc;
+    s->pm_rows = 0;
+    if (pick.pair_steps == 1) {
+        s->spare[0].release();
+        s->spare[1].release();
+    }
     s->drop_graphs();
     VIRS_TRY(ready_to_run(s));
     VIRS_TRY(reset_state(s));
     VIRS_CUDA(cudaEventRecord(s->done, s->stream));
-    if (best) *best = pick;
+    if (best) *best = pick.t;
     return VIRS_OK;
 }
 
@@ -1921,7 +2260,7 @@ virs_status batch_build(virs_batch *b)
         b->gen[i] = s->gen;
     }
     VIRS_TRY(b->desc.alloc(h.size() * sizeof(BatchMember), "batch descriptors"));
-    VIRS_CUDA(cudaMemcpy(b->desc.ptr, h.data(), h.size() * sizeof(BatchMember), cudaMemcpyHostToDevice));
+    VIRS_CUDA(copy_on(b->stream, b->desc.ptr, h.data(), h.size() * sizeof(BatchMember), cudaMemcpyHostToDevice));
     b->ntiles = tiles;
     b->nbnd = bnd;
     return VIRS_OK;
@@ -2013,7 +2352,7 @@ VIRS_EXPORT virs_status virs_batch_create(virs_sim *const *sims, uint32_t n, vir
     b->storage = sims[0]->prm.storage;
     VIRS_TRY(use_device(sims[0]));
     for (virs_sim *s : b->mem) VIRS_TRY(wait_done(s));
-    VIRS_CUDA(cudaStreamCreate(&b->stream));
+    VIRS_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     VIRS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
     VIRS_TRY(b->err.alloc(sizeof(int), "batch error flag"));
     VIRS_TRY(batch_build(b.get()));
@@ -2048,9 +2387,9 @@ VIRS_EXPORT virs_status virs_batch_synchronize(virs_batch *b)
     VIRS_CUDA(cudaSetDevice(b->dev));
     VIRS_CUDA(cudaEventSynchronize(b->done));
     int e = 0;
-    VIRS_CUDA(cudaMemcpy(&e, b->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    VIRS_CUDA(copy_on(b->stream, &e, b->err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
-        VIRS_CUDA(cudaMemset(b->err.ptr, 0, sizeof(int)));
+        VIRS_CUDA(zero_on(b->stream, b->err.ptr, sizeof(int)));
         return fail(VIRS_E_TIMEOUT, "a batched stencil block gave up waiting for its staged planes");
     }
     return VIRS_OK;
@@ -2189,7 +2528,7 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
     VIRS_TRY(A.grad.alloc(ncoef * sizeof(double), "coefficient gradients"));
     VIRS_TRY(A.dl.alloc(std::max<uint32_t>(s->nrcv, 1) * steps * 4, "loss gradient"));
     VIRS_TRY(A.gsig.alloc(std::max<uint32_t>(s->nsrc, 1) * steps * 4, "signal gradients"));
-    if (s->nrcv) VIRS_CUDA(cudaMemcpy(A.dl.ptr, dl_dir, (size_t)s->nrcv * steps * 4, cudaMemcpyHostToDevice));
+    if (s->nrcv) VIRS_CUDA(copy_on(s->stream, A.dl.ptr, dl_dir, (size_t)s->nrcv * steps * 4, cudaMemcpyHostToDevice));
     const CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     for (int k = 0; k < 2; ++k) {
         VIRS_TRY(encode(&A.mapP[k], dt, 4, A.buf[k].ptr, s, (uint32_t)tma_box_width(VIRS_STORAGE_F32), s->tile_rows + 2));
@@ -2253,9 +2592,9 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
     }
     VIRS_CUDA(cudaStreamSynchronize(st));
     VIRS_TRY(check_err(s));
-    if (grad_coef) VIRS_CUDA(cudaMemcpy(grad_coef, A.grad.ptr, ncoef * sizeof(double), cudaMemcpyDeviceToHost));
+    if (grad_coef) VIRS_CUDA(copy_on(s->stream, grad_coef, A.grad.ptr, ncoef * sizeof(double), cudaMemcpyDeviceToHost));
     if (grad_signal && s->nsrc)
-        VIRS_CUDA(cudaMemcpy(grad_signal, A.gsig.ptr, (size_t)s->nsrc * steps * 4, cudaMemcpyDeviceToHost));
+        VIRS_CUDA(copy_on(s->stream, grad_signal, A.gsig.ptr, (size_t)s->nsrc * steps * 4, cudaMemcpyDeviceToHost));
     // the fields now hold an intermediate forward state
     s->fields_valid = false;
     VIRS_CUDA(cudaEventRecord(s->done, st));

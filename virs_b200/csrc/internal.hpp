@@ -150,6 +150,31 @@ cudaError_t launch_step_tma(int storage, int tile_rows, int depth, const StepArg
 int tma_box_width(int storage);   // x extent of the halo box (elements)
 int tma_pad(int storage);         // x halo on each side (elements)
 int tma_tile_x();                 // x extent of a tile
+// two steps in one pass (kernels_step_tma.cu): p^n (a.p, maps m.p) and
+// p^{n-1} (a.q, maps m.q) in, p^{n+1} to zout and p^{n+2} to wout; tiles of
+// tile_rows (16 or 32) rows, a.zc planes (0: all); then, after the first
+// boundary pass and post kernel, launch_boundary_fix (kernels_step.cu) runs
+// the second boundary pass (a.p = p^{n+1}, a.q = p^{n+2}) together with the
+// recomputation of the p^{n+2} of the voxels in list from p^{n+1} and p^n
+cudaError_t launch_pair_tma(int storage, int tile_rows, const StepArgs &a, const TmaMaps &m, void *zout, void *wout,
+                            int *err, cudaStream_t s);
+cudaError_t launch_boundary_fix(int storage, const StepArgs &a, const void *pn, const uint32_t *list, uint32_t nlist,
+                                cudaStream_t s);
+int pair_tile_x(int storage);   // inner tile width of the two-step kernel
+int pair_code_box();            // width of its code box (bytes)
+// the voxels whose p^{n+2} the two-step kernel leaves provisional
+// (kernels_classify.cu): marks (zeroed by the caller) and per-segment counts
+// of 1024 voxels, then, with the counts scanned, their ascending positions
+// per tile of the two-step kernel (inner width ix, vector width v), the
+// stages whose codes are all zero (kernels_classify.cu)
+cudaError_t launch_pair_zero_masks(const uint8_t *segnz, uint32_t px, uint32_t ny, uint32_t nz, uint32_t spr,
+                                   uint32_t rows, uint32_t zc, uint32_t ix, uint32_t v, uint32_t gx, uint32_t gy,
+                                   uint32_t gz, uint64_t *mask, cudaStream_t s);
+size_t mark_segments(uint64_t nvox);
+cudaError_t launch_pair_marks(const uint8_t *code, uint32_t px, uint32_t ny, uint32_t nz, const uint32_t *bpos,
+                              uint64_t nb, const uint32_t *hpos, uint32_t nh, const uint64_t *src, uint32_t nsrc,
+                              uint8_t *mark, uint32_t *cnt, cudaStream_t s);
+cudaError_t launch_mark_list(const uint8_t *mark, uint64_t nvox, const uint32_t *off, uint32_t *list, cudaStream_t s);
 cudaError_t launch_wait_probe(int *err, uint32_t limit, cudaStream_t s);
 
 // classification launchers (kernels_classify.cu)

@@ -16,6 +16,8 @@
 // first voxel in the reference's scan order (dz, then dy, then dx
 // ascending); the offsets of the winner locate the nearest wall voxel, whose
 // material becomes the boundary voxel's material.  W <= 31.
+#include <algorithm>
+
 #include "internal.hpp"
 
 namespace virs {
@@ -355,6 +357,126 @@ cudaError_t launch_tile_zero_masks(const uint8_t *segnz, uint32_t ny, uint32_t n
     const uint64_t ntiles = (uint64_t)gx * gy * gz;
     if (ntiles == 0) return cudaSuccess;
     k_tile_zero_mask<<<(unsigned)ntiles, 64, 0, s>>>(segnz, ny, nz, spr, rows, zc, gx, gy, mask);
+    return cudaGetLastError();
+}
+
+// The same masks for the tiles of the two-step kernel: a tile covers x in
+// [bx*ix - v, bx*ix - v + 128) and rows [by*iy - 1, by*iy - 1 + rows) (the
+// parts outside the grid read as code 0), and stage j holds plane
+// zs - 2 + j with zs = 1 + bz*zc; the stages with codes are the planes
+// zs-1 .. z1.  A bit is set when every 128-voxel segment the tile's codes
+// touch on that plane holds only zeros.
+namespace {
+__global__ void __launch_bounds__(64) k_pair_zero_mask(const uint8_t *__restrict segnz, uint32_t px, uint32_t ny,
+                                                       uint32_t nz, uint32_t spr, uint32_t rows, uint32_t zc,
+                                                       uint32_t ix, uint32_t v, uint32_t gx, uint32_t gy,
+                                                       uint64_t *__restrict mask)
+{
+    __shared__ unsigned w[2];
+    const uint32_t t = blockIdx.x, j = threadIdx.x;
+    const uint32_t bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
+    const int zs = 1 + (int)(bz * zc), z1 = min(zs + (int)zc, (int)nz - 1);
+    const int k = zs - 2 + (int)j;
+    bool zero = false;
+    if (k >= zs - 1 && k <= z1 && k >= 0 && k < (int)nz) {
+        zero = true;
+        const int xs = (int)(bx * ix) - (int)v, ys = (int)(by * (rows - 2)) - 1;
+        const int xa = max(xs, 0), xb = min(xs + 128, (int)px);
+        const int ya = max(ys, 0), yb = min(ys + (int)rows, (int)ny);
+        for (int y = ya; y < yb && zero; ++y)
+            for (int sx = xa / 128; sx <= (xb - 1) / 128 && zero; ++sx)
+                zero = segnz[((size_t)k * ny + y) * spr + sx] == 0;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, zero);
+    if ((j & 31) == 0) w[j >> 5] = b;
+    __syncthreads();
+    if (j == 0) mask[t] = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+}
+} // namespace
+
+cudaError_t launch_pair_zero_masks(const uint8_t *segnz, uint32_t px, uint32_t ny, uint32_t nz, uint32_t spr,
+                                   uint32_t rows, uint32_t zc, uint32_t ix, uint32_t v, uint32_t gx, uint32_t gy,
+                                   uint32_t gz, uint64_t *mask, cudaStream_t s)
+{
+    const uint64_t ntiles = (uint64_t)gx * gy * gz;
+    if (ntiles == 0) return cudaSuccess;
+    k_pair_zero_mask<<<(unsigned)ntiles, 64, 0, s>>>(segnz, px, ny, nz, spr, rows, zc, ix, v, gx, gy, mask);
+    return cudaGetLastError();
+}
+
+// ---- voxels whose second step of a two-step pass is provisional --------------
+//
+// The two-step stencil computes p^{n+2} from p^{n+1} before the boundary
+// pass and the post kernel have changed p^{n+1} at boundary voxels and
+// sources.  The p^{n+2} of every voxel the stencil updates (air or mirror
+// code: bit 7 clear) that is such a voxel or its face neighbour must be
+// recomputed afterwards.  k_pair_mark marks them, k_mark_count counts the
+// marks of each 1024-voxel segment, and after an exclusive scan of the
+// counts k_mark_list writes their positions in ascending order.
+namespace {
+constexpr int MARK_B = 1024;
+
+__device__ __forceinline__ void mark_around(const uint8_t *__restrict code, uint8_t *mark, uint64_t v, uint32_t px,
+                                            uint32_t ny, uint32_t nz)
+{
+    const uint64_t plane = (uint64_t)px * ny;
+    const uint32_t x = (uint32_t)(v % px), y = (uint32_t)((v / px) % ny), z = (uint32_t)(v / plane);
+    if (z >= nz) return;
+    const uint64_t nbv[7] = {v, v + 1, v - 1, v + px, v - px, v + plane, v - plane};
+    const bool in[7] = {true, x + 1 < px, x > 0, y + 1 < ny, y > 0, z + 1 < nz, z > 0};
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        if (in[k] && (code[nbv[k]] & CODE_BND) == 0) mark[nbv[k]] = 1;
+}
+
+__global__ void k_pair_mark(const uint8_t *__restrict code, uint32_t px, uint32_t ny, uint32_t nz,
+                            const uint32_t *__restrict bpos, uint64_t nb, const uint32_t *__restrict hpos, uint32_t nh,
+                            const uint64_t *__restrict src, uint32_t nsrc, uint8_t *mark)
+{
+    const uint64_t n = nb + nh + nsrc;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = i < nb ? (uint64_t)bpos[i] : i < nb + nh ? (uint64_t)hpos[i - nb] : src[i - nb - nh];
+        mark_around(code, mark, v, px, ny, nz);
+    }
+}
+
+__global__ void __launch_bounds__(MARK_B) k_mark_count(const uint8_t *__restrict mark, uint64_t n, uint32_t *cnt)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * MARK_B + threadIdx.x;
+    const int c = __syncthreads_count(i < n && mark[i] != 0);
+    if (threadIdx.x == 0) cnt[blockIdx.x] = (uint32_t)c;
+}
+
+__global__ void __launch_bounds__(MARK_B) k_mark_list(const uint8_t *__restrict mark, uint64_t n,
+                                                      const uint32_t *__restrict off, uint32_t *list)
+{
+    __shared__ uint32_t tot;
+    const uint64_t i = (uint64_t)blockIdx.x * MARK_B + threadIdx.x;
+    const uint32_t f = i < n && mark[i] != 0 ? 1u : 0u;
+    const uint32_t e = block_excl_scan(f, &tot);
+    if (f) list[off[blockIdx.x] + e] = (uint32_t)i;
+}
+} // namespace
+
+size_t mark_segments(uint64_t nvox) { return (size_t)((nvox + MARK_B - 1) / MARK_B); }
+
+cudaError_t launch_pair_marks(const uint8_t *code, uint32_t px, uint32_t ny, uint32_t nz, const uint32_t *bpos,
+                              uint64_t nb, const uint32_t *hpos, uint32_t nh, const uint64_t *src, uint32_t nsrc,
+                              uint8_t *mark, uint32_t *cnt, cudaStream_t s)
+{
+    const uint64_t nvox = (uint64_t)px * ny * nz;
+    if (nb + nh + nsrc) {
+        const uint64_t n = nb + nh + nsrc;
+        const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+        k_pair_mark<<<g, 256, 0, s>>>(code, px, ny, nz, bpos, nb, hpos, nh, src, nsrc, mark);
+    }
+    k_mark_count<<<(unsigned)mark_segments(nvox), MARK_B, 0, s>>>(mark, nvox, cnt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mark_list(const uint8_t *mark, uint64_t nvox, const uint32_t *off, uint32_t *list, cudaStream_t s)
+{
+    k_mark_list<<<(unsigned)mark_segments(nvox), MARK_B, 0, s>>>(mark, nvox, off, list);
     return cudaGetLastError();
 }
 

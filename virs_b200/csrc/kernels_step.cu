@@ -251,6 +251,73 @@ __global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArg
     if (h1) bvox_update<T, MODE, MAXS>(a, s1, v1);
 }
 
+// The second step of a two-step pass (kernels_step_tma.cu, k_pair_tma):
+// its boundary pass and the recomputation of its provisional voxels, in one
+// launch.  Blocks [0, gb) take boundary slots as k_boundary does; the others
+// take entries of the provisional-voxel list: air and mirror voxels at or
+// next to a voxel whose p^{n+1} the first step's boundary pass or post
+// kernel changed, whose p^{n+2} the two-step kernel computed from the
+// provisional p^{n+1}.  They are recomputed from the final p^{n+1} (a.p) and
+// p^n (pn) with leapfrog(code, ...), which is bit-identical to the air
+// update for code 0 and is the mirror update for the others.  Both parts
+// read p^{n+1} and write disjoint voxels of p^{n+2} (a.q): boundary voxels,
+// and air or mirror voxels.  Two entries per thread, loads first, as in the
+// boundary pass.
+template <typename T> struct FixVox {
+    size_t i;
+    uint8_t c;
+    float ce, qv, nb[6];
+};
+
+template <typename T>
+__device__ __forceinline__ void fix_load(const StepArgs &a, const T *pn, size_t i, FixVox<T> &v)
+{
+    using IO = Io<T>;
+    const size_t sy = a.px, sz = (size_t)a.px * a.ny;
+    const T *P = static_cast<const T *>(a.p);
+    v.i = i;
+    v.c = __ldg(a.code + i);
+    v.ce = IO::get(P[i]);
+    v.qv = IO::get(pn[i]);
+    v.nb[0] = IO::get(P[i + 1]);
+    v.nb[1] = IO::get(P[i - 1]);
+    v.nb[2] = IO::get(P[i + sy]);
+    v.nb[3] = IO::get(P[i - sy]);
+    v.nb[4] = IO::get(P[i + sz]);
+    v.nb[5] = IO::get(P[i - sz]);
+}
+
+template <typename T> __device__ __forceinline__ void fix_store(const StepArgs &a, const FixVox<T> &v)
+{
+    const float r = leapfrog(v.c, v.ce, v.nb[0], v.nb[1], v.nb[2], v.nb[3], v.nb[4], v.nb[5], v.qv, a.c2dt2, a.inv_h2);
+    static_cast<T *>(a.q)[v.i] = Io<T>::put(r);
+}
+
+template <typename T, int MAXS>
+__global__ void __launch_bounds__(BT) k_boundary_fix(const __grid_constant__ StepArgs a, const void *pn,
+                                                     const uint32_t *__restrict list, uint32_t nlist, uint32_t gb)
+{
+    if (a.stop && *a.stop) return;
+    if (blockIdx.x < gb) {
+        const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
+        const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
+        BVox<T, MAXS> v0, v1;
+        if (h0) bvox_load<T, BND_UPDATE, MAXS>(a, s0, v0);
+        if (h1) bvox_load<T, BND_UPDATE, MAXS>(a, s1, v1);
+        if (h0) bvox_update<T, BND_UPDATE, MAXS>(a, s0, v0);
+        if (h1) bvox_update<T, BND_UPDATE, MAXS>(a, s1, v1);
+        return;
+    }
+    const uint32_t f0 = (blockIdx.x - gb) * (2 * BT) + threadIdx.x, f1 = f0 + BT;
+    const bool h0 = f0 < nlist, h1 = f1 < nlist;
+    const T *P0 = static_cast<const T *>(pn);
+    FixVox<T> v0, v1;
+    if (h0) fix_load<T>(a, P0, __ldg(list + f0), v0);
+    if (h1) fix_load<T>(a, P0, __ldg(list + f1), v1);
+    if (h0) fix_store<T>(a, v0);
+    if (h1) fix_store<T>(a, v1);
+}
+
 // batched: thread g belongs to the last member whose first boundary index
 // is <= g (members without boundary voxels are skipped by that rule); the
 // members' first indices are searched in shared memory
@@ -406,6 +473,32 @@ void boundary_batch_by_sections(uint32_t maxs, unsigned g, const BatchMember *me
 }
 
 } // namespace
+
+namespace {
+template <typename T>
+void boundary_fix_t(const StepArgs &a, const void *pn, const uint32_t *list, uint32_t nlist, cudaStream_t s)
+{
+    const unsigned gb = (unsigned)((a.nb + 2 * BT - 1) / (2 * BT));
+    const unsigned g = gb + (nlist + 2 * BT - 1) / (2 * BT);
+    const uint32_t ns = a.nsec;
+    if (ns <= 1) k_boundary_fix<T, 1><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else if (ns == 2) k_boundary_fix<T, 2><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else if (ns <= 4) k_boundary_fix<T, 4><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else k_boundary_fix<T, 0><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+}
+} // namespace
+
+cudaError_t launch_boundary_fix(int storage, const StepArgs &a, const void *pn, const uint32_t *list, uint32_t nlist,
+                                cudaStream_t s)
+{
+    if (a.nb == 0 && nlist == 0) return cudaSuccess;
+    switch (storage) {
+    case VIRS_STORAGE_F16: boundary_fix_t<__half>(a, pn, list, nlist, s); break;
+    case VIRS_STORAGE_BF16: boundary_fix_t<__nv_bfloat16>(a, pn, list, nlist, s); break;
+    default: boundary_fix_t<float>(a, pn, list, nlist, s); break;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_boundary(int storage, const StepArgs &a, int mode, cudaStream_t s)
 {

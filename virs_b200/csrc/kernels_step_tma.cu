@@ -142,6 +142,54 @@ template <> struct Codes<8> {
     __device__ bool is_mirror(uint32_t m, int k) const { return (m >> (8 * (k & 3) + (k < 4 ? 7 : 6))) & 1u; }
 };
 
+// The update of one thread's V voxels of a plane: cc holds the centres,
+// left / right the x neighbours beyond the vector, ym / yp / zm / zp the y
+// and z neighbours, qv p^{n-1}.
+template <typename T>
+__device__ __forceinline__ void tile_update(const Codes<Lay<T>::V> &code, const float (&cc)[Lay<T>::V], float left,
+                                        float right, const float (&yp)[Lay<T>::V], const float (&ym)[Lay<T>::V],
+                                        const float (&zp)[Lay<T>::V], const float (&zm)[Lay<T>::V],
+                                        const float (&qv)[Lay<T>::V], float2 c2dt2, float2 inv_h2, float c2dt2s,
+                                        float inv_h2s, float (&r)[Lay<T>::V])
+{
+    constexpr int V = Lay<T>::V;
+    // every voxel as air without wall neighbours, the common case, two
+    // at a time ...
+#pragma unroll
+    for (int k = 0; k < V; k += 2) {
+        const float2 x2 = make_float2(__fadd_rn(cc[k + 1], k > 0 ? cc[k - 1] : left),
+                                      __fadd_rn(k + 2 < V ? cc[k + 2] : right, cc[k]));
+        const float2 o = leapfrog_air2(make_float2(cc[k], cc[k + 1]), x2, make_float2(yp[k], yp[k + 1]),
+                                       make_float2(ym[k], ym[k + 1]), make_float2(zp[k], zp[k + 1]),
+                                       make_float2(zm[k], zm[k + 1]), make_float2(qv[k], qv[k + 1]), c2dt2, inv_h2);
+        r[k] = o.x;
+        r[k + 1] = o.y;
+    }
+    // ... then the voxels with another code.  Walls take 0; border,
+    // hard-source and boundary voxels keep p^{n-1} (the post kernel
+    // writes the hard-source value, the boundary pass updates boundary
+    // voxels from the untouched p^n buffer): a test and a select per
+    // voxel, no divergence.  Only air next to a wall outside the
+    // boundary layer (a grid without a sponge layer) needs the update
+    // with the mirror rule; such codes have bit 7 clear and other bits
+    // set, found for four bytes at once.
+    if (__any_sync(FULL, code.any())) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const uint32_t c = code.get(k);
+            if (c & CODE_BND) r[k] = c == CODE_WALL ? 0.f : qv[k];
+        }
+        const uint32_t mirror = code.mirror();
+        if (__any_sync(FULL, mirror != 0u)) {
+#pragma unroll
+            for (int k = 0; k < V; ++k)
+                if (code.is_mirror(mirror, k))
+                    r[k] = leapfrog((uint8_t)code.get(k), cc[k], k == V - 1 ? right : cc[k + 1],
+                                    k == 0 ? left : cc[k - 1], yp[k], ym[k], zp[k], zm[k], qv[k], c2dt2s, inv_h2s);
+        }
+    }
+}
+
 // waits for phase `parity` of *b for at most limit_ns; on timeout sets *err
 __device__ __forceinline__ bool bounded_wait(uint64_t *b, uint32_t parity, uint64_t limit_ns, int *err)
 {
@@ -227,43 +275,8 @@ template <typename T, int TY, int L> struct Tile {
         if (sl == 0) left = IO::ld1(Ph + c0 - 1);
         if (sl == LPR - 1) right = IO::ld1(Ph + c0 + V);
 
-        // every voxel as air without wall neighbours, the common case, two
-        // at a time ...
         float r[V];
-#pragma unroll
-        for (int k = 0; k < V; k += 2) {
-            const float2 x2 = make_float2(__fadd_rn(cc[k + 1], k > 0 ? cc[k - 1] : left),
-                                          __fadd_rn(k + 2 < V ? cc[k + 2] : right, cc[k]));
-            const float2 o = leapfrog_air2(make_float2(cc[k], cc[k + 1]), x2, make_float2(yp[k], yp[k + 1]),
-                                           make_float2(ym[k], ym[k + 1]), make_float2(zp[k], zp[k + 1]),
-                                           make_float2(zm[k], zm[k + 1]), make_float2(qv[k], qv[k + 1]), c2dt2, inv_h2);
-            r[k] = o.x;
-            r[k + 1] = o.y;
-        }
-        // ... then the voxels with another code.  Walls take 0; border,
-        // hard-source and boundary voxels keep p^{n-1} (the post kernel
-        // writes the hard-source value, the boundary pass updates boundary
-        // voxels from the untouched p^n buffer): a test and a select per
-        // voxel, no divergence.  Only air next to a wall outside the
-        // boundary layer (a grid without a sponge layer) needs the update
-        // with the mirror rule; such codes have bit 7 clear and other bits
-        // set, found for four bytes at once.
-        if (__any_sync(FULL, code.any())) {
-#pragma unroll
-            for (int k = 0; k < V; ++k) {
-                const uint32_t c = code.get(k);
-                if (c & CODE_BND) r[k] = c == CODE_WALL ? 0.f : qv[k];
-            }
-            const uint32_t mirror = code.mirror();
-            if (__any_sync(FULL, mirror != 0u)) {
-#pragma unroll
-                for (int k = 0; k < V; ++k)
-                    if (code.is_mirror(mirror, k))
-                        r[k] = leapfrog((uint8_t)code.get(k), cc[k], k == V - 1 ? right : cc[k + 1],
-                                        k == 0 ? left : cc[k - 1], yp[k], ym[k], zp[k], zm[k], qv[k], a->c2dt2,
-                                        a->inv_h2);
-            }
-        }
+        tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, r);
         if (act) IO::st(out, r);
         out += plane;
         sh = sz;
@@ -507,6 +520,284 @@ cudaError_t launch_batch1(int rows, int depth, const BatchMember *mem, uint32_t 
     }
 }
 
+// ============================================================================
+// Two steps in one pass (k_pair_tma)
+// ============================================================================
+// A block owns a tile of TX x TY voxels of (x, y), streamed along z as
+// above, and computes p^{n+1} on the whole tile and p^{n+2} on its inner
+// part: rows 1 .. TY-2 and the vectors 1 .. LPR-2 of each row (TX - 2V
+// voxels).  Tiles overlap by one row and one vector on each side, so the
+// inner parts cover the grid once; neighbouring tiles recompute the p^{n+1}
+// of the overlap with the same operations, so every value agrees.  Along z
+// a block computes p^{n+1} on the planes zs-1 .. z1 and p^{n+2} on
+// zs .. z1-1.
+//
+// p^{n+1}(z) is computed from the staged planes exactly as k_step_tma does,
+// rounded to the storage type, written to a two-plane ring in shared memory
+// (for the y neighbours of the second step) and, on the inner part of the
+// block's own planes, to p^{n+1} in global memory.  In the same iteration
+// the block computes p^{n+2}(z-1): its centre and x neighbours are the
+// thread's p^{n+1}(z-1) (registers, warp shuffles), its y neighbours come
+// from the ring, its z neighbours are p^{n+1}(z-2) and p^{n+1}(z) in
+// registers, and p^{n-1} of that step is the staged P(z-1).  Boundary,
+// hard-source and border voxels keep the previous value in both steps, as
+// in k_step_tma.
+//
+// Voxels whose p^{n+1} changes after the stencil (boundary voxels, by the
+// boundary pass; hard and soft sources, by the post kernel) make the
+// p^{n+2} of their air neighbours (and of a soft source itself) provisional:
+// k_boundary_fix (kernels_step.cu) recomputes those from the final p^{n+1}
+// in the launch of the second boundary pass, so two steps through this
+// kernel give the results of two single steps bit for bit.  The fields are read once and written once per
+// two steps: four buffers, p^n and p^{n-1} in, p^{n+1} and p^{n+2} out.
+//
+// The code box is TX + 16 bytes wide with its x origin rounded down to 16
+// bytes (a TMA copy of 8-bit elements must start on a 16-byte boundary).
+// A tile plane whose codes are all zero (a.tzmask, built per tiling by
+// launch_pair_zero_masks) is not copied, as in k_step_tma.
+template <typename T, int TY> struct PStage {
+    static constexpr int CW = TX + 16;
+    static constexpr uint32_t PB = Lay<T>::PW * (TY + 2) * sizeof(T);
+    static constexpr uint32_t QB = TX * TY * sizeof(T);
+    static constexpr uint32_t CB = CW * TY;
+    static constexpr uint32_t PBa = (PB + 127u) & ~127u;
+    static constexpr uint32_t QBa = (QB + 127u) & ~127u;
+    static constexpr uint32_t CBa = (CB + 127u) & ~127u;
+    static constexpr uint32_t SB = PBa + QBa + CBa;
+    // one plane of p^{n+1} in the ring: TY + 2 rows (the first and the last
+    // are read for tile rows 0 and TY-1, whose results are not kept)
+    static constexpr uint32_t RB = ((TY + 2) * TX * sizeof(T) + 127u) & ~127u;
+};
+
+// V values rounded to the storage type, as a store and a reload would give
+template <typename T> __device__ __forceinline__ void round_to(float (&r)[Lay<T>::V])
+{
+#pragma unroll
+    for (int k = 0; k < Lay<T>::V; ++k) r[k] = Io<T>::get(Io<T>::put(r[k]));
+}
+
+// a plain 16-byte store of V values (shared memory)
+__device__ __forceinline__ void put_vec(float *p, const float (&r)[4])
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(r[0], r[1], r[2], r[3]);
+}
+template <typename H> __device__ __forceinline__ void put_vec(H *p, const float (&r)[8])
+{
+    uint4 v;
+    H *h = reinterpret_cast<H *>(&v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) h[k] = Io<H>::put(r[k]);
+    *reinterpret_cast<uint4 *>(p) = v;
+}
+
+template <typename T, int TY, int L> struct PairTile {
+    using S = PStage<T, TY>;
+    using G = Lay<T>;
+    static constexpr int D = L + 2, V = G::V;
+    const StepArgs *a;
+    unsigned char *smem;
+    T *ring;
+    uint64_t *bars;
+    const CUtensorMap *mP, *mQ, *mC;
+    int *err;
+    T *zo, *wo; // this thread's voxel in plane 0 of p^{n+1} / p^{n+2}
+    int xs, ys, zs, z1, xc, nst, sl, c0, t0, k0, r0;
+    bool leader, inner;
+    float2 c2dt2, inv_h2;
+    size_t plane;
+    uint64_t zmask; // bit j: the codes of stage j are all zero (not copied)
+
+    __device__ __forceinline__ bool codes_zero(int j) const { return j < 64 && ((zmask >> j) & 1ull); }
+
+    // stage j holds plane zs - 2 + j: P always, Q and the codes for the
+    // planes zs-1 .. z1 (j = 1 .. nst-2)
+    __device__ __forceinline__ void issue(int j) const
+    {
+        const int k = zs - 2 + j;
+        unsigned char *st = smem + (uint32_t)(j % D) * S::SB;
+        uint64_t *b = bars + (j % D);
+        const bool full = j >= 1 && j <= nst - 2;
+        const bool codes = full && !codes_zero(j);
+        mbar_expect_tx(b, S::PB + (full ? S::QB : 0u) + (codes ? S::CB : 0u));
+        tma_load_3d(st, mP, b, xs - G::PAD, ys - 1, k);
+        if (full) tma_load_3d(st + S::PBa, mQ, b, xs, ys, k);
+        if (codes) tma_load_3d(st + S::PBa + S::QBa, mC, b, xc, ys, k);
+    }
+
+    // Plane z = zs - 1 + i.  zm, cc: centres of P(z-1), P(z); zp receives
+    // the centre of P(z+1).  um, uc: p^{n+1}(z-2), p^{n+1}(z-1); up
+    // receives p^{n+1}(z).  cprev: the codes of plane z-1, replaced by those
+    // of plane z.
+    __device__ __forceinline__ bool plane_step(int i, const float (&zm)[V], const float (&cc)[V], float (&zp)[V],
+                                               const float (&um)[V], const float (&uc)[V], float (&up)[V],
+                                               Codes<V> &cprev, uint32_t &sh) const
+    {
+        using IO = Io<T>;
+        constexpr int LPR = G::LPR, PW = G::PW;
+        bool bad = false;
+        if (leader) bad = !wait_stage(bars, (uint32_t)i + 2u, D, err);
+        if (__syncthreads_or(bad)) return false;
+        if (leader && i + D < nst) issue(i + D);
+        const uint32_t sz = sh + 1u == (uint32_t)D ? 0u : sh + 1u;
+        const int z = zs - 1 + i;
+
+        // first step: p^{n+1}(z)
+        const unsigned char *s0 = smem + sh * S::SB;
+        const T *Ph = reinterpret_cast<const T *>(s0);
+        {
+            float ym[V], yp[V], qv[V];
+            IO::ld(reinterpret_cast<const T *>(smem + sz * S::SB) + c0, zp);
+            IO::ld(Ph + c0 - PW, ym);
+            IO::ld(Ph + c0 + PW, yp);
+            IO::ld(reinterpret_cast<const T *>(s0 + S::PBa) + t0, qv);
+            Codes<V> code; // stage i + 1 holds plane z
+            if (codes_zero(i + 1)) code.clear();
+            else code.load(s0 + S::PBa + S::QBa + k0);
+            float left = __shfl_up_sync(FULL, cc[V - 1], 1, LPR);
+            float right = __shfl_down_sync(FULL, cc[0], 1, LPR);
+            if (sl == 0) left = IO::ld1(Ph + c0 - 1);
+            if (sl == LPR - 1) right = IO::ld1(Ph + c0 + V);
+            tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, up);
+            round_to<T>(up);
+            put_vec(ring + (uint32_t)(i & 1) * (S::RB / sizeof(T)) + r0, up);
+            if (inner && z >= zs && z < z1) IO::st(zo + (size_t)z * plane, up);
+            // second step: p^{n+2}(z-1), from the ring plane written in the
+            // previous iteration (visible since this iteration's barrier)
+            if (i >= 2) {
+                const T *rm = ring + (uint32_t)((i - 1) & 1) * (S::RB / sizeof(T)) + r0;
+                float ym2[V], yp2[V], r2[V];
+                IO::ld(rm - TX, ym2);
+                IO::ld(rm + TX, yp2);
+                const float left2 = __shfl_up_sync(FULL, uc[V - 1], 1, LPR);
+                const float right2 = __shfl_down_sync(FULL, uc[0], 1, LPR);
+                tile_update<T>(cprev, uc, left2, right2, yp2, ym2, up, um, zm, c2dt2, inv_h2, a->c2dt2, a->inv_h2,
+                               r2);
+                if (inner) IO::st(wo + (size_t)(z - 1) * plane, r2);
+            }
+            cprev = code;
+        }
+        sh = sz;
+        return true;
+    }
+};
+
+// blocks per SM the register allocation must allow: two FP32 blocks of 512
+// threads (64 registers, no spills); the 16-bit kernels keep their registers
+template <typename T, int TY> constexpr int pair_min_blocks()
+{
+    return sizeof(T) == 4 && block_threads<T, TY>() <= 512 ? 2 : 1;
+}
+
+template <typename T, int TY, int L>
+__global__ void __launch_bounds__(block_threads<T, TY>(), (pair_min_blocks<T, TY>())) k_pair_tma(const __grid_constant__ StepArgs a,
+                                                                        const __grid_constant__ CUtensorMap mP,
+                                                                        const __grid_constant__ CUtensorMap mQ,
+                                                                        const __grid_constant__ CUtensorMap mC,
+                                                                        void *zout, void *wout, int *err)
+{
+    using G = Lay<T>;
+    using S = PStage<T, TY>;
+    using IO = Io<T>;
+    constexpr int V = G::V, LPR = G::LPR, PW = G::PW, PAD = G::PAD, D = L + 2;
+    constexpr int IX = TX - 2 * V, IY = TY - 2;
+    if (a.stop && *a.stop) return; // the stop rule fired at an earlier step (uniform over the block)
+    extern __shared__ __align__(128) unsigned char smem[];
+    PairTile<T, TY, L> t;
+    t.a = &a;
+    t.smem = smem;
+    t.ring = reinterpret_cast<T *>(smem + D * S::SB);
+    t.bars = reinterpret_cast<uint64_t *>(smem + D * S::SB + 2 * S::RB);
+    t.mP = &mP;
+    t.mQ = &mQ;
+    t.mC = &mC;
+    t.err = err;
+    const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
+    for (uint32_t k = tid; k < 2 * S::RB / 16; k += blockDim.x * blockDim.y)
+        reinterpret_cast<uint4 *>(t.ring)[k] = make_uint4(0u, 0u, 0u, 0u);
+    init_bars<D>(t.bars);
+    t.zs = 1 + (int)blockIdx.z * a.zc;
+    t.z1 = min(t.zs + a.zc, (int)a.nz - 1);
+    if (t.zs >= t.z1) return; // uniform over the block
+    t.nst = t.z1 - t.zs + 4;  // P planes zs-2 .. z1+1
+    t.xs = (int)blockIdx.x * IX - V;
+    t.ys = (int)blockIdx.y * IY - 1;
+    t.xc = t.xs & ~15; // rounded down to 16 bytes of codes (two's complement: also below zero)
+    const int row = threadIdx.y * G::RPW + lane / LPR;
+    t.sl = lane % LPR;
+    const int x = t.xs + t.sl * V, y = t.ys + row;
+    t.inner = t.sl >= 1 && t.sl <= LPR - 2 && row >= 1 && row <= TY - 2 && x < (int)a.px && y < (int)a.ny;
+    t.leader = tid == 0;
+    t.c0 = (row + 1) * PW + PAD + t.sl * V;
+    t.t0 = row * TX + t.sl * V;
+    t.k0 = row * S::CW + (t.xs - t.xc) + t.sl * V;
+    t.r0 = (row + 1) * TX + t.sl * V;
+    t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
+    t.inv_h2 = make_float2(a.inv_h2, a.inv_h2);
+    t.plane = (size_t)a.px * a.ny;
+    t.zmask = a.tzmask ? __ldg(a.tzmask + ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x)
+                       : 0ull;
+    const size_t off = t.inner ? (size_t)y * a.px + (size_t)x : 0;
+    t.zo = static_cast<T *>(zout) + off;
+    t.wo = static_cast<T *>(wout) + off;
+
+    if (t.leader)
+        for (int j = 0; j < D && j < t.nst; ++j) t.issue(j);
+
+    float A[V], B[V], C[V], X0[V], X1[V], X2[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) X0[k] = X1[k] = X2[k] = 0.f;
+    {
+        bool bad = false;
+        if (t.leader) bad = !wait_stage(t.bars, 0u, D, err) || !wait_stage(t.bars, 1u, D, err);
+        if (__syncthreads_or(bad)) return;
+        IO::ld(reinterpret_cast<const T *>(smem) + t.c0, A);                        // P(zs-2)
+        IO::ld(reinterpret_cast<const T *>(smem + (1u % D) * S::SB) + t.c0, B);     // P(zs-1)
+    }
+    uint32_t sh = 1u % D;
+    Codes<V> cprev;
+    cprev.clear();
+    // i = 0 .. n-1 computes p^{n+1} of plane zs-1+i; the p^{n+1} centres
+    // rotate through X0..X2 with the P centres A..C, three planes per turn
+    const int n = t.nst - 2;
+    int i = 0;
+    for (; i + 3 <= n; i += 3) {
+        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh)) return;
+        if (!t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh)) return;
+        if (!t.plane_step(i + 2, C, A, B, X0, X1, X2, cprev, sh)) return;
+    }
+    if (i < n) {
+        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh)) return;
+        if (i + 1 < n && !t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh)) return;
+    }
+}
+
+template <typename T, int TY, int L> constexpr size_t pair_smem_bytes()
+{
+    return (size_t)(L + 2) * PStage<T, TY>::SB + 2 * PStage<T, TY>::RB + (L + 2) * sizeof(uint64_t);
+}
+
+template <typename T, int TY, int L>
+cudaError_t pair3(const StepArgs &a, const TmaMaps &m, void *zout, void *wout, int *err, cudaStream_t s)
+{
+    auto kern = k_pair_tma<T, TY, L>;
+    constexpr size_t sm = pair_smem_bytes<T, TY, L>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    constexpr int IX = TX - 2 * Lay<T>::V, IY = TY - 2;
+    const unsigned gx = (a.px + IX - 1) / IX, gy = (a.ny + IY - 1) / IY;
+    const unsigned gz = (a.nz - 2 + a.zc - 1) / a.zc;
+    kern<<<dim3(gx, gy, gz), dim3(32, block_threads<T, TY>() / 32), sm, s>>>(a, *m.p, *m.q, *m.c, zout, wout, err);
+    return cudaGetLastError();
+}
+
+// two planes in flight (a 32-row FP32 tile at three would not fit in
+// shared memory)
+template <typename T>
+cudaError_t pair1(int rows, const StepArgs &a, const TmaMaps &m, void *zout, void *wout, int *err, cudaStream_t s)
+{
+    return rows == 32 ? pair3<T, 32, 2>(a, m, zout, wout, err, s) : pair3<T, 16, 2>(a, m, zout, wout, err, s);
+}
+
 } // namespace
 
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
@@ -544,5 +835,22 @@ cudaError_t launch_step_tma(int storage, int tile_rows, int depth, const StepArg
     default: return launch1<float>(tile_rows, depth, a, m, err, s);
     }
 }
+
+int pair_tile_x(int storage) { return TX - 2 * (storage == VIRS_STORAGE_F32 ? 4 : 8); }
+int pair_code_box() { return TX + 16; }
+
+cudaError_t launch_pair_tma(int storage, int tile_rows, const StepArgs &a0, const TmaMaps &m, void *zout, void *wout,
+                            int *err, cudaStream_t s)
+{
+    if (a0.nz < 3 || a0.ny < 3 || a0.nx < 3) return cudaSuccess;
+    StepArgs a = a0;
+    if (a.zc <= 0) a.zc = (int)a.nz - 2;
+    switch (storage) {
+    case VIRS_STORAGE_F16: return pair1<__half>(tile_rows, a, m, zout, wout, err, s);
+    case VIRS_STORAGE_BF16: return pair1<__nv_bfloat16>(tile_rows, a, m, zout, wout, err, s);
+    default: return pair1<float>(tile_rows, a, m, zout, wout, err, s);
+    }
+}
+
 
 } // namespace virs
