@@ -239,6 +239,9 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         out["kernel_ms"] = t.step_kernel_ms / max(t.step_launches, 1)
         per = 2 if out["time_blocking"]["active"] else 1
         out["boundary_ms"] = t.boundary_kernel_ms / max(t.step_launches * per, 1)
+        # the library's count of its kernel launches (5 per two steps with
+        # time blocking, 3 per step otherwise)
+        out["launches_per_step"] = t.kernel_launches / args.kernel_steps
     if want_e2e:
         nsrc, nrcv = len(sc.src_pos), len(sc.rcv_pos)
         first = int(sim.info().steps_done)
@@ -423,6 +426,9 @@ def run_virs(args):
             "steps_per_launch": steps_per_launch,
             "bytes_per_voxel": bpv,
             "boundary_pass_ms": r32.get("boundary_ms"),
+            "boundary_pass_note": ("per step: a two-step pass's two boundary launches (the second also recomputes "
+                                   "the voxels next to boundary voxels and sources), halved" if steps_per_launch == 2
+                                   else "per step"),
         },
         "e2e": {
             "value": round(nvox * args.steps / (r32["e2e_ms"] * 1e-3) / 1e9 * world, 3),
@@ -432,7 +438,7 @@ def run_virs(args):
             "api": "virs_run_host (pinned host buffers)",
             "wall_ms": r32["e2e_wall_ms"],
         },
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": round(r32.get("launches_per_step", 3) * args.steps),
         "clocks": r32["clocks"],
         "variants": variants,
     }
