@@ -343,9 +343,11 @@ virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block, 
  * runs single steps).  The voxels next to boundary voxels and sources are
  * recomputed after the first step is complete, so the results are
  * bit-identical to single steps.  tile_rows 16 or 32 (0 = 16), planes per
- * block 0 = all.  Off (1) by default; not used with the device stop rule or
- * the register-streaming kernel (pipeline depth 0).  *active tells whether
- * the current settings run two steps per pass. */
+ * block 0 = all.  Off (1) by default; not used with the register-streaming
+ * kernel (pipeline depth 0).  With the device stop rule, a run that stops
+ * inside a group of four steps leaves the stop step's fields in the usual
+ * buffers, as single steps do.  *active tells whether the current settings
+ * run two steps per pass. */
 virs_status virs_set_time_blocking(virs_sim *sim, int steps_per_pass, int tile_rows, int planes_per_block);
 virs_status virs_get_time_blocking(const virs_sim *sim, int *steps_per_pass, int *tile_rows, int *planes_per_block,
                                    int *active);

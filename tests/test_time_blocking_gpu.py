@@ -171,13 +171,44 @@ def test_moved_sources_rebuild_the_fix_list():
     assert _same(runs[0][0], runs[1][0]) and _same(runs[0][1], runs[1][1])
 
 
-def test_not_used_with_the_stop_rule_or_register_kernel():
+@pytest.mark.parametrize("lead", [0, 1, 2, 3])
+def test_stop_rule_inside_a_group_of_four(lead):
+    """The device stop rule fires at the same step as with single steps,
+    wherever that step falls in a group of four (lead single steps shift the
+    groups), and leaves the same samples and fields."""
+    sc = scenes.reference_room(steps=3200, size=(24, 20, 16))
+    ref, _ = scenes.build_simulation(sc)
+    ref.set_stop_rule(True)
+    ref.run(sc.steps)
+    stopped, stop = ref.stop_state()
+    assert stopped and stop > 3000
+    dev, _ = scenes.build_simulation(sc)
+    dev.set_stop_rule(True)
+    dev.set_time_blocking(2)
+    assert dev.time_blocking()["active"]
+    if lead:
+        dev.run(lead)
+    dev.run(sc.steps - lead)
+    assert dev.stop_state() == (True, stop)
+    assert dev.info().steps_done == stop + 1
+    assert _same(dev.ir(0, stop + 1), ref.ir(0, stop + 1))
+    p, pp = dev.pressure(prev=True)
+    rp, rpp = ref.pressure(prev=True)
+    assert _same(p, rp) and _same(pp, rpp)
+    dev.run(8)                                              # nothing runs after the stop
+    assert dev.info().steps_done == stop + 1
+    assert _same(dev.pressure(), rp)
+    ref.close()
+    dev.close()
+
+
+def test_not_used_with_the_register_kernel():
     make, want, _ = _random_case((40, 30, 20), 1, 3, 20)
     sim = make()
     sim.set_time_blocking(2)
     assert sim.time_blocking()["active"]
     sim.set_stop_rule(True)
-    assert not sim.time_blocking()["active"]
+    assert sim.time_blocking()["active"]
     sim.set_stop_rule(False)
     sim.set_tiling(8, 0, 0)
     assert not sim.time_blocking()["active"]

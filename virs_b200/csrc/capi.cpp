@@ -696,8 +696,7 @@ void *buf_ptr(const virs_sim *s, int k) { return k < 2 ? s->field[k].ptr : s->sp
 
 bool pair_on(const virs_sim *s)
 {
-    return s->pair_steps == 2 && !s->pair_nomem && s->depth > 0 && !s->stop_rule && s->nx >= 3 && s->ny >= 3 &&
-           s->nz >= 3;
+    return s->pair_steps == 2 && !s->pair_nomem && s->depth > 0 && s->nx >= 3 && s->ny >= 3 && s->nz >= 3;
 }
 
 // the voxels whose p^{n+2} the two-step kernel leaves provisional, for the
@@ -866,6 +865,28 @@ virs_status build_graphs(virs_sim *s, cudaStream_t st)
     return VIRS_OK;
 }
 
+// The stop rule fired after step `ran` of a run whose first 4*quads steps
+// went through the four-buffer rotation from parity par: every later kernel
+// returned at entry, so the last step's p and p^{n-1} are where that step
+// left them.  Put them back into field[cur] and field[cur ^ 1] (cur = par ^
+// (ran & 1)), the layout the rest of the library reads.
+virs_status settle_pair_stop(virs_sim *s, int par, uint64_t ran, cudaStream_t st)
+{
+    const size_t fb = s->field[0].bytes;
+    auto copy = [&](int k) { return cudaMemcpyAsync(s->field[k].ptr, s->spare[k].ptr, fb, cudaMemcpyDeviceToDevice, st); };
+    switch ((ran - 1) % 4) {
+    case 0: VIRS_CUDA(copy(par ^ 1)); break;     // p: spare[par^1]; p^{n-1}: field[par]
+    case 1:                                       // p: spare[par]; p^{n-1}: spare[par^1]
+        VIRS_CUDA(copy(par));
+        VIRS_CUDA(copy(par ^ 1));
+        break;
+    case 2: VIRS_CUDA(copy(par)); break;         // p: field[par^1]; p^{n-1}: spare[par]
+    default: break;                              // a whole group: the usual layout
+    }
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    return VIRS_OK;
+}
+
 virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
 {
     if (s->stop_rule && s->stopped) return VIRS_OK; // nothing runs after the rule fired, until a new start
@@ -973,6 +994,7 @@ virs_status run_steps(virs_sim *s, uint64_t n, cudaStream_t st)
             s->steps_done = (uint64_t)sb[1] + 1;
             s->stopped = true;
             s->stop_step = sb[1];
+            if (ran <= 4 * quads) VIRS_TRY(settle_pair_stop(s, cur0, ran, st));
         }
     }
     return VIRS_OK;
