@@ -151,6 +151,18 @@ public:
     void start(uint64_t steps) { check(virs_start_simulation(h_, steps)); }
     void run(uint64_t steps, void *stream = nullptr) { check(virs_run(h_, steps, stream)); }
     void synchronize() { check(virs_synchronize(h_)); }
+    /* right after start: the fastest tiling and steps per pass for this grid */
+    virs_tiling autotune(uint32_t trial_steps = 4)
+    {
+        virs_tiling t{};
+        check(virs_autotune(h_, trial_steps, &t));
+        return t;
+    }
+    /* two steps per pass over the fields (bit-identical to single steps) */
+    void set_time_blocking(int steps_per_pass, int tile_rows = 0, int planes_per_block = 0)
+    {
+        check(virs_set_time_blocking(h_, steps_per_pass, tile_rows, planes_per_block));
+    }
     /* receiver samples [n_receivers][steps] from step `first` */
     std::vector<float> ir(uint64_t first, uint64_t steps, uint32_t n_receivers) const
     {

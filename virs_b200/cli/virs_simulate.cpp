@@ -522,6 +522,7 @@ int main(int argc, char **argv)
         sim.set_receivers({((uint64_t)rz * g.ny + (uint64_t)ry) * g.nx + (uint64_t)rx});
         virs::check(virs_set_stop_rule(sim.handle(), 1));
         sim.start(steps);
+        sim.autotune(); // tiling and steps per pass for this grid; results are the same bits either way
         sim.run(steps);
         sim.synchronize();
         const virs_grid_info after = sim.info();
