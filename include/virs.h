@@ -363,7 +363,8 @@ typedef struct virs_tiling {
  * times `trial_steps` steps of each TMA variant (tile rows 4/8/16, depth
  * 1..3, 8..64 planes per block) and then of the two-step variants (time
  * blocking: tile rows 16/32, 32..128 planes per block, trial_steps rounded
- * up to a multiple of four) on this handle's own grid and keeps the fastest:
+ * up to a multiple of four, at least eight) on this handle's own grid and
+ * keeps the fastest:
  * the tiling it returns, and the steps per pass that virs_get_time_blocking
  * reports.  The simulation is then back at rest.  Results are cached per
  * device, storage and grid shape for the life of the process. */

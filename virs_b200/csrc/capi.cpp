@@ -2037,7 +2037,8 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
         }
     }
     if (!cached) {
-        const uint32_t quads = (trial_steps + 3) / 4;
+        // two-step trials: at least two groups of four steps each
+        const uint32_t quads = std::max<uint32_t>(2, (trial_steps + 3) / 4);
         VIRS_TRY(ensure_ir(s, std::max<uint64_t>(2ull * trial_steps, 4ull * quads + 4) + 2));
         s->pair_steps = 1;
         cudaEvent_t e0, e1;
@@ -2085,7 +2086,7 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
             s->depth = pick.t.pipeline_depth;
             s->zc = pick.t.planes_per_block;
             s->maps_rows = 0;
-            const int prow_c[] = {16, 32}, pplanes_c[] = {32, 51, 64, 102, 128};
+            const int prow_c[] = {16, 32}, pplanes_c[] = {32, 42, 51, 64, 102, 128};
             for (int r : prow_c)
                 for (int pl : pplanes_c) {
                     if (st != VIRS_OK) break;

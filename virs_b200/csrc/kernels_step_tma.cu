@@ -630,7 +630,7 @@ template <typename T, int TY, int L> struct PairTile {
     // of plane z.
     __device__ __forceinline__ bool plane_step(int i, const float (&zm)[V], const float (&cc)[V], float (&zp)[V],
                                                const float (&um)[V], const float (&uc)[V], float (&up)[V],
-                                               Codes<V> &cprev, uint32_t &sh) const
+                                               Codes<V> &cprev, uint32_t &sh, T *&zout, T *&wout) const
     {
         using IO = Io<T>;
         constexpr int LPR = G::LPR, PW = G::PW;
@@ -660,10 +660,14 @@ template <typename T, int TY, int L> struct PairTile {
             tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, up);
             round_to<T>(up);
             put_vec(ring + (uint32_t)(i & 1) * (S::RB / sizeof(T)) + r0, up);
-            if (inner && z >= zs && z < z1) IO::st(zo + (size_t)z * plane, up);
+            if (inner && z >= zs && z < z1) IO::st(zout, up);
+            zout += plane;
             // second step: p^{n+2}(z-1), from the ring plane written in the
-            // previous iteration (visible since this iteration's barrier)
-            if (i >= 2) {
+            // previous iteration (visible since this iteration's barrier).
+            // Computed in every iteration, without a branch, so that the
+            // compiler can interleave it with the first step; kept from
+            // i = 2 on (the first two planes are the halo below the block).
+            {
                 const T *rm = ring + (uint32_t)((i - 1) & 1) * (S::RB / sizeof(T)) + r0;
                 float ym2[V], yp2[V], r2[V];
                 IO::ld(rm - TX, ym2);
@@ -672,7 +676,8 @@ template <typename T, int TY, int L> struct PairTile {
                 const float right2 = __shfl_down_sync(FULL, uc[0], 1, LPR);
                 tile_update<T>(cprev, uc, left2, right2, yp2, ym2, up, um, zm, c2dt2, inv_h2, a->c2dt2, a->inv_h2,
                                r2);
-                if (inner) IO::st(wo + (size_t)(z - 1) * plane, r2);
+                if (inner && i >= 2) IO::st(wout, r2);
+                if (i >= 2) wout += plane;
             }
             cprev = code;
         }
@@ -739,6 +744,8 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), (pair_min_blocks<T, TY
     const size_t off = t.inner ? (size_t)y * a.px + (size_t)x : 0;
     t.zo = static_cast<T *>(zout) + off;
     t.wo = static_cast<T *>(wout) + off;
+    T *zrun = t.zo + (size_t)(t.zs - 1) * t.plane; // p^{n+1} of the plane of the current iteration
+    T *wrun = t.wo + (size_t)t.zs * t.plane;       // p^{n+2} of the plane the second step writes next
 
     if (t.leader)
         for (int j = 0; j < D && j < t.nst; ++j) t.issue(j);
@@ -761,13 +768,13 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), (pair_min_blocks<T, TY
     const int n = t.nst - 2;
     int i = 0;
     for (; i + 3 <= n; i += 3) {
-        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh)) return;
-        if (!t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh)) return;
-        if (!t.plane_step(i + 2, C, A, B, X0, X1, X2, cprev, sh)) return;
+        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh, zrun, wrun)) return;
+        if (!t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh, zrun, wrun)) return;
+        if (!t.plane_step(i + 2, C, A, B, X0, X1, X2, cprev, sh, zrun, wrun)) return;
     }
     if (i < n) {
-        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh)) return;
-        if (i + 1 < n && !t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh)) return;
+        if (!t.plane_step(i, A, B, C, X1, X2, X0, cprev, sh, zrun, wrun)) return;
+        if (i + 1 < n && !t.plane_step(i + 1, B, C, A, X2, X0, X1, cprev, sh, zrun, wrun)) return;
     }
 }
 
