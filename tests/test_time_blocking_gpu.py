@@ -223,3 +223,55 @@ def test_not_used_with_the_register_kernel():
     with pytest.raises(capi.VirsError):
         sim.set_time_blocking(2, 8)
     sim.close()
+
+
+def test_adjoint_forward_pass_and_gradients_unchanged():
+    """virs_forward_checkpointed advances its segments through virs_run, so
+    with two steps per pass: the same receiver samples bit for bit, and the
+    same gradients (their FP64 sums are accumulated with atomics, whose order
+    varies from run to run, so they agree to 1e-9 relative)."""
+    sc, _ = scenes.inverse_design(steps=200, size=(40, 36, 28), h=0.04, n_materials=6)
+    dl = np.random.default_rng(5).standard_normal((len(sc.rcv_pos), sc.steps)).astype(np.float32)
+    out = []
+    for pair in (False, True):
+        sim, _ = scenes.build_simulation(sc)
+        if pair:
+            sim.set_time_blocking(2)
+            assert sim.time_blocking()["active"]
+        sim.forward_checkpointed(sc.steps, 32)
+        ir = sim.ir(0, sc.steps)
+        gc, gs = sim.adjoint(dl, sc.n_materials, sc.n_sections)
+        out.append((ir, gc, gs))
+        sim.close()
+    assert _same(out[0][0], out[1][0])
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
+
+
+def test_batch_of_members_that_ran_two_steps_per_pass():
+    """Members advanced two steps per pass keep their state in the usual two
+    buffers, so a batch built from them continues exactly as their solo
+    runs."""
+    shape, steps = (64, 40, 36), 48
+    solo = []
+    for seed in (31, 32):
+        make, _, _ = _random_case(shape, 1, seed, steps)
+        s = make()
+        s.run(steps)
+        solo.append(s.ir())
+        s.close()
+    members = []
+    for seed in (31, 32):
+        make, _, _ = _random_case(shape, 1, seed, steps)
+        s = make()
+        s.set_time_blocking(2)
+        s.run(20)                                   # five groups of four
+        members.append(s)
+    batch = capi.Batch(members)
+    batch.run(steps - 20)
+    batch.synchronize()
+    for m, want in zip(members, solo):
+        assert _same(m.ir(), want)
+    batch.close()
+    for m in members:
+        m.close()
