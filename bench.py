@@ -358,12 +358,13 @@ def run_virs(args):
         rb = bench_storage(sc, capi.STORAGE_BF16, args, stream, dev, world, dist, want_e2e=False)
         gv = nvox * args.steps / (rb["ms"] * 1e-3) / 1e9 * world
         peak, _ = peaks()
-        bb, _, bkern, _ = stencil_roofline(rb, "bf16")
+        _, bsteps, bkern, _ = stencil_roofline(rb, "bf16")
         variants["bf16_storage"] = {
             "value": gv, "ms_per_step": rb["ms"] / args.steps,
             "speedup_vs_f32": (r32["ms"] / rb["ms"]),
-            "roofline_frac": (nvox * bb / (rb["kernel_ms"] * 1e-3) / 1e9) / peak if rb.get("kernel_ms") else None,
-            "bytes_per_voxel": bb,
+            "roofline_frac": (nvox * BYTES_16 * bsteps / (rb["kernel_ms"] * 1e-3) / 1e9) / peak
+            if rb.get("kernel_ms") else None,
+            "bytes_per_voxel": BYTES_16,
             "kernel": bkern.split(" ")[0],
             "time_blocking": rb["time_blocking"],
         }
@@ -382,7 +383,14 @@ def run_virs(args):
     interior = int(np.prod([d - 2 for d in args.size]))
     kernel_ms = r32.get("kernel_ms")
     bpv, steps_per_launch, kernel_name, traffic_file = stencil_roofline(r32, args.storage)
-    achieved = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    # algorithmic bytes per launch: 13 B (7 B in 16-bit storage) per voxel
+    # update times the updates one launch makes (two per voxel with time
+    # blocking, an effective bandwidth that exceeds the DRAM bytes); the
+    # kernel's own bytes per voxel and launch (17 / 9 with time blocking)
+    # and the measured DRAM traffic are reported beside it
+    upd = BYTES_F32 if args.storage == "f32" else BYTES_16
+    achieved = nvox * upd * steps_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    own = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -424,7 +432,10 @@ def run_virs(args):
             "kernel": kernel_name,
             "kernel_ms": kernel_ms,
             "steps_per_launch": steps_per_launch,
-            "bytes_per_voxel": bpv,
+            "basis": "%g B per voxel update x %d update(s) per voxel per launch" % (upd, steps_per_launch),
+            "bytes_per_voxel": upd,
+            "launch_bytes_per_voxel": bpv,
+            "launch_frac": round(own / peak, 4) if own else None,
             "boundary_pass_ms": r32.get("boundary_ms"),
             "boundary_pass_note": ("per step: a two-step pass's two boundary launches (the second also recomputes "
                                    "the voxels next to boundary voxels and sources), halved" if steps_per_launch == 2
@@ -448,6 +459,8 @@ def run_virs(args):
     if tr:
         line["roofline"]["traffic"] = tr["bytes"]
         line["roofline"]["traffic_source"] = tr["source"]
+        if kernel_ms:
+            line["roofline"]["dram_frac"] = round(tr["bytes"] / (kernel_ms * 1e-3) / 1e9 / peak, 4)
     if world == 1 and not args.no_cpu:
         th = host_threads()
         gv, desc, secs = cpu_sample(tuple(args.size), args.cpu_seconds, th)
