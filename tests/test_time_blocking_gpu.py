@@ -275,3 +275,46 @@ def test_batch_of_members_that_ran_two_steps_per_pass():
     batch.close()
     for m in members:
         m.close()
+
+
+@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 4, 3), (33, 3, 7), (130, 5, 4), (260, 17, 9), (40, 40, 5)])
+def test_degenerate_grids(shape):
+    """One interior voxel, one interior plane, grids thinner than a tile in
+    y, narrower than a tile in x and wider than two: two steps per pass
+    equal the oracle."""
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    rng = np.random.default_rng(sum(shape))
+    flags = np.zeros(n, np.uint8)
+    if n > 27:
+        flags[rng.random(n) < 0.05] = 1
+    ref_flags, bm, bd = oracle.classify(shape, 1, flags, None)
+    bidx = oracle.boundary_list(shape, ref_flags)
+    interior = [i for i in range(n)
+                if 0 < i % nx < nx - 1 and 0 < (i // nx) % ny < ny - 1 and 0 < i // (nx * ny) < nz - 1
+                and ref_flags[i] in (0, 2)]
+    src = np.array(interior[:1], np.uint64)
+    rcv = np.array(interior[-2:], np.uint64)
+    sig = np.linspace(-1, 1, 30, dtype=np.float32)[None, :]
+    steps = 26
+    _, c2dt2, inv_h2, K = oracle.step_constants(0.05, 343.0, 1.0)
+    fs = oracle.filter_fs(0.05, 343.0, 1.0)
+    coef = oracle.rbj_highpass_ref(fs, 440.0, 0.1)[None, None, :]
+    osc = oracle.Scene(shape, ref_flags, bidx, bm[bidx], oracle.sponge_weights_for(1, bd[bidx]), coef, 1,
+                       hard=np.full(10, 10.0, np.float32), src_idx=src, src_sig=sig, rcv_idx=rcv,
+                       consts=(c2dt2, inv_h2, K), form=1)
+    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(bidx.size * 4 + 1, np.float32))
+    want = osc.run(steps, state=st)
+    sim = capi.Simulation(capi.default_params(courant=1.0, boundary_form=1))
+    sim.set_grid(shape, 0.05, flags)
+    sim.classify()
+    sim.set_sources(src, sig)
+    sim.set_receivers(rcv)
+    sim.start(steps)
+    sim.set_time_blocking(2, 16, 0)
+    assert sim.time_blocking()["active"]
+    sim.run(steps)
+    assert _same(sim.ir(), want)
+    p, pp = sim.pressure(prev=True)
+    assert _same(p, st[0]) and _same(pp, st[1])
+    sim.close()
