@@ -1938,6 +1938,7 @@ VIRS_EXPORT virs_status virs_set_time_blocking(virs_sim *s, int steps_per_pass, 
     if (tile_rows != 0 && tile_rows != 16 && tile_rows != 32)
         return fail(VIRS_E_ARG, "two-step tile rows must be 16 or 32");
     if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
+    VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     s->pair_steps = steps_per_pass;
     s->pair_rows = tile_rows ? tile_rows : 16;
