@@ -66,8 +66,10 @@ def test_oracle_rigid_walls_match_reference_gpu():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("steps_per_pass", [1, 2])
 @pytest.mark.parametrize("name", CASES + [RIGID])
-def test_cuda_path_matches_reference_gpu(name):
+def test_cuda_path_matches_reference_gpu(name, steps_per_pass):
+    """The reference's own kernels' outputs, one or two steps per pass."""
     from virs_b200 import capi
     d = _load(name)
     shape = tuple(int(s) for s in d["shape"])
@@ -81,6 +83,8 @@ def test_cuda_path_matches_reference_gpu(name):
     sim.set_receivers(d["rcv"])
     steps = d["ir"].shape[1]
     sim.start(steps)
+    sim.set_time_blocking(steps_per_pass)
+    assert sim.time_blocking()["active"] == (steps_per_pass == 2)
     sim.run(steps)
     got = sim.ir()
     assert np.array_equal(got.view(np.uint32), d["ir"].view(np.uint32))
