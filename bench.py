@@ -214,7 +214,7 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         # two-step tiling when it chose one, else --pair-tiling
         tb = sim.time_blocking()
         rows, planes = (tb["rows"], tb["planes"]) if tb["active"] and not args.pair_tiling else \
-            tuple(args.pair_tiling or (16, 64))
+            tuple(args.pair_tiling or (14, 42))
         sim.set_time_blocking(args.steps_per_pass, rows, planes)
     sim.run(warm, stream.cuda_stream)
     torch.cuda.synchronize()
@@ -552,7 +552,7 @@ def main():
     ap.add_argument("--steps-per-pass", type=int, choices=[0, 1, 2], default=0,
                     help="0: the autotuner's choice; 1: single steps; 2: two steps per pass (time blocking)")
     ap.add_argument("--pair-tiling", type=int, nargs=2, default=None, metavar=("ROWS", "PLANES"),
-                    help="tile rows (16/32) and planes per block of the two-step kernel with --steps-per-pass 2")
+                    help="tile rows (12/14/16/32) and planes per block of the two-step kernel with --steps-per-pass 2")
     ap.add_argument("--traffic", default=None,
                     help="ncu DRAM-traffic summary of the stencil kernel")
     args = ap.parse_args()

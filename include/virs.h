@@ -342,8 +342,9 @@ virs_status virs_set_tiling(virs_sim *sim, int tile_rows, int planes_per_block, 
  * more field buffers allocated on first use (a grid for which they do not fit
  * runs single steps).  The voxels next to boundary voxels and sources are
  * recomputed after the first step is complete, so the results are
- * bit-identical to single steps.  tile_rows 16 or 32 (0 = 16), planes per
- * block 0 = all.  Off (1) by default; not used with the register-streaming
+ * bit-identical to single steps.  tile_rows 12, 14, 16 or 32 (0 = 14; with
+ * 12, 14 and 16 rows 4, 3 and 2 planes are in flight), planes per block
+ * 0 = all.  Off (1) by default; not used with the register-streaming
  * kernel (pipeline depth 0).  With the device stop rule, a run that stops
  * inside a group of four steps leaves the stop step's fields in the usual
  * buffers, as single steps do.  *active tells whether the current settings
@@ -362,9 +363,9 @@ typedef struct virs_tiling {
 /* Autotuner (no reference counterpart): right after virs_start_simulation,
  * times `trial_steps` steps of each TMA variant (tile rows 4/8/16, depth
  * 1..3, 8..64 planes per block) and then of the two-step variants (time
- * blocking: tile rows 16/32, 32..128 planes per block, trial_steps rounded
- * up to a multiple of four, at least eight) on this handle's own grid and
- * keeps the fastest:
+ * blocking: tile rows 14/16/12, 32..102 planes per block, trial_steps
+ * rounded up to a multiple of four, at least eight, each timed twice) on
+ * this handle's own grid and keeps the fastest:
  * the tiling it returns, and the steps per pass that virs_get_time_blocking
  * reports.  The simulation is then back at rest.  Results are cached per
  * device, storage and grid shape for the life of the process. */

@@ -71,6 +71,9 @@ def _same(a, b):
     ((300, 40, 30), 2, 5, 16, 7),
     ((33, 64, 40), 5, 3, 32, 0),
     ((250, 31, 18), 1, 6, 16, 1),
+    ((45, 27, 19), 2, 7, 14, 3),
+    ((270, 23, 25), 1, 8, 12, 0),
+    ((64, 50, 30), 3, 9, 12, 6),
 ])
 def test_random_grids_match_oracle(shape, W, seed, rows, planes):
     """123 steps: 30 groups of four (a CUDA graph of eight, then eager
@@ -217,7 +220,7 @@ def test_not_used_with_the_register_kernel():
     sim.set_tiling(8, 0, 2)
     assert sim.time_blocking()["active"]
     sim.set_time_blocking(1)
-    assert sim.time_blocking() == {"steps_per_pass": 1, "rows": 16, "planes": 0, "active": False}
+    assert sim.time_blocking() == {"steps_per_pass": 1, "rows": 14, "planes": 0, "active": False}
     with pytest.raises(capi.VirsError):
         sim.set_time_blocking(3)
     with pytest.raises(capi.VirsError):

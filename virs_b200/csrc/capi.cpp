@@ -172,7 +172,7 @@ struct virs_sim {
     // spare[1] (index 0..3) for pm_rows-row tiles, pmC the wider code box;
     // plist holds the voxels whose second step is provisional (pl_ok: built
     // for the current codes and sources)
-    int pair_steps = 1, pair_rows = 16, pair_zc = 0;
+    int pair_steps = 1, pair_rows = 14, pair_zc = 0;
     DevBuf spare[2];
     CUtensorMap pmP[4], pmQ[4], pmC;
     int pm_rows = 0;
@@ -1935,13 +1935,13 @@ VIRS_EXPORT virs_status virs_set_time_blocking(virs_sim *s, int steps_per_pass, 
 {
     if (!s) return fail(VIRS_E_ARG, "virs_set_time_blocking: null");
     if (steps_per_pass != 1 && steps_per_pass != 2) return fail(VIRS_E_ARG, "steps per pass must be 1 or 2");
-    if (tile_rows != 0 && tile_rows != 16 && tile_rows != 32)
-        return fail(VIRS_E_ARG, "two-step tile rows must be 16 or 32");
+    if (tile_rows != 0 && tile_rows != 12 && tile_rows != 14 && tile_rows != 16 && tile_rows != 32)
+        return fail(VIRS_E_ARG, "two-step tile rows must be 12, 14, 16 or 32");
     if (planes < 0 || planes > 4096) return fail(VIRS_E_ARG, "planes per block must be 0..4096");
     VIRS_TRY(use_device(s));
     VIRS_TRY(wait_done(s));
     s->pair_steps = steps_per_pass;
-    s->pair_rows = tile_rows ? tile_rows : 16;
+    s->pair_rows = tile_rows ? tile_rows : 14;
     s->pair_zc = planes;
     s->pm_rows = 0;
     s->pair_nomem = false;
@@ -1994,7 +1994,7 @@ struct TuneKey {
 // the single-step tiling, and the two-step settings when those won
 struct TunePick {
     virs_tiling t{};
-    int pair_steps = 1, pair_rows = 16, pair_zc = 0;
+    int pair_steps = 1, pair_rows = 14, pair_zc = 0;
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TunePick> g_tune;
@@ -2087,39 +2087,49 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
             s->depth = pick.t.pipeline_depth;
             s->zc = pick.t.planes_per_block;
             s->maps_rows = 0;
-            const int prow_c[] = {16, 32}, pplanes_c[] = {32, 42, 51, 64, 102, 128};
-            for (int r : prow_c)
-                for (int pl : pplanes_c) {
-                    if (st != VIRS_OK) break;
-                    s->pair_steps = 2;
-                    s->pair_rows = r;
-                    s->pair_zc = pl;
-                    s->pm_rows = 0;
-                    if ((st = ready_to_run(s)) != VIRS_OK || (st = ready_pairs(s)) != VIRS_OK) break;
-                    if (!pair_on(s)) break; // no room for the spare buffers, or a grid too small
-                    if ((st = sync_border_planes(s, s->stream)) != VIRS_OK) break;
-                    cudaError_t e = enqueue_quad(s, s->cur, s->stream);
-                    cudaEventRecord(e0, s->stream);
-                    for (uint32_t k = 0; k < quads && e == cudaSuccess; ++k) e = enqueue_quad(s, s->cur, s->stream);
-                    cudaEventRecord(e1, s->stream);
-                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-                    float ms = 0;
-                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-                    if (e != cudaSuccess) {
-                        st = cuda_fail(e, "autotune trial (two steps per pass)");
-                        break;
-                    }
-                    if ((st = check_err(s)) != VIRS_OK) break;
-                    const float per = ms / (4.f * quads);
-                    if (per < best_ms) {
-                        best_ms = per;
-                        pick.t.ms_per_step = per;
-                        pick.pair_steps = 2;
-                        pick.pair_rows = r;
-                        pick.pair_zc = pl;
-                    }
-                    if ((st = reset_state(s)) != VIRS_OK) break;
+            // Each candidate is timed twice, in forward and then reverse
+            // order: a sustained load brings the GPU to its power cap within
+            // about a second, which would favour the candidates timed first.
+            std::vector<std::pair<int, int>> cand;
+            for (int r : {14, 16, 12})
+                for (int pl : {32, 42, 64, 102}) cand.emplace_back(r, pl);
+            bool room = true;
+            for (size_t c = 0; c < 2 * cand.size() && room; ++c) {
+                const int r = cand[c < cand.size() ? c : 2 * cand.size() - 1 - c].first;
+                const int pl = cand[c < cand.size() ? c : 2 * cand.size() - 1 - c].second;
+                if (st != VIRS_OK) break;
+                s->pair_steps = 2;
+                s->pair_rows = r;
+                s->pair_zc = pl;
+                s->pm_rows = 0;
+                if ((st = ready_to_run(s)) != VIRS_OK || (st = ready_pairs(s)) != VIRS_OK) break;
+                if (!pair_on(s)) { // no room for the spare buffers, or a grid too small
+                    room = false;
+                    break;
                 }
+                if ((st = sync_border_planes(s, s->stream)) != VIRS_OK) break;
+                cudaError_t e = enqueue_quad(s, s->cur, s->stream);
+                cudaEventRecord(e0, s->stream);
+                for (uint32_t k = 0; k < quads && e == cudaSuccess; ++k) e = enqueue_quad(s, s->cur, s->stream);
+                cudaEventRecord(e1, s->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e != cudaSuccess) {
+                    st = cuda_fail(e, "autotune trial (two steps per pass)");
+                    break;
+                }
+                if ((st = check_err(s)) != VIRS_OK) break;
+                const float per = ms / (4.f * quads);
+                if (per < best_ms) {
+                    best_ms = per;
+                    pick.t.ms_per_step = per;
+                    pick.pair_steps = 2;
+                    pick.pair_rows = r;
+                    pick.pair_zc = pl;
+                }
+                if ((st = reset_state(s)) != VIRS_OK) break;
+            }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

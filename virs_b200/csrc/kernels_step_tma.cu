@@ -797,12 +797,18 @@ cudaError_t pair3(const StepArgs &a, const TmaMaps &m, void *zout, void *wout, i
     return cudaGetLastError();
 }
 
-// two planes in flight (a 32-row FP32 tile at three would not fit in
-// shared memory)
+// planes in flight per tile height: as many as two FP32 blocks per SM
+// leave room for (12 rows: 4, 14 rows: 3, 16 rows: 2); the 32-row tile fills
+// an SM alone and keeps 2
 template <typename T>
 cudaError_t pair1(int rows, const StepArgs &a, const TmaMaps &m, void *zout, void *wout, int *err, cudaStream_t s)
 {
-    return rows == 32 ? pair3<T, 32, 2>(a, m, zout, wout, err, s) : pair3<T, 16, 2>(a, m, zout, wout, err, s);
+    switch (rows) {
+    case 12: return pair3<T, 12, 4>(a, m, zout, wout, err, s);
+    case 14: return pair3<T, 14, 3>(a, m, zout, wout, err, s);
+    case 32: return pair3<T, 32, 2>(a, m, zout, wout, err, s);
+    default: return pair3<T, 16, 2>(a, m, zout, wout, err, s);
+    }
 }
 
 } // namespace
