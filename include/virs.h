@@ -364,11 +364,15 @@ typedef struct virs_tiling {
  * times `trial_steps` steps of each TMA variant (tile rows 4/8/16, depth
  * 1..3, 8..64 planes per block) and then of the two-step variants (time
  * blocking: tile rows 14/16/12, 32..102 planes per block, trial_steps
- * rounded up to a multiple of four, at least eight, each timed twice) on
- * this handle's own grid and keeps the fastest:
- * the tiling it returns, and the steps per pass that virs_get_time_blocking
- * reports.  The simulation is then back at rest.  Results are cached per
- * device, storage and grid shape for the life of the process. */
+ * rounded up to a multiple of four, at least eight) on this handle's own
+ * grid and keeps the fastest: the tiling it returns, and the steps per pass
+ * that virs_get_time_blocking reports.  Every candidate is timed twice, in
+ * forward and then reverse order, because a sustained load reaches the
+ * GPU's power cap within about a second and would favour the candidates
+ * timed first.  The simulation is then back at rest.  Results are cached
+ * per device, storage and grid shape for the life of the process.
+ * virs_batch_autotune does the same for a batch's tilings (one tile per
+ * block or persistent). */
 virs_status virs_autotune(virs_sim *sim, uint32_t trial_steps, virs_tiling *best);
 virs_status virs_get_tiling(const virs_sim *sim, virs_tiling *out);
 

@@ -2046,40 +2046,49 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
         VIRS_CUDA(cudaEventCreate(&e0));
         VIRS_CUDA(cudaEventCreate(&e1));
         float best_ms = 1e30f;
-        const int rows_c[] = {4, 8, 16}, depth_c[] = {1, 2, 3}, planes_c[] = {8, 16, 32, 64};
+        // Every candidate is timed twice, in forward and then reverse order:
+        // a sustained load brings the GPU to its power cap within about a
+        // second, which would favour the candidates timed first.
+        struct Cand {
+            int d, r, pl;
+        };
+        std::vector<Cand> sc;
+        for (int d : {1, 2, 3})
+            for (int r : {4, 8, 16})
+                for (int pl : {8, 16, 32, 64}) sc.push_back({d, r, pl});
         virs_status st = VIRS_OK;
-        for (int d : depth_c)
-            for (int r : rows_c)
-                for (int pl : planes_c) {
-                    if (st != VIRS_OK) break;
-                    s->tile_rows = r;
-                    s->depth = d;
-                    s->zc = pl;
-                    s->maps_rows = 0;
-                    if ((st = ready_to_run(s)) != VIRS_OK) break;
-                    // one untimed step, then trial_steps timed ones
-                    cudaError_t e = enqueue_step(s, s->cur, s->stream);
-                    s->cur ^= 1;
-                    cudaEventRecord(e0, s->stream);
-                    for (uint32_t k = 0; k < trial_steps && e == cudaSuccess; ++k) {
-                        e = enqueue_step(s, s->cur, s->stream);
-                        s->cur ^= 1;
-                    }
-                    cudaEventRecord(e1, s->stream);
-                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-                    float ms = 0;
-                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-                    if (e != cudaSuccess) {
-                        st = cuda_fail(e, "autotune trial");
-                        break;
-                    }
-                    if ((st = check_err(s)) != VIRS_OK) break;
-                    if (ms / trial_steps < best_ms) {
-                        best_ms = ms / trial_steps;
-                        pick.t = {r, pl, d, ms / trial_steps};
-                    }
-                    if ((st = reset_state(s)) != VIRS_OK) break;
-                }
+        for (size_t c = 0; c < 2 * sc.size(); ++c) {
+            const Cand &cd = sc[c < sc.size() ? c : 2 * sc.size() - 1 - c];
+            const int d = cd.d, r = cd.r, pl = cd.pl;
+            if (st != VIRS_OK) break;
+            s->tile_rows = r;
+            s->depth = d;
+            s->zc = pl;
+            s->maps_rows = 0;
+            if ((st = ready_to_run(s)) != VIRS_OK) break;
+            // one untimed step, then trial_steps timed ones
+            cudaError_t e = enqueue_step(s, s->cur, s->stream);
+            s->cur ^= 1;
+            cudaEventRecord(e0, s->stream);
+            for (uint32_t k = 0; k < trial_steps && e == cudaSuccess; ++k) {
+                e = enqueue_step(s, s->cur, s->stream);
+                s->cur ^= 1;
+            }
+            cudaEventRecord(e1, s->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                st = cuda_fail(e, "autotune trial");
+                break;
+            }
+            if ((st = check_err(s)) != VIRS_OK) break;
+            if (ms / trial_steps < best_ms) {
+                best_ms = ms / trial_steps;
+                pick.t = {r, pl, d, ms / trial_steps};
+            }
+            if ((st = reset_state(s)) != VIRS_OK) break;
+        }
         // two steps per pass (groups of four steps), with the best single-step
         // tiling for the steps that do not fill a group
         if (st == VIRS_OK) {
@@ -2460,35 +2469,44 @@ VIRS_EXPORT virs_status virs_batch_autotune(virs_batch *b, uint32_t trial_steps,
     bool pick_persistent = false;
     float best_ms = 1e30f;
     virs_status st = VIRS_OK;
+    // every candidate timed twice, in forward and then reverse order (the
+    // power cap would favour the candidates timed first)
+    struct Cand {
+        int pers, d, r, pl;
+    };
+    std::vector<Cand> cand;
     for (int pers : {0, 1})
-    for (int d : {1, 2, 3})
-        for (int r : {4, 8, 16})
-            for (int pl : {8, 16, 32, 64}) {
-                if (st != VIRS_OK) break;
-                b->rows = r;
-                b->depth = d;
-                b->planes = pl;
-                b->persistent = pers != 0;
-                if ((st = batch_build(b)) != VIRS_OK) break;
-                if ((st = batch_steps(b, 1, b->stream, false)) != VIRS_OK) break;
-                cudaEventRecord(e0, b->stream);
-                if ((st = batch_steps(b, trial_steps, b->stream, false)) != VIRS_OK) break;
-                cudaEventRecord(e1, b->stream);
-                cudaError_t e = cudaEventSynchronize(e1);
-                float ms = 0;
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-                if (e != cudaSuccess) {
-                    st = cuda_fail(e, "batch autotune trial");
-                    break;
-                }
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    pick = {r, pl, d, ms / trial_steps};
-                    pick_persistent = pers != 0;
-                }
-                for (virs_sim *s : b->mem)
-                    if ((st = reset_state(s)) != VIRS_OK) break;
-            }
+        for (int d : {1, 2, 3})
+            for (int r : {4, 8, 16})
+                for (int pl : {8, 16, 32, 64}) cand.push_back({pers, d, r, pl});
+    for (size_t c = 0; c < 2 * cand.size(); ++c) {
+        const Cand &cd = cand[c < cand.size() ? c : 2 * cand.size() - 1 - c];
+        const int pers = cd.pers, d = cd.d, r = cd.r, pl = cd.pl;
+        if (st != VIRS_OK) break;
+        b->rows = r;
+        b->depth = d;
+        b->planes = pl;
+        b->persistent = pers != 0;
+        if ((st = batch_build(b)) != VIRS_OK) break;
+        if ((st = batch_steps(b, 1, b->stream, false)) != VIRS_OK) break;
+        cudaEventRecord(e0, b->stream);
+        if ((st = batch_steps(b, trial_steps, b->stream, false)) != VIRS_OK) break;
+        cudaEventRecord(e1, b->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            st = cuda_fail(e, "batch autotune trial");
+            break;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            pick = {r, pl, d, ms / trial_steps};
+            pick_persistent = pers != 0;
+        }
+        for (virs_sim *s : b->mem)
+            if ((st = reset_state(s)) != VIRS_OK) break;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != VIRS_OK) return st;
