@@ -318,7 +318,9 @@ virs_status virs_energy(virs_sim *sim, double *out);
  * handle's stream); nothing waits for it.  The first call on a device looks
  * up the array's address (cudaGetSymbolAddress): make it before any stream
  * capture.  All calls share the array, so calls whose work overlaps on the
- * GPU race. */
+ * GPU race: callers serialise them.  The call records the handle's
+ * completion event on the stream it used, so virs_synchronize and
+ * virs_destroy wait for its reads of the fields. */
 #define VIRS_ENERGY_MAX_PLANES 8192
 virs_status virs_energy_noalloc(virs_sim *sim, double *d_out, void *stream);
 

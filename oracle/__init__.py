@@ -38,10 +38,25 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
+def reference_tree() -> Path | None:
+    """The Snipet/VIRS source tree the reference-built checkers compile from:
+    $VIRS_REFERENCE_TREE when set (it must then be that tree), else a
+    directory named `reference` beside this repository, else None."""
+    env = os.environ.get("VIRS_REFERENCE_TREE")
+    if env:
+        if not Path(env, "src/simulator/biquad.cpp").exists():
+            raise FileNotFoundError(f"VIRS_REFERENCE_TREE={env} is not the Snipet/VIRS source tree "
+                                    "(no src/simulator/biquad.cpp)")
+        return Path(env)
+    sibling = HERE.parent.parent / "reference"
+    return sibling if Path(sibling, "src/simulator/biquad.cpp").exists() else None
+
+
 def build_ref() -> bool:
-    """Compile the reference-built checkers when the reference tree exists."""
-    ref = os.environ.get("VIRS_REFERENCE_TREE", "/root/reference")
-    if not Path(ref, "src/simulator/biquad.cpp").exists():
+    """Compile the reference-built checkers when the reference tree exists
+    (reference_tree()); False when there is none."""
+    ref = reference_tree()
+    if ref is None:
         return False
     subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
     return True
@@ -403,6 +418,18 @@ def round16(x, storage: int):
     out = np.empty_like(x)
     lib().vo_round16(x.ctypes.data, out.ctypes.data, C.c_uint64(x.size), C.c_int32(storage))
     return out
+
+
+def init_sphere(p, shape, center, radius: int, pressure: float, zero_outside: bool = True):
+    """initSphereKernel (init_sphere.cu:4-25) applied in place to the flat
+    float32 field `p` of `shape` (nx, ny, nz); returns p."""
+    nx, ny, nz = shape
+    assert p.dtype == np.float32 and p.flags.c_contiguous and p.size == nx * ny * nz
+    cx, cy, cz = (int(c) for c in center)
+    lib().vo_init_sphere(C.c_void_p(p.ctypes.data), C.c_uint64(nx), C.c_uint64(ny), C.c_uint64(nz), C.c_uint64(cx),
+                         C.c_uint64(cy), C.c_uint64(cz), C.c_uint64(int(radius)), C.c_float(pressure),
+                         C.c_int(int(zero_outside)))
+    return p
 
 
 def energy(shape, flags, p, pprev, lambda2: float) -> float:

@@ -484,6 +484,28 @@ static inline float vo_round_f16(float x)
     return x;
 }
 
+/* initSphereKernel (src/simulator/init_sphere.cu:4-25), one loop iteration
+ * per thread of its 3D grid: every voxel (x, y, z) of the nx*ny*nz field
+ * whose integer squared distance to (cx, cy, cz) is at most r^2 (the
+ * launcher passes radius * radius, init_sphere.cu:44) takes `pressure`;
+ * with zero_outside every other voxel takes 0, else it keeps its value.
+ * Distances are formed from unsigned differences as the kernel does. */
+VO_API void vo_init_sphere(float *p, uint64_t nx, uint64_t ny, uint64_t nz, uint64_t cx, uint64_t cy, uint64_t cz,
+                           uint64_t radius, float pressure, int zero_outside)
+{
+    const uint64_t r2 = radius * radius;
+    for (uint64_t z = 0; z < nz; ++z)
+        for (uint64_t y = 0; y < ny; ++y)
+            for (uint64_t x = 0; x < nx; ++x) {
+                const uint64_t dx = x > cx ? x - cx : cx - x;
+                const uint64_t dy = y > cy ? y - cy : cy - y;
+                const uint64_t dz = z > cz ? z - cz : cz - z;
+                const uint64_t i = (z * ny + y) * nx + x;
+                if (dx * dx + dy * dy + dz * dz <= r2) p[i] = pressure;
+                else if (zero_outside) p[i] = 0.f;
+            }
+}
+
 /* the storage rounding on its own (tests) */
 VO_API void vo_round16(const float *in, float *out, uint64_t n, int32_t storage)
 {

@@ -247,21 +247,40 @@ def test_energy_monitor_matches_oracle_and_is_conserved():
     sim.close()
 
 
-@pytest.mark.parametrize("storage", [capi.STORAGE_F16, capi.STORAGE_BF16])
-def test_16bit_storage_error_is_bounded(storage):
-    """16-bit pressure storage, FP32 update: the receiver IR against the FP64
-    oracle stays within the stated bound (FP16 5e-2, BF16 2e-1 at 600 steps)."""
+# Receiver-IR error of 16-bit storage against the FP64 oracle on the
+# 160x120x100 room over 600 steps, as measured (the GPU path equals the
+# rounding oracle bit for bit, test_16bit_storage_bit_exact): FP16 5.6e-3,
+# BF16 3.0e-2.  The regression bound is 1.25x the measured value; the
+# accuracy target of 1e-3 is not met and is kept as a strict expected
+# failure, so that a form that meets it shows up as an unexpected pass.
+SMALL_16BIT_MEASURED = {capi.STORAGE_F16: 5.6e-3, capi.STORAGE_BF16: 3.0e-2}
+IR_TARGET = 1e-3
+
+
+def _small_16bit_error(storage):
     sc = scenes.plain_small(steps=600)
     g = oracle_grid(sc)
     want64 = oracle_scene(sc, g).run(sc.steps, f64=True)
     sim, _ = scenes.build_simulation(sc, storage=storage)
     sim.run(sc.steps)
     got = sim.ir()
+    sim.close()
+    assert np.isfinite(got).all()
     err = rel_l2(got, want64)
     print(f"storage {storage}: IR rel-L2 vs FP64 = {err:.3e}")
-    assert np.isfinite(got).all()
-    assert err < (5e-2 if storage == capi.STORAGE_F16 else 2e-1)
-    sim.close()
+    return err
+
+
+@pytest.mark.parametrize("storage", [capi.STORAGE_F16, capi.STORAGE_BF16])
+def test_16bit_storage_error_regression(storage):
+    assert _small_16bit_error(storage) <= 1.25 * SMALL_16BIT_MEASURED[storage]
+
+
+@pytest.mark.xfail(strict=True, reason="16-bit storage: measured FP16 5.6e-3, BF16 3.0e-2 over 600 steps "
+                                       "against the 1e-3 target (rounding of every stored value, every step)")
+@pytest.mark.parametrize("storage", [capi.STORAGE_F16, capi.STORAGE_BF16])
+def test_16bit_storage_error_meets_target(storage):
+    assert _small_16bit_error(storage) <= IR_TARGET
 
 
 def _storage_scale(sc) -> float:
@@ -494,4 +513,40 @@ def test_wide_grid_skips_zero_code_planes_bit_exact(storage, rows, planes):
     if storage != capi.STORAGE_F32:
         want_p[np.abs(want_p) < np.finfo(np.float32).tiny] *= np.float32(0.0)
     assert np.array_equal(p.view(np.uint32), want_p.view(np.uint32))
+    sim.close()
+
+
+@pytest.mark.parametrize("storage", [capi.STORAGE_F32, capi.STORAGE_BF16])
+def test_init_sphere_matches_oracle(storage):
+    """virs_init_pressure_sphere against the oracle's restatement of
+    initSphereKernel (init_sphere.cu:4-25): spheres inside the grid, cut by
+    its faces and of radius 0, with and without zeroing the rest.  The
+    library keeps the domain border at 0 (the step never writes it, so a
+    pressure there would stay for ever); every interior voxel must equal the
+    oracle's, and p^{n-1} is left alone, as in the reference."""
+    shape = (37, 29, 23)
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    rng = np.random.default_rng(11)
+    sim = capi.Simulation(storage=storage, storage_scale=1.0 if storage else 0.0)
+    sim.set_grid(shape, 0.05, np.zeros(n, np.uint8))
+    sim.classify()
+    sim.start(1)
+    interior = np.zeros((nz, ny, nx), bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    interior = interior.reshape(-1)
+    cases = [((18, 14, 11), 5, 1.25, True), ((1, 2, 3), 7, -0.5, False), ((36, 28, 22), 11, 2.0, False),
+             ((10, 10, 10), 0, 3.0, False), ((0, 14, 11), 3, 0.75, True)]
+    for center, radius, value, zero in cases:
+        base = rng.integers(-8, 8, n).astype(np.float32) / 4      # exact in BF16
+        base[~interior] = 0
+        prev = rng.integers(-8, 8, n).astype(np.float32) / 4
+        prev[~interior] = 0
+        sim.set_pressure(base, prev)
+        sim.init_pressure_sphere(*center, radius, value, zero)
+        got, got_prev = sim.pressure(prev=True)
+        want = oracle.init_sphere(base.copy(), shape, center, radius, value, zero)
+        assert np.array_equal(got[interior], want[interior]), (center, radius)
+        assert not got[~interior].any()
+        assert np.array_equal(got_prev, prev)
     sim.close()

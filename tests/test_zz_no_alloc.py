@@ -16,10 +16,13 @@ pytestmark = pytest.mark.gpu
 REL_TOL = 1e-9      # the tolerance of the other energy-monitor checks
 
 
-def test_energy_noalloc_matches_energy_on_two_calls():
+@pytest.mark.parametrize("storage", [capi.STORAGE_F32, capi.STORAGE_BF16, capi.STORAGE_F16])
+def test_energy_noalloc_matches_energy_on_two_calls(storage):
+    """FP32, BF16 and FP16 fields: each storage type has its own conversion
+    and the inverse scale squared in the sum."""
     import torch
     sc = scenes.plain_small(steps=300)
-    sim, _ = scenes.build_simulation(sc)
+    sim, _ = scenes.build_simulation(sc, storage=storage)
     out = torch.zeros(2, dtype=torch.float64, device="cuda:0")   # the caller's output buffer
     side = torch.cuda.Stream()
     for k in range(2):
@@ -34,7 +37,7 @@ def test_energy_noalloc_matches_energy_on_two_calls():
         got = float(out[k].item())
         assert want > 0
         assert abs(got - want) <= REL_TOL * abs(want), (k, got, want)
-    sim.close()
+    sim.close()                                                   # waits for the reads on `side` too
 
 
 def test_energy_noalloc_rejects_grids_beyond_the_scratch():

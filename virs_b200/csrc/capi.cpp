@@ -1076,6 +1076,8 @@ VIRS_EXPORT virs_status virs_destroy(virs_sim *s)
 {
     if (!s) return VIRS_OK;
     cudaSetDevice(s->prm.device);
+    // the last work queued for the handle, on its own stream or a caller's
+    if (s->done) cudaEventSynchronize(s->done);
     cudaStreamSynchronize(s->stream);
     delete s;
     return VIRS_OK;
@@ -2196,6 +2198,7 @@ virs_status energy_inputs(virs_sim *s, void *stream, EnergyInputs *in)
     in->lambda2 = (double)s->c2dt2 * (double)s->inv_h2;
     in->scale2 = (double)s->inv_scale * (double)s->inv_scale;
     in->stream = stream ? (cudaStream_t)stream : s->stream;
+    in->done = s->done;
     if (in->stream != s->stream) {
         VIRS_CUDA(cudaEventRecord(s->done, s->stream));
         VIRS_CUDA(cudaStreamWaitEvent(in->stream, s->done, 0));

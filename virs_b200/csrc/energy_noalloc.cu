@@ -16,6 +16,8 @@
 // point runs on it (make that first call before any stream capture).  All
 // calls share the array: every call writes each partial it reads, so no
 // state carries over, but calls whose work overlaps on the GPU race on it.
+// The call records the handle's completion event on the stream it used, so
+// virs_synchronize and virs_destroy wait for its reads of the fields.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -143,5 +145,9 @@ VIRS_EXPORT virs_status virs_energy_noalloc(virs_sim *sim, double *d_out, void *
     }
     k_energy_planes_sum<<<1, 32, 0, in.stream>>>(scratch, in.nz, in.scale2, d_out);
     VIRS_CUDA(cudaGetLastError());
+    // the handle's completion event now follows these reads of its fields, so
+    // virs_synchronize and virs_destroy wait for them (also on a caller's
+    // stream) before the fields can be freed
+    VIRS_CUDA(cudaEventRecord(in.done, in.stream));
     return VIRS_OK;
 }

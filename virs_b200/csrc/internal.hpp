@@ -272,6 +272,7 @@ struct EnergyInputs {
     int storage, device;
     double lambda2, scale2;
     cudaStream_t stream;
+    cudaEvent_t done; // the handle's completion event, recorded after the launches
 };
 virs_status energy_inputs(virs_sim *sim, void *stream, EnergyInputs *out);
 

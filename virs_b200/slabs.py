@@ -63,10 +63,18 @@ class _DeviceBytes:
                                          "strides": None}
 
 
-def device_bytes(ptr: int, n: int):
-    """A uint8 CUDA tensor viewing `n` bytes at device address `ptr`."""
+def device_bytes(ptr: int, n: int, device: int | None = None):
+    """A uint8 CUDA tensor viewing `n` bytes at device address `ptr` on GPU
+    `device` (None = the current one).  The view aliases the memory: a copy
+    into it writes `ptr` (torch would otherwise copy a buffer of another GPU
+    to the current one, and a write would go to that copy)."""
     import torch
-    return torch.as_tensor(_DeviceBytes(ptr, n), device="cuda")
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else int(device))
+    with torch.cuda.device(dev):
+        t = torch.as_tensor(_DeviceBytes(ptr, n), device=dev)
+    if t.data_ptr() != ptr:
+        raise RuntimeError(f"device_bytes: the view of {ptr:#x} on {dev} does not alias it")
+    return t
 
 
 def exchange(first, last, ghost_lo, ghost_hi, rank: int, world: int, group=None) -> None:
@@ -90,16 +98,18 @@ def exchange(first, last, ghost_lo, ghost_hi, rank: int, world: int, group=None)
 
 
 def exchange_local(sims) -> None:
-    """The same exchange between slab handles of one process (one GPU or
-    several), as copies on the current torch stream: sims[r] owns the r-th
-    range from the bottom."""
+    """The same exchange between slab handles of one process, as copies on
+    the current torch stream: sims[r] owns the r-th range from the bottom.
+    Each plane is viewed on its own handle's GPU, so handles may sit on
+    different GPUs (a copy between two GPUs is a peer copy)."""
     planes = [s.slab_planes() for s in sims]
+    dev = [int(s.params.device) for s in sims]
     for r in range(len(sims)):
         nb = planes[r][4]
         if r > 0:
-            device_bytes(planes[r][2], nb).copy_(device_bytes(planes[r - 1][1], planes[r - 1][4]))
+            device_bytes(planes[r][2], nb, dev[r]).copy_(device_bytes(planes[r - 1][1], planes[r - 1][4], dev[r - 1]))
         if r + 1 < len(sims):
-            device_bytes(planes[r][3], nb).copy_(device_bytes(planes[r + 1][0], planes[r + 1][4]))
+            device_bytes(planes[r][3], nb, dev[r]).copy_(device_bytes(planes[r + 1][0], planes[r + 1][4], dev[r + 1]))
 
 
 class SlabRun:
@@ -117,7 +127,9 @@ class SlabRun:
         stream = torch.cuda.current_stream().cuda_stream
         for _ in range(steps):
             first, last, glo, ghi, nb = self.sim.slab_planes()
-            exchange(device_bytes(first, nb), device_bytes(last, nb), device_bytes(glo, nb), device_bytes(ghi, nb),
+            d = int(self.sim.params.device)
+            exchange(device_bytes(first, nb, d), device_bytes(last, nb, d), device_bytes(glo, nb, d),
+                     device_bytes(ghi, nb, d),
                      self.rank, self.world, self.group)
             self.sim.run(1, stream=stream)
 
