@@ -209,7 +209,9 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
     total = warm + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
     total += args.sustained_steps if want_e2e else 0
     sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
+    t_pre = time.perf_counter()
     tiling = sim.autotune(args.tune_steps) if args.tune_steps else sim.tiling()
+    tune_s = time.perf_counter() - t_pre
     if args.steps_per_pass:
         # forced: single steps, or two steps per pass with the autotuner's
         # two-step tiling when it chose one, else --pair-tiling
@@ -219,12 +221,15 @@ def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
         sim.set_time_blocking(args.steps_per_pass, rows, planes)
     sim.run(warm, stream.cuda_stream)
     torch.cuda.synchronize()
+    pre_s = time.perf_counter() - t_pre
     if dist:
         dist.barrier()
     with Clocks(gpu_uuid(dev)) as clk:
         ms = time_run(sim, args.steps, stream)
     ms = max_over_ranks(ms, dist, f"cuda:{dev}")
     out = {"ms": ms, "clocks": clk.summary(), "meta": meta,
+           "warmup": {"steps": warm, "autotune_s": round(tune_s, 2), "seconds": round(pre_s, 2),
+                      "autotune_trial_steps": args.tune_steps},
            "tiling": {"tile_rows": tiling.tile_rows, "planes_per_block": tiling.planes_per_block,
                       "pipeline_depth": tiling.pipeline_depth},
            "time_blocking": sim.time_blocking()}
@@ -313,17 +318,25 @@ def bench_batch(storage, args, stream, dev, dist=None):
             "ir_finite": ok, "launches_per_step": 3}
 
 
+CPU_CROP_PLANES = 16   # planes of the hall crop both CPU figures time
+
+
 def cpu_sample(shape, steps_budget_s, threads):
-    """The oracle's FP32 step on a crop of the hall (same x, y extent, fewer
-    planes), timed on the host; returns (Gvox/s, description)."""
+    """The oracle's FP32 step on a crop of the hall (same x, y extent,
+    CPU_CROP_PLANES planes), timed on the host in chunks of about a second
+    until the budget is spent; returns (Gvox/s, description, seconds).  The
+    main arm's cpu_baseline and the reference arm both report this figure.
+    The scene's absorbers are designed with the oracle's FP64 designs, so
+    this leg runs no part of the library."""
     import oracle
     from virs_b200 import scenes
     sys.path.insert(0, str(ROOT / "tests"))
     from helpers import oracle_grid, oracle_scene
     oracle.set_threads(threads)
     nx, ny, nz = shape
-    nzc = 16
-    sc = scenes.large_hall(steps=64, size=(nx, ny, nzc))
+    nzc = CPU_CROP_PLANES
+    with scenes.designs(oracle.design_first_order, oracle.design_octave_cascade):
+        sc = scenes.large_hall(steps=64, size=(nx, ny, nzc))
     g = oracle_grid(sc)
     osc = oracle_scene(sc, g)
     n = nx * ny * nzc
@@ -408,7 +421,14 @@ def run_virs(args):
         "unit": "Gvoxel-updates/s",
         "n_gpus": world,
         "steps": args.steps,
-        "warmup": args.warmup,
+        # untimed steps run right before the timed region (at least the 64
+        # that build and launch both step graphs); before them the autotuner
+        # timed its candidates
+        "warmup": r32["warmup"]["steps"],
+        "warmup_detail": dict(r32["warmup"], requested=args.warmup,
+                              note="autotuner: every candidate tiling timed twice for autotune_trial_steps steps "
+                                   "(at least 8 for two-step candidates), then the simulation restarted from rest; "
+                                   "seconds = autotuner + warm-up steps"),
         "ms_per_step": r32["ms"] / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
@@ -493,43 +513,17 @@ def run_virs(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's step (the
+    reference's own CPU build cannot be compiled: oneTBB, Embree,
+    tinyobjloader, kfr and AudioFile are absent) on all host threads, timed
+    exactly as the main arm's cpu_baseline: the same crop of the hall, the
+    same chunks, the same budget.  Nothing of the library is loaded."""
     rank, world, _ = env_rank()
     if rank != 0:
         return
     th = host_threads()
-    # size the crop so that warmup + steps fit in about two minutes
-    budget = 120.0 / max(args.steps + args.warmup, 1)
-    import oracle
-    from virs_b200 import scenes
-    sys.path.insert(0, str(ROOT / "tests"))
-    from helpers import oracle_grid, oracle_scene
-    oracle.set_threads(th)
     nx, ny, nz = args.size
-    nzc = 8
-    sc = scenes.large_hall(steps=args.steps + args.warmup + 2, size=(nx, ny, nzc))
-    g = oracle_grid(sc)
-    osc = oracle_scene(sc, g)
-    n = nx * ny * nzc
-    st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
-    t0 = time.perf_counter()
-    osc.run(1, state=st)
-    per = time.perf_counter() - t0
-    if per > budget:           # shrink to fewer rows
-        frac = max(budget / per, 1 / ny)
-        nyc = max(8, int(ny * frac))
-        sc = scenes.large_hall(steps=args.steps + args.warmup + 2, size=(nx, nyc, nzc))
-        g = oracle_grid(sc)
-        osc = oracle_scene(sc, g)
-        n = nx * nyc * nzc
-        st = (np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(g["bidx"].size * 12 + 1, np.float32))
-        desc = f"{nx}x{nyc}x{nzc} crop of the hall"
-    else:
-        desc = f"{nx}x{ny}x{nzc} crop of the hall"
-    osc.run(args.warmup, state=st, step0=1)
-    t0 = time.perf_counter()
-    osc.run(args.steps, state=st, step0=1 + args.warmup)
-    secs = time.perf_counter() - t0
-    gv = n * args.steps / secs / 1e9
+    gv, desc, secs = cpu_sample(tuple(args.size), max(10.0, args.cpu_seconds), th)
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -538,20 +532,24 @@ def run_reference(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": secs * 1e3 / args.steps,
+        "ms_per_step": nx * ny * CPU_CROP_PLANES / (gv * 1e9) * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded hall geometry)",
-        "config": {"workload": "large_hall %dx%dx%d FP32 (CPU arm runs a crop; one step = one time step of the crop)"
-                               % tuple(args.size)},
+        "config": {"workload": "large_hall %dx%dx%d FP32 (the CPU arm runs a %d-plane crop; one step = one time step "
+                               "of the crop)" % (nx, ny, nz, CPU_CROP_PLANES)},
         "cpu_baseline": {"value": round(gv, 4), "unit": "Gvoxel-updates/s", "cores": th, "kind": "port",
-                         "sample": f"{args.steps} steps of a {desc}; the reference CPU build (oneTBB, Embree, "
-                                   "tinyobjloader, kfr, AudioFile) cannot be compiled here, so this is the CPU "
-                                   "restatement of its step"},
+                         "sample": f"{desc}, {secs:.1f} s; the reference CPU build (oneTBB, Embree, tinyobjloader, "
+                                   "kfr, AudioFile) cannot be compiled here, so this is the CPU restatement of its step"},
         "e2e": {"value": round(gv, 4), "unit": "Gvoxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        maps = Path("/proc/self/maps").read_text()
+        line["config"]["libvirs_b200_mapped"] = "libvirs_b200" in maps
+    except OSError:
+        pass
     print(json.dumps(line), flush=True)
 
 

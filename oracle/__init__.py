@@ -420,6 +420,21 @@ def round16(x, storage: int):
     return out
 
 
+def design_first_order(fs: float, reflection: float, fc: float) -> np.ndarray:
+    """The library's first-order absorber design restated in FP64 ({b0, b1, b2, a1, a2})."""
+    out = np.zeros(5, np.float64)
+    lib().vo_design_first_order(C.c_double(fs), C.c_double(reflection), C.c_double(fc), C.c_void_p(out.ctypes.data))
+    return out
+
+
+def design_octave_cascade(fs: float, alpha) -> np.ndarray:
+    """The library's three-section octave cascade restated in FP64 ([3][5])."""
+    a = np.ascontiguousarray(alpha, np.float64)
+    out = np.zeros(15, np.float64)
+    lib().vo_design_octave_cascade(C.c_double(fs), C.c_void_p(a.ctypes.data), C.c_void_p(out.ctypes.data))
+    return out.reshape(3, 5)
+
+
 def init_sphere(p, shape, center, radius: int, pressure: float, zero_outside: bool = True):
     """initSphereKernel (init_sphere.cu:4-25) applied in place to the flat
     float32 field `p` of `shape` (nx, ny, nz); returns p."""

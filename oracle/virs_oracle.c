@@ -248,41 +248,81 @@ VO_API void vo_classify(uint64_t nx, uint64_t ny, uint64_t nz, int W, const uint
     if (bmat) memset(bmat, 0, n);
     if (bd2) memset(bd2, 0, n * sizeof(uint16_t));
     const int lim = W * W + 1;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(vo_get_threads())
-    for (int64_t z = 1; z < (int64_t)nz - 1; ++z)
-        for (int64_t y = 1; y < (int64_t)ny - 1; ++y)
-            for (int64_t x = 1; x < (int64_t)nx - 1; ++x) {
-                uint64_t id = ((uint64_t)z * ny + (uint64_t)y) * nx + (uint64_t)x;
-                if (flags_in[id] != 0) continue;
-                int best = 1 << 30;
-                uint64_t bestn = 0;
-                for (int dz = -W; dz <= W; ++dz) {
-                    int64_t zz = z + dz;
-                    if (zz < 0 || zz >= (int64_t)nz) continue;
-                    for (int dy = -W; dy <= W; ++dy) {
-                        int64_t yy = y + dy;
-                        if (yy < 0 || yy >= (int64_t)ny) continue;
-                        const uint8_t *row = flags_in + ((uint64_t)zz * ny + (uint64_t)yy) * nx;
-                        for (int dx = -W; dx <= W; ++dx) {
-                            int64_t xx = x + dx;
-                            if (xx < 0 || xx >= (int64_t)nx) continue;
-                            if (row[xx] != 1) continue;
-                            int d2 = dx * dx + dy * dy + dz * dz;
-                            if (d2 < best) {
-                                best = d2;
-                                bestn = ((uint64_t)zz * ny + (uint64_t)yy) * nx + (uint64_t)xx;
-                            }
+    /* Per row of the cube only the wall voxels nearest to x on either side
+     * can win: d2 = dx^2 + dy^2 + dz^2 grows with |dx| within a row, and of
+     * two at the same |dx| the scan (dx ascending, strict <) keeps the one
+     * at -|dx|.  So the row's candidate is its nearest wall at or left of x
+     * unless the nearest at or right of x is strictly closer, and rows are
+     * then compared in the cube's (dz, dy) order with the same strict <:
+     * the same winner as scanning every voxel of the cube.  lft / rgt hold,
+     * per voxel, the x of the nearest wall voxel at or before / at or after
+     * it in its row (-1 / nx when there is none). */
+    int32_t *lft = malloc(n * sizeof(int32_t)), *rgt = malloc(n * sizeof(int32_t));
+    if (!lft || !rgt) { free(lft); free(rgt); return; }
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+    for (int64_t r = 0; r < (int64_t)(ny * nz); ++r) {
+        const uint8_t *row = flags_in + (uint64_t)r * nx;
+        int32_t *L = lft + (uint64_t)r * nx, *R = rgt + (uint64_t)r * nx;
+        int32_t last = -1;
+        for (uint64_t x = 0; x < nx; ++x) { if (row[x] == 1) last = (int32_t)x; L[x] = last; }
+        last = (int32_t)nx;
+        for (uint64_t x = nx; x-- > 0;) { if (row[x] == 1) last = (int32_t)x; R[x] = last; }
+    }
+    /* one output row at a time: the cube's rows in (dz, dy) order, each
+     * compared with every voxel's best so far (the per-voxel order of the
+     * scan is unchanged, the loops are only interchanged) */
+#pragma omp parallel num_threads(vo_get_threads())
+    {
+        int *best = malloc(nx * sizeof(int));
+        uint64_t *bestn = malloc(nx * sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t zy = 0; zy < (int64_t)(ny * nz); ++zy) {
+            const int64_t z = zy / (int64_t)ny, y = zy % (int64_t)ny;
+            if (!best || !bestn || z < 1 || z >= (int64_t)nz - 1 || y < 1 || y >= (int64_t)ny - 1) continue;
+            for (uint64_t x = 0; x < nx; ++x) best[x] = 1 << 30;
+            for (int dz = -W; dz <= W; ++dz) {
+                const int64_t zz = z + dz;
+                if (zz < 0 || zz >= (int64_t)nz) continue;
+                for (int dy = -W; dy <= W; ++dy) {
+                    const int64_t yy = y + dy;
+                    if (yy < 0 || yy >= (int64_t)ny) continue;
+                    const uint64_t r = (uint64_t)zz * ny + (uint64_t)yy;
+                    const int32_t *L = lft + r * nx, *R = rgt + r * nx;
+                    const int e = dy * dy + dz * dz;
+                    for (int64_t x = 1; x < (int64_t)nx - 1; ++x) {
+                        const int64_t l = L[x], g = R[x];
+                        int64_t dx;
+                        if (l >= 0 && x - l <= W && (g >= (int64_t)nx || g - x > W || x - l <= g - x))
+                            dx = l - x;
+                        else if (g < (int64_t)nx && g - x <= W)
+                            dx = g - x;
+                        else
+                            continue;                       /* no wall voxel within [x-W, x+W] */
+                        const int d2 = (int)(dx * dx) + e;
+                        if (d2 < best[x]) {
+                            best[x] = d2;
+                            bestn[x] = r * nx + (uint64_t)(x + dx);
                         }
                     }
                 }
-                if (best < lim) {
+            }
+            for (int64_t x = 1; x < (int64_t)nx - 1; ++x) {
+                const uint64_t id = ((uint64_t)z * ny + (uint64_t)y) * nx + (uint64_t)x;
+                if (flags_in[id] != 0) continue;
+                if (best[x] < lim) {
                     flags_out[id] = 2;
-                    if (bmat) bmat[id] = wall_mat ? wall_mat[bestn] : 0;
-                    if (bd2) bd2[id] = (uint16_t)best;
+                    if (bmat) bmat[id] = wall_mat ? wall_mat[bestn[x]] : 0;
+                    if (bd2) bd2[id] = (uint16_t)best[x];
                 } else {
                     flags_out[id] = 0;
                 }
             }
+        }
+        free(best);
+        free(bestn);
+    }
+    free(lft);
+    free(rgt);
 }
 
 /* simulator.cpp:480-531: bit set for each of the 6 neighbours whose flag is 0
@@ -482,6 +522,62 @@ static inline float vo_round_f16(float x)
     v = (v & ~0x1fffu) | sign;
     memcpy(&x, &v, 4);
     return x;
+}
+
+/* The FP64 absorber designs of the library (no reference counterpart):
+ * the definitions the benchmark's CPU arm designs its cascades with, so that
+ * it needs no part of the library.
+ * First order: bilinear transform, prewarped at fc, of G wc / (s + wc) with
+ * G = (1 - R) / (1 + R); out5 = {b0, b1, b2, a1, a2}. */
+VO_API void vo_design_first_order(double fs, double reflection, double fc, double *out5)
+{
+    const double g = (1.0 - reflection) / (1.0 + reflection);
+    const double k = tan(M_PI * fc / fs);
+    out5[0] = g * k / (1.0 + k);
+    out5[1] = g * k / (1.0 + k);
+    out5[2] = 0.0;
+    out5[3] = (k - 1.0) / (k + 1.0);
+    out5[4] = 0.0;
+}
+
+static void vo_norm5(double *o, double b0, double b1, double b2, double a0, double a1, double a2)
+{
+    o[0] = b0 / a0; o[1] = b1 / a0; o[2] = b2 / a0; o[3] = a1 / a0; o[4] = a2 / a0;
+}
+
+/* Octave cascade from absorption alpha[0..2] at 250, 1000 and 4000 Hz: band
+ * gains G_b = (1 - R_b) / (1 + R_b), R_b = sqrt(1 - alpha_b), as an RBJ low
+ * shelf (G_0 below 250 Hz), a peaking section (G_1 at 1 kHz, Q = 1/sqrt 2)
+ * and a high shelf (G_2 above 4 kHz), shelf slope 1; out15 = 3 x out5. */
+VO_API void vo_design_octave_cascade(double fs, const double *alpha, double *out15)
+{
+    const double f[3] = {250.0, 1000.0, 4000.0};
+    double G[3];
+    for (int b = 0; b < 3; ++b) {
+        const double R = sqrt(1.0 - alpha[b]);
+        G[b] = (1.0 - R) / (1.0 + R);
+    }
+    {
+        const double A = sqrt(G[0]);
+        const double w = 2.0 * M_PI * f[0] / fs, cw = cos(w), al = sin(w) / 2.0 * sqrt(2.0);
+        const double sA = 2.0 * sqrt(A) * al;
+        vo_norm5(out15, A * ((A + 1) - (A - 1) * cw + sA), 2 * A * ((A - 1) - (A + 1) * cw),
+                 A * ((A + 1) - (A - 1) * cw - sA), (A + 1) + (A - 1) * cw + sA, -2 * ((A - 1) + (A + 1) * cw),
+                 (A + 1) + (A - 1) * cw - sA);
+    }
+    {
+        const double A = sqrt(G[1]);
+        const double w = 2.0 * M_PI * f[1] / fs, cw = cos(w), al = sin(w) / (2.0 / sqrt(2.0));
+        vo_norm5(out15 + 5, 1 + al * A, -2 * cw, 1 - al * A, 1 + al / A, -2 * cw, 1 - al / A);
+    }
+    {
+        const double A = sqrt(G[2]);
+        const double w = 2.0 * M_PI * f[2] / fs, cw = cos(w), al = sin(w) / 2.0 * sqrt(2.0);
+        const double sA = 2.0 * sqrt(A) * al;
+        vo_norm5(out15 + 10, A * ((A + 1) + (A - 1) * cw + sA), -2 * A * ((A - 1) + (A + 1) * cw),
+                 A * ((A + 1) + (A - 1) * cw - sA), (A + 1) - (A - 1) * cw + sA, 2 * ((A - 1) - (A + 1) * cw),
+                 (A + 1) - (A - 1) * cw - sA);
+    }
 }
 
 /* initSphereKernel (src/simulator/init_sphere.cu:4-25), one loop iteration

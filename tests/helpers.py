@@ -47,3 +47,16 @@ def rel_l2(a, b) -> float:
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def grid_parity(sim, g: dict) -> None:
+    """A classified simulation's grid against the oracle's: shape, flags,
+    normals, boundary list, and each boundary voxel's material and sponge
+    weight, all bit for bit."""
+    assert sim.shape == tuple(g["shape"])
+    assert np.array_equal(sim.flags(), g["flags"])
+    assert np.array_equal(sim.normals(), g["normals"])
+    assert np.array_equal(sim.boundary_indices(), g["bidx"])
+    m, w = sim.boundary_materials()
+    assert np.array_equal(m, g["bmat"])
+    assert np.array_equal(w.view(np.uint32), g["bw"].view(np.uint32))

@@ -116,6 +116,57 @@ def test_sponge_nearest_material_tie_break():
     assert out[c] == 2 and bd2[c] == 4 and bm[c] == 7
 
 
+def _classify_cube_scan(shape, W, flags, wmat):
+    """sponge_kernel.cu:8-62 generalised to width W as written: each
+    interior air voxel scans its whole cube in (dz, dy, dx) order and keeps
+    the first smallest squared distance to a wall voxel."""
+    nx, ny, nz = shape
+    f = flags.reshape(nz, ny, nx)
+    out = f.copy()
+    bm = np.zeros_like(f)
+    bd = np.zeros(f.shape, np.uint16)
+    for z in range(1, nz - 1):
+        for y in range(1, ny - 1):
+            for x in range(1, nx - 1):
+                if f[z, y, x] != 0:
+                    continue
+                best, where = 1 << 30, None
+                for dz in range(-W, W + 1):
+                    for dy in range(-W, W + 1):
+                        for dx in range(-W, W + 1):
+                            zz, yy, xx = z + dz, y + dy, x + dx
+                            if 0 <= zz < nz and 0 <= yy < ny and 0 <= xx < nx and f[zz, yy, xx] == 1:
+                                d2 = dx * dx + dy * dy + dz * dz
+                                if d2 < best:
+                                    best, where = d2, (zz, yy, xx)
+                if best < W * W + 1:
+                    out[z, y, x] = 2
+                    bm[z, y, x] = wmat.reshape(f.shape)[where]
+                    bd[z, y, x] = best
+                else:
+                    out[z, y, x] = 0
+    return out.reshape(-1), bm.reshape(-1), bd.reshape(-1)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_classification_equals_cube_scan(seed):
+    """The oracle's classification (the cube scan with rows reduced to
+    their nearest wall voxels) against the literal cube scan: flags,
+    nearest-wall materials and distances on random small grids."""
+    rng = np.random.default_rng(seed)
+    shape = tuple(int(v) for v in rng.integers(4, 14, 3))
+    W = int(rng.integers(1, 5))
+    n = int(np.prod(shape))
+    flags = np.zeros(n, np.uint8)
+    flags[rng.random(n) < rng.uniform(0.02, 0.15)] = 1
+    flags[rng.random(n) < 0.02] = 3
+    wmat = rng.integers(0, 4, n).astype(np.uint8)
+    got = oracle.classify(shape, W, flags, wmat)
+    want = _classify_cube_scan(shape, W, flags, wmat)
+    for a, b in zip(got, want):
+        assert np.array_equal(np.asarray(a).reshape(-1), np.asarray(b).reshape(-1).astype(np.asarray(a).dtype))
+
+
 def test_boundary_list_sorted_interior():
     sc = scenes.reference_room()
     g = oracle_grid(sc)
@@ -289,3 +340,20 @@ def test_storage_rounding_matches_ieee_conversions():
     u = x.view(np.uint32).astype(np.uint64)
     wantb = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
     assert np.array_equal(oracle.round16(x, 2).view(np.uint32), wantb)
+
+
+def test_oracle_absorber_designs_equal_the_library():
+    """The oracle's FP64 absorber designs (used by the benchmark's CPU arm
+    instead of the library's) equal the library's bit for bit."""
+    from virs_b200 import capi
+    rng = np.random.default_rng(3)
+    for _ in range(100):
+        fs = rng.uniform(2e4, 4e5)
+        a = rng.uniform(0.05, 1.0, 3)
+        got = oracle.design_octave_cascade(fs, a)
+        want = np.asarray(capi.design_octave_cascade(fs, a), np.float64).reshape(3, 5)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        r, fc = rng.uniform(-0.9, 0.99), rng.uniform(50.0, fs / 2.5)
+        got = oracle.design_first_order(fs, r, fc)
+        want = np.asarray(capi.design_first_order(fs, r, fc), np.float64)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import oracle_grid, oracle_scene, rel_l2
+from helpers import grid_parity, oracle_grid, oracle_scene, rel_l2
 from virs_b200 import capi, scenes
 
 pytestmark = pytest.mark.gpu
@@ -20,15 +20,7 @@ pytestmark = pytest.mark.gpu
 FP32_REL_L2 = 1e-5
 
 
-def _grid_parity(sim, g):
-    assert sim.shape == tuple(g["shape"])
-    assert np.array_equal(sim.flags(), g["flags"])
-    assert np.array_equal(sim.normals(), g["normals"])
-    bidx = sim.boundary_indices()
-    assert np.array_equal(bidx, g["bidx"])
-    m, w = sim.boundary_materials()
-    assert np.array_equal(m, g["bmat"])
-    assert np.array_equal(w.view(np.uint32), g["bw"].view(np.uint32))
+_grid_parity = grid_parity
 
 
 def test_reference_room_bit_exact():

@@ -24,6 +24,7 @@ Workloads (sizes as the benchmark configurations name them):
 """
 from __future__ import annotations
 
+import contextlib
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -249,12 +250,36 @@ def fs_of(h: float, courant: float, c: float = 343.0) -> float:
     return 1.0 / dt
 
 
+# absorber designs used by the scene builders: the library's by default; a
+# caller that must not load the library (the benchmark's CPU arm) installs
+# other implementations of the same designs with `designs`
+_DESIGNS = {}
+
+
+@contextlib.contextmanager
+def designs(first_order, octave_cascade):
+    """Build scenes with these absorber designs (callables with the
+    signatures of design_first_order_np / design_octave_cascade_np) instead
+    of the library's, inside the `with` block."""
+    old = dict(_DESIGNS)
+    _DESIGNS.update(first_order=first_order, octave_cascade=octave_cascade)
+    try:
+        yield
+    finally:
+        _DESIGNS.clear()
+        _DESIGNS.update(old)
+
+
 def design_first_order_np(fs: float, reflection: float, fc: float) -> np.ndarray:
+    if "first_order" in _DESIGNS:
+        return np.asarray(_DESIGNS["first_order"](fs, reflection, fc), np.float64)
     from . import capi
     return capi.design_first_order(fs, reflection, fc)
 
 
 def design_octave_cascade_np(fs: float, alpha) -> np.ndarray:
+    if "octave_cascade" in _DESIGNS:
+        return np.asarray(_DESIGNS["octave_cascade"](fs, alpha), np.float64)
     from . import capi
     return capi.design_octave_cascade(fs, alpha)
 
