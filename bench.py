@@ -200,15 +200,18 @@ def time_run(sim, steps, stream):
     return e0.elapsed_time(e1)
 
 
-def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e):
+def bench_storage(sc, storage, args, stream, dev, world, dist, want_e2e, rounding=0):
     """Warm up, then time K steps: device-resident graph run, a per-kernel
-    CUDA-event pass, and (optionally) the end-to-end host run."""
+    CUDA-event pass, and (optionally) the end-to-end host run.  rounding:
+    the 16-bit stores' rounding (virs_set_rounding)."""
     import torch
     from virs_b200 import scenes
     warm = max(args.warmup, GRAPH_WARMUP)
     total = warm + args.steps + (args.kernel_steps if args.kernel_steps else 0) + (args.steps if want_e2e else 0)
     total += args.sustained_steps if want_e2e else 0
     sim, meta = scenes.build_simulation(sc, storage=storage, device=dev, steps=total)
+    if rounding:
+        sim.set_rounding(rounding)
     t_pre = time.perf_counter()
     tiling = sim.autotune(args.tune_steps) if args.tune_steps else sim.tiling()
     tune_s = time.perf_counter() - t_pre
@@ -391,6 +394,16 @@ def run_virs(args):
             "bytes_per_voxel": BYTES_16,
             "kernel": bkern.split(" ")[0],
             "time_blocking": rb["time_blocking"],
+        }
+        # the same with stochastic rounding of the 16-bit stores: the cost of
+        # the per-voxel hash (two steps per pass do not apply it)
+        rs = bench_storage(sc, capi.STORAGE_BF16, args, stream, dev, world, dist, want_e2e=False,
+                           rounding=capi.ROUND_STOCHASTIC)
+        variants["bf16_storage_stochastic_rounding"] = {
+            "value": nvox * args.steps / (rs["ms"] * 1e-3) / 1e9 * world, "ms_per_step": rs["ms"] / args.steps,
+            "vs_bf16_nearest": rb["ms"] / rs["ms"],
+            "kernel_ms": rs.get("kernel_ms"), "kernel_ms_nearest": rb.get("kernel_ms"),
+            "boundary_ms": rs.get("boundary_ms"),
         }
     if args.batch_steps:
         for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):

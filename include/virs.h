@@ -355,6 +355,20 @@ virs_status virs_set_time_blocking(virs_sim *sim, int steps_per_pass, int tile_r
 virs_status virs_get_time_blocking(const virs_sim *sim, int *steps_per_pass, int *tile_rows, int *planes_per_block,
                                    int *active);
 
+/* Rounding of the values stored in 16-bit fields (no reference counterpart;
+ * the reference stores FP32).  VIRS_ROUND_NEAREST (default): to nearest,
+ * ties to even.  VIRS_ROUND_STOCHASTIC: a value is rounded up in magnitude
+ * with the probability of its distance from the value below, from 16 bits of
+ * a counter-based hash of (voxel, step), so a run is reproducible and equal
+ * for every kernel variant, in batches and in z-slabs; FP16 values below
+ * 2^-14 or of 65504 and more in magnitude still round to nearest.  It
+ * applies to the step's stores (stencil, boundary pass, sources); values set
+ * with virs_set_pressure or virs_init_pressure_sphere round to nearest.  No
+ * effect on FP32 storage.  Two steps per pass do not apply it: with it on,
+ * virs_run takes single steps and the autotuner tries no two-step variant. */
+enum { VIRS_ROUND_NEAREST = 0, VIRS_ROUND_STOCHASTIC = 1 };
+virs_status virs_set_rounding(virs_sim *sim, int mode);
+
 typedef struct virs_tiling {
     int32_t tile_rows;        /* 4, 8 or 16                                        */
     int32_t planes_per_block; /* z planes streamed by one block                    */

@@ -257,6 +257,7 @@ class _RunArgs(C.Structure):
         ("ir64", C.c_void_p),
         ("storage", C.c_int32), ("scale", C.c_float),
         ("rigid", C.c_int32), ("l2", C.c_float), ("normals", C.c_void_p),
+        ("rounding", C.c_int32), ("sr_base", C.c_uint64),
     ]
 
 
@@ -275,7 +276,7 @@ class Scene:
     def __init__(self, shape, flags, bidx, bmat, bw, coef32, n_sections, *, coef64=None,
                  hard=None, src_idx=(), src_sig=None, rcv_idx=(), consts=None, consts64=None,
                  mix_y=0.1, mix_d=0.9, gain=float(np.float32(0.4)), form=0, storage=0, scale=1.0,
-                 normals=None, rigid=False, l2=0.0):
+                 normals=None, rigid=False, l2=0.0, rounding=0):
         self.shape = tuple(int(s) for s in shape)
         self.flags = np.ascontiguousarray(flags, np.uint8)
         self.bidx = np.ascontiguousarray(bidx, np.uint32)
@@ -301,6 +302,7 @@ class Scene:
         self.normals = None if normals is None else np.ascontiguousarray(normals, np.uint8)
         self.rigid = bool(rigid)      # FP32 run: rigid-wall update of the boundary voxels
         self.l2 = float(l2)           # its (c dt / h)^2
+        self.rounding = int(rounding) # 16-bit storage: 0 to nearest, 1 stochastic (the library's definition)
 
     def _args(self, steps, step0, ir, p, pp, st, f64):
         a = _RunArgs()
@@ -322,6 +324,7 @@ class Scene:
         a.steps, a.step0, a.ir_stride = steps, step0, steps
         a.ir, a.p, a.pprev, a.state = _ptr(ir), _ptr(p), _ptr(pp), _ptr(st)
         a.storage, a.scale = self.storage, self.scale
+        a.rounding = self.rounding
         if self.rigid:
             if self.normals is None:
                 raise ValueError("the rigid-wall update needs the normals")
@@ -445,6 +448,17 @@ def init_sphere(p, shape, center, radius: int, pressure: float, zero_outside: bo
                          C.c_uint64(cy), C.c_uint64(cz), C.c_uint64(int(radius)), C.c_float(pressure),
                          C.c_int(int(zero_outside)))
     return p
+
+
+def sr16(x, storage: int, r16):
+    """Values rounded stochastically as the library's 16-bit stores round
+    them (1 FP16, 2 BF16), each with its 16 random bits r16."""
+    x = np.ascontiguousarray(x, np.float32)
+    r = np.ascontiguousarray(np.broadcast_to(np.asarray(r16, np.uint32), x.shape))
+    out = np.empty_like(x)
+    lib().vo_sr16_array(C.c_void_p(x.ctypes.data), C.c_void_p(out.ctypes.data), C.c_uint64(x.size),
+                        C.c_int32(storage), C.c_void_p(r.ctypes.data))
+    return out
 
 
 def energy(shape, flags, p, pprev, lambda2: float) -> float:

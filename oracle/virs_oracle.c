@@ -474,6 +474,8 @@ typedef struct vo_run_args {
     int32_t rigid;                 /* FP32 run: rigid-wall update of boundary voxels */
     float l2;                      /* (c dt / h)^2 of that update            */
     const uint8_t *normals;        /* air-neighbour mask per voxel           */
+    int32_t rounding;              /* 16-bit storage: 0 to nearest, 1 stochastic */
+    uint64_t sr_base;              /* its key offset (a slab's first padded voxel) */
 } vo_run_args;
 
 /* 16-bit field storage, as the GPU path stores it: every value written to
@@ -602,6 +604,70 @@ VO_API void vo_init_sphere(float *p, uint64_t nx, uint64_t ny, uint64_t nz, uint
             }
 }
 
+/* Stochastic rounding of the 16-bit stores, as the library defines it: a
+ * value is rounded up in magnitude with the probability of its distance
+ * from the value below, using 16 random bits that are a pure function of
+ * (voxel, step, phase):
+ *   s = mix32(2 step + phase + 0x9e3779b9), w = mix32(((pos + base) >> 1) ^ s),
+ *   bits = w & 0xffff for an even pos + base, w >> 16 for an odd one,
+ * with pos the voxel's position in the library's padded layout (rows of
+ * ceil(nx / 32) * 32 voxels) and phase 0 for the step's store of p^{n+1}
+ * (interior, boundary, hard source) and 1 for the soft-source addition.
+ * mix32 is the "lowbias32" integer hash (Chris Wellons, hash-prospector).
+ * The bits are added below the kept bits of the FP32 pattern, which is then
+ * truncated; FP16 values below 2^-14 or of 65504 and more in magnitude, and
+ * non-finite values, round to nearest. */
+static inline uint32_t vo_mix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+static inline uint32_t vo_sr_key(uint64_t step, uint32_t phase)
+{
+    return vo_mix32((uint32_t)(2u * (uint32_t)step + phase + 0x9e3779b9u));
+}
+
+static inline uint32_t vo_sr_bits(uint64_t pos, uint32_t key)
+{
+    const uint32_t w = vo_mix32((uint32_t)(pos >> 1) ^ key);
+    return (pos & 1u) ? (w >> 16) : (w & 0xffffu);
+}
+
+static inline float vo_sr16(float x, int storage, uint32_t r16)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    const uint32_t a = u & 0x7fffffffu;
+    if (storage == 2) {
+        if (a >= 0x7f7f0000u) return vo_round_bf16(x);
+        u = (u + r16) & 0xffff0000u;
+    } else {
+        if (a < 0x38800000u || a >= 0x477fe000u) return vo_round_f16(x);
+        u = (u + (r16 & 0x1fffu)) & ~0x1fffu;
+    }
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+/* the stochastic rounding on its own (tests): out[i] = in[i] rounded with
+ * the random bits r16[i] */
+VO_API void vo_sr16_array(const float *in, float *out, uint64_t n, int32_t storage, const uint32_t *r16)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = vo_sr16(in[i], storage, r16[i]);
+}
+
+/* padded position of reference index i (rows of px voxels), plus the key offset */
+static inline uint64_t vo_padded(const vo_run_args *a, uint64_t i)
+{
+    const uint64_t px = (a->nx + 31) / 32 * 32, row = i / a->nx;
+    return row * px + (i - row * a->nx) + a->sr_base;
+}
+
 /* the storage rounding on its own (tests) */
 VO_API void vo_round16(const float *in, float *out, uint64_t n, int32_t storage)
 {
@@ -613,6 +679,14 @@ static void vo_round_field(float *f, uint64_t n, int storage)
     if (storage == 0) return;
 #pragma omp parallel for num_threads(vo_get_threads()) schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i) f[i] = storage == 1 ? vo_round_f16(f[i]) : vo_round_bf16(f[i]);
+}
+
+/* the step's store of p^{n+1} rounded stochastically (phase 0) */
+static void vo_sr_field(const vo_run_args *a, float *f, uint64_t n, uint64_t step)
+{
+    const uint32_t key = vo_sr_key(step, 0);
+#pragma omp parallel for num_threads(vo_get_threads()) schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) f[i] = vo_sr16(f[i], a->storage, vo_sr_bits(vo_padded(a, (uint64_t)i), key));
 }
 
 static inline float vsel(const uint8_t *fl, const float *p, uint64_t n, float c)
@@ -762,14 +836,17 @@ VO_API int vo_run_f32(const vo_run_args *a)
         interior_f32(a, pc, pp, pn, hard);
         if (a->nb && a->rigid) rigid_f32(a, pc, pp, pn);
         if (a->nb) boundary_f32(a, pc, pp, pn, st);
-        vo_round_field(pn, N, sto);
+        const int sr = sto && a->rounding == 1;
+        if (sr) vo_sr_field(a, pn, N, sn);
+        else vo_round_field(pn, N, sto);
         for (uint32_t s = 0; s < a->n_src; ++s) {
             const uint64_t i = a->src_idx[s];
             const float v = sig_at(a, s, sn) * scale;   /* scaled on the host, without FTZ */
             ftz_on();
             pn[i] = pn[i] + v;
             ftz_off();
-            if (sto) pn[i] = sto == 1 ? vo_round_f16(pn[i]) : vo_round_bf16(pn[i]);
+            if (sr) pn[i] = vo_sr16(pn[i], sto, vo_sr_bits(vo_padded(a, i), vo_sr_key(sn, 1)));
+            else if (sto) pn[i] = sto == 1 ? vo_round_f16(pn[i]) : vo_round_bf16(pn[i]);
         }
         /* rotation (simulator_gpu.cu:292-293): prev <- curr <- next */
         float *t = pp; pp = pc; pc = pn; pn = t;

@@ -357,3 +357,25 @@ def test_oracle_absorber_designs_equal_the_library():
         got = oracle.design_first_order(fs, r, fc)
         want = np.asarray(capi.design_first_order(fs, r, fc), np.float64)
         assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_stochastic_rounding_is_unbiased_and_exact_on_representable_values(storage):
+    """The library's stochastic rounding (restated in the oracle): every
+    result is one of the two neighbouring 16-bit values, values already
+    representable never move, and over all 2^16 random words the mean of
+    the results is the value itself (exactly, in double)."""
+    rng = np.random.default_rng(7)
+    r = np.arange(65536, dtype=np.uint32)
+    xs = rng.normal(0, 50, 40).astype(np.float32)
+    if storage == 1:
+        xs = np.concatenate([xs, np.float32([1e-3, -3.5e-4, 60000.0])])
+    for x in xs:
+        y = oracle.sr16(np.full(65536, x, np.float32), storage, r)
+        vals = sorted({float(v) for v in y})
+        assert len(vals) <= 2
+        near = float(oracle.round16(np.float32([x]), storage)[0])
+        assert near in vals
+        assert abs(float(np.mean(y.astype(np.float64))) - float(x)) <= 1e-12 * abs(float(x)) + 1e-30
+        rep = oracle.round16(np.float32([x]), storage)
+        assert np.array_equal(oracle.sr16(np.full(65536, rep[0], np.float32), storage, r), np.full(65536, rep[0]))

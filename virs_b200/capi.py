@@ -17,6 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libvirs_b200.so"
 OK, E_ARG, E_OOM, E_CUDA, E_UNSTABLE, E_TIMEOUT, E_STATE, E_IO = range(8)
 STATUS_NAMES = {0: "OK", 1: "E_ARG", 2: "E_OOM", 3: "E_CUDA", 4: "E_UNSTABLE", 5: "E_TIMEOUT", 6: "E_STATE", 7: "E_IO"}
 STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2
+ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 ROLE_IGNORE, ROLE_SOURCE = 0xFF, 0xFE
 BOUNDARY_REFERENCE, BOUNDARY_CENTERED = 0, 1
 
@@ -109,6 +110,7 @@ _SIGS = {
     "virs_get_timing": ([_P, _P], C.c_int),
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_set_time_blocking": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "virs_set_rounding": ([_P, C.c_int], C.c_int),
     "virs_get_time_blocking": ([_P, _P, _P, _P, _P], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
@@ -511,6 +513,10 @@ class Simulation:
     def set_time_blocking(self, steps_per_pass: int = 2, rows: int = 0, planes: int = 0):
         """Two steps per pass over the fields (bit-identical to single steps)."""
         check(lib().virs_set_time_blocking(self._h, steps_per_pass, rows, planes))
+
+    def set_rounding(self, mode: int) -> None:
+        """Rounding of the 16-bit stores: ROUND_NEAREST or ROUND_STOCHASTIC."""
+        check(lib().virs_set_rounding(self._h, int(mode)))
 
     def time_blocking(self) -> dict:
         v = [C.c_int() for _ in range(4)]

@@ -117,6 +117,7 @@ struct virs_sim {
     // the owned planes and a ghost plane each side) starts slab_drop planes
     // into them.  For a whole grid ext_nz == nz and slab_drop == 0.
     bool slab = false;
+    int rounding = VIRS_ROUND_NEAREST; // of the 16-bit stores (virs_set_rounding)
     uint32_t ext_nz = 0, slab_drop = 0;
     uint64_t slab_lo = 0, slab_hi = 0, global_nz = 0; // owned global planes and the global grid's planes
 
@@ -612,9 +613,16 @@ virs_status ready_to_run(virs_sim *s)
     return VIRS_OK;
 }
 
+// stochastic rounding of the 16-bit stores, and its key offset: a slab's
+// voxels take the keys of the same voxels of the whole grid
+bool sr_on(const virs_sim *s) { return s->rounding == VIRS_ROUND_STOCHASTIC && s->prm.storage != VIRS_STORAGE_F32; }
+uint64_t sr_base(const virs_sim *s) { return s->slab ? (s->slab_lo - 1) * (uint64_t)s->ny * s->px : 0; }
+
 StepArgs step_args(const virs_sim *s, int parity)
 {
     StepArgs a{};
+    a.sr = sr_on(s) ? 1 : 0;
+    a.sr_base = sr_base(s);
     a.side = s->side.as<float4>();
     a.p = s->field[parity].ptr;
     a.q = s->field[parity ^ 1].ptr;
@@ -654,6 +662,8 @@ StepArgs step_args(const virs_sim *s, int parity)
 PostArgs post_args(const virs_sim *s, int parity)
 {
     PostArgs a{};
+    a.sr = sr_on(s) ? 1 : 0;
+    a.sr_base = sr_base(s);
     a.q = s->field[parity ^ 1].ptr;
     if (s->stop_rule) a.stop = s->stopbuf.as<uint32_t>();
     a.src = s->src.as<uint64_t>();
@@ -696,7 +706,8 @@ void *buf_ptr(const virs_sim *s, int k) { return k < 2 ? s->field[k].ptr : s->sp
 
 bool pair_on(const virs_sim *s)
 {
-    return s->pair_steps == 2 && !s->pair_nomem && s->depth > 0 && s->nx >= 3 && s->ny >= 3 && s->nz >= 3;
+    return s->pair_steps == 2 && !s->pair_nomem && !sr_on(s) && s->depth > 0 && s->nx >= 3 && s->ny >= 3 &&
+           s->nz >= 3;
 }
 
 // the voxels whose p^{n+2} the two-step kernel leaves provisional, for the
@@ -1958,6 +1969,18 @@ VIRS_EXPORT virs_status virs_set_time_blocking(virs_sim *s, int steps_per_pass, 
     return VIRS_OK;
 }
 
+VIRS_EXPORT virs_status virs_set_rounding(virs_sim *s, int mode)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_set_rounding: null");
+    if (mode != VIRS_ROUND_NEAREST && mode != VIRS_ROUND_STOCHASTIC)
+        return fail(VIRS_E_ARG, "rounding must be VIRS_ROUND_NEAREST or VIRS_ROUND_STOCHASTIC");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    s->rounding = mode;
+    s->drop_graphs();
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_get_time_blocking(const virs_sim *s, int *steps_per_pass, int *tile_rows, int *planes,
                                                int *active)
 {
@@ -2092,8 +2115,9 @@ VIRS_EXPORT virs_status virs_autotune(virs_sim *s, uint32_t trial_steps, virs_ti
             if ((st = reset_state(s)) != VIRS_OK) break;
         }
         // two steps per pass (groups of four steps), with the best single-step
-        // tiling for the steps that do not fill a group
-        if (st == VIRS_OK) {
+        // tiling for the steps that do not fill a group; not with stochastic
+        // rounding, which two steps per pass do not apply
+        if (st == VIRS_OK && !sr_on(s)) {
             s->tile_rows = pick.t.tile_rows;
             s->depth = pick.t.pipeline_depth;
             s->zc = pick.t.planes_per_block;

@@ -93,6 +93,8 @@ struct StepArgs {
     float c2dt2, inv_h2;
     float l2;               // (c dt / h)^2 of the rigid-wall update
     int rigid;              // boundary voxels: rigid-wall update instead of the mirrored leapfrog
+    int sr;                 // 16-bit storage: stochastic rounding of the stores (step_common.cuh)
+    uint64_t sr_base;       // its key offset: a slab's first padded voxel in the whole grid (0 otherwise)
     double K, mix_y, mix_d, gain;
 };
 
@@ -111,6 +113,8 @@ struct PostArgs {
     uint32_t nhard;         // per-step hard-source values (scaled) in `hard`
     const float *hard;
     uint32_t *stop;         // the RMS stop rule on the device (nullptr: off): {stopped, stop step, filter state}
+    int sr;                 // as StepArgs::sr / sr_base
+    uint64_t sr_base;
 };
 
 // one member of a batched run (device-resident descriptor)

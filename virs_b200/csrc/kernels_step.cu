@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
     }
     __syncthreads();
 
+    const uint32_t srk = a.sr ? sr_step_key(*a.ctr, 0u) : 0u;
     for (int z = z0; z < z1; ++z) {
         const int b = (z - z0) & 1;
         const size_t zc = (size_t)z * plane, zn = zc + plane;
@@ -136,7 +137,8 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
         }
 
         if (act) {
-            IO::st(Q + zc + own, r);
+            if (a.sr) st_sr<T>(Q + zc + own, r, zc + own, a.sr_base, srk);
+            else IO::st(Q + zc + own, r);
 #pragma unroll
             for (int k = 0; k < VEC; ++k) sm[b ^ 1][ty + 1][lane * VEC + k] = cp[k];
         }
@@ -218,7 +220,8 @@ __device__ __forceinline__ void bvox_update(const StepArgs &a, uint64_t slot, co
     if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, v.ce, v.qv, 0.f);
     if (MODE == BND_RECORD) return;
     r = MAXS > 0 ? bcompute<MAXS>(a, r, v.ce, v.qv, slot, v.st) : boundary_loop(a, r, v.ce, v.qv, slot);
-    static_cast<T *>(a.q)[v.i] = Io<T>::put(r);
+    static_cast<T *>(a.q)[v.i] =
+        put_rounded<T>(r, a.sr, v.i, a.sr_base, a.sr ? sr_step_key(*a.ctr, 0u) : 0u);
 }
 
 // The compacted boundary pass (simulator_gpu.cu:105-150), in list order.
@@ -382,14 +385,18 @@ template <typename T> __device__ __forceinline__ void post_body(const PostArgs &
     // them alone; their value of this step is written here, before the soft
     // sources are added
     if (a.nhpos) {
-        const T hv = IO::put(sn < a.nhard ? a.hard[sn] : 0.f);
-        for (uint32_t i = threadIdx.x; i < a.nhpos; i += blockDim.x) Q[a.hpos[i]] = hv;
+        // the step's own store at these voxels (phase 0 of the rounding key)
+        const float hv = sn < a.nhard ? a.hard[sn] : 0.f;
+        const uint32_t k0 = a.sr ? sr_step_key(sn, 0u) : 0u;
+        for (uint32_t i = threadIdx.x; i < a.nhpos; i += blockDim.x)
+            Q[a.hpos[i]] = put_rounded<T>(hv, a.sr, a.hpos[i], a.sr_base, k0);
         __syncthreads();
     }
+    const uint32_t k1 = a.sr ? sr_step_key(sn, 1u) : 0u;
     for (uint32_t i = threadIdx.x; i < a.nsrc; i += blockDim.x) {
         const float v = sn < a.siglen ? a.sig[(uint64_t)i * a.siglen + sn] : 0.f;
         const uint64_t j = a.src[i];
-        Q[j] = IO::put(__fadd_rn(IO::get(Q[j]), v));
+        Q[j] = put_rounded<T>(__fadd_rn(IO::get(Q[j]), v), a.sr, j, a.sr_base, k1);
     }
     __syncthreads();
     if (sn < a.cap)

@@ -217,6 +217,7 @@ template <typename T, int TY, int L> struct Tile {
     int x0, y0, z0, nst, row, sl, c0, t0;
     uint32_t j0;
     bool act, leader;
+    uint32_t srk; // the stochastic-rounding key of this step's stores (a->sr)
     float2 c2dt2, inv_h2;
     size_t plane;
     uint64_t zmask; // bit j: the codes of stage j are all zero (not copied)
@@ -277,7 +278,10 @@ template <typename T, int TY, int L> struct Tile {
 
         float r[V];
         tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, r);
-        if (act) IO::st(out, r);
+        if (act) {
+            if (a->sr) st_sr<T>(out, r, (uint64_t)(out - static_cast<T *>(a->q)), a->sr_base, srk);
+            else IO::st(out, r);
+        }
         out += plane;
         sh = sz;
         return true;
@@ -332,6 +336,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.t0 = t.row * TX + t.sl * V;            // ... and in a tile box
     t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
     t.inv_h2 = make_float2(a.inv_h2, a.inv_h2);
+    t.srk = a.sr ? sr_step_key(*a.ctr, 0u) : 0u;
     t.plane = (size_t)a.px * a.ny;
     {
         const uint32_t gx = (a.px + TX - 1) / TX, gy = (a.ny + TY - 1) / TY;

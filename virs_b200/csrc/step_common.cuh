@@ -96,6 +96,114 @@ template <> struct Io<__nv_bfloat16> {
     __device__ static __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
 };
 
+// ---- stochastic rounding of the 16-bit stores (opt-in) -----------------------
+//
+// With VIRS_ROUND_STOCHASTIC a value stored as FP16 / BF16 is rounded up in
+// magnitude with a probability equal to the fraction it lies between its two
+// neighbours, instead of to the nearest: 16 random bits are added below the
+// kept bits of the FP32 pattern, which is then truncated.  The bits are a
+// pure function of (voxel, step, phase), so runs are reproducible and every
+// kernel variant rounds a voxel alike:
+//   s    = mix32(2 * step + phase + SR_SEED)      phase 0: the step's store of
+//                                                 p^{n+1} (stencil, boundary pass,
+//                                                 hard source); 1: soft sources
+//   w    = mix32((pos + base) / 2 ^ s)            pos: padded device index;
+//                                                 base: a slab's offset in the
+//                                                 whole grid (0 otherwise)
+//   bits = low 16 of w for an even position, high 16 for an odd one
+// mix32 is Chris Wellons' "lowbias32" integer hash (hash-prospector, public
+// domain).  Values that round to themselves (exact ones: walls, kept
+// p^{n-1}) are unchanged; FP16 values below 2^-14 or from 65504 up in
+// magnitude, and non-finite values, round to nearest.
+constexpr uint32_t SR_SEED = 0x9e3779b9u;
+
+__device__ __forceinline__ uint32_t mix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// the per-launch part of the key
+__device__ __forceinline__ uint32_t sr_step_key(uint32_t step, uint32_t phase)
+{
+    return mix32(2u * step + phase + SR_SEED);
+}
+
+// the random word of the voxel pair holding padded position pos
+__device__ __forceinline__ uint32_t sr_word(uint64_t pos, uint64_t base, uint32_t key)
+{
+    return mix32((uint32_t)((pos + base) >> 1) ^ key);
+}
+
+__device__ __forceinline__ uint32_t sr_bits(uint64_t pos, uint64_t base, uint32_t key)
+{
+    const uint32_t w = sr_word(pos, base, key);
+    return ((pos + base) & 1u) ? (w >> 16) : (w & 0xffffu);
+}
+
+// FP32 pattern rounded stochastically to the kept bits of T (truncated,
+// exactly representable in T), or to nearest where stated above
+__device__ __forceinline__ __nv_bfloat16 sr_bf16(float f, uint32_t r16)
+{
+    uint32_t u = __float_as_uint(f);
+    if ((u & 0x7fffffffu) < 0x7f7f0000u) {
+        u = (u + r16) & 0xffff0000u;
+        return __ushort_as_bfloat16((unsigned short)(u >> 16));
+    }
+    return __float2bfloat16_rn(f);
+}
+
+__device__ __forceinline__ __half sr_f16(float f, uint32_t r16)
+{
+    const uint32_t u = __float_as_uint(f), a = u & 0x7fffffffu;
+    if (a >= 0x38800000u && a < 0x477fe000u) return __float2half_rn(__uint_as_float((u + (r16 & 0x1fffu)) & ~0x1fffu));
+    return __float2half_rn(f);
+}
+
+template <typename T> struct Sr;
+template <> struct Sr<float> {
+    __device__ static float put(float f, uint32_t) { return f; }
+};
+template <> struct Sr<__nv_bfloat16> {
+    __device__ static __nv_bfloat16 put(float f, uint32_t r16) { return sr_bf16(f, r16); }
+};
+template <> struct Sr<__half> {
+    __device__ static __half put(float f, uint32_t r16) { return sr_f16(f, r16); }
+};
+
+// a store of one value: to nearest, or stochastic with `key` (sr != 0)
+template <typename T>
+__device__ __forceinline__ T put_rounded(float f, int sr, uint64_t pos, uint64_t base, uint32_t key)
+{
+    return sr ? Sr<T>::put(f, sr_bits(pos, base, key)) : Io<T>::put(f);
+}
+
+// a stochastic store of one 16-byte vector of V values starting at the
+// (even) padded position pos0: one hash per voxel pair
+template <typename T>
+__device__ __forceinline__ void st_sr(T *p, const float (&r)[Io<T>::VEC], uint64_t pos0, uint64_t base, uint32_t key)
+{
+    constexpr int V = Io<T>::VEC;
+    if constexpr (V == 8) {
+        uint4 v;
+        uint32_t *w32 = reinterpret_cast<uint32_t *>(&v);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t w = sr_word(pos0 + 2 * k, base, key);
+            const T lo = Sr<T>::put(r[2 * k], w & 0xffffu), hi = Sr<T>::put(r[2 * k + 1], w >> 16);
+            w32[k] = (uint32_t)*reinterpret_cast<const unsigned short *>(&lo) |
+                     ((uint32_t)*reinterpret_cast<const unsigned short *>(&hi) << 16);
+        }
+        __stcs(reinterpret_cast<uint4 *>(p), v);
+    } else {
+        Io<T>::st(p, r);
+    }
+}
+
 template <int VEC> __device__ inline void ld_code(const uint8_t *p, uint8_t (&c)[VEC]);
 template <> __device__ inline void ld_code<4>(const uint8_t *p, uint8_t (&c)[4])
 {
