@@ -178,6 +178,26 @@ virs_status virs_get_slab_info(const virs_sim *sim, uint64_t *z_lo, uint64_t *z_
 virs_status virs_slab_planes(const virs_sim *sim, void **first, void **last, void **ghost_lo, void **ghost_hi,
                              size_t *plane_bytes);
 
+/* The exchange in the library (no reference counterpart): lo and hi are
+ * adjacent slabs of one grid (lo's owned planes end where hi's begin) at the
+ * same step, on one GPU or two GPUs of this process.  Each handle pulls its
+ * ghost plane of p^n from the other -- lo's ghost_hi from hi's first owned
+ * plane, hi's ghost_lo from lo's last -- with a device (or peer) copy on its
+ * own stream, after the other handle's last queued work; the kernels only
+ * ever read their own GPU's memory.  Returns when the copies are queued; the
+ * handles' next runs follow them.  Call it for every adjacent pair before
+ * every step (a slab's step writes the buffer its neighbour pulled from one
+ * step later). */
+virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi);
+
+/* `steps` steps of a grid split into the n slabs slabs[0..n-1] (in order,
+ * covering planes 1..nz-2): per step every adjacent pair exchanges
+ * (virs_slab_exchange), then every slab takes one step on its own stream.
+ * Slabs on different GPUs of this process run concurrently.  Returns when
+ * the work is queued (virs_synchronize each handle to wait).  Single steps,
+ * no CUDA graph; the device stop rule is refused. */
+virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps);
+
 virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);
 
 /* Replaces buildSpongeLayer / buildSpongeLayerGPU (simulator_dispatch.cpp:83-91,

@@ -65,3 +65,14 @@ def test_facade_matches_python_binding(tmp_path):
     sim.close()
     assert got.size == steps and np.abs(want).max() > 0
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_slab_room_program_compiles(tmp_path):
+    """The C++ slab driver (tests/cpp/slab_room.cpp) builds against the ABI."""
+    if shutil.which("g++") is None or not (LIBDIR / "libvirs_b200.so").exists():
+        pytest.skip("no g++ or library")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{ROOT / 'include'}",
+           str(ROOT / "tests" / "cpp" / "slab_room.cpp"), f"-L{LIBDIR}", "-lvirs_b200", f"-Wl,-rpath,{LIBDIR}",
+           "-o", str(tmp_path / "slab_room")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

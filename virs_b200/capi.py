@@ -111,6 +111,8 @@ _SIGS = {
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_set_time_blocking": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_set_rounding": ([_P, C.c_int], C.c_int),
+    "virs_slab_exchange": ([_P, _P], C.c_int),
+    "virs_slab_run": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "virs_get_time_blocking": ([_P, _P, _P, _P, _P], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
@@ -522,6 +524,19 @@ class Simulation:
         v = [C.c_int() for _ in range(4)]
         check(lib().virs_get_time_blocking(self._h, *[C.byref(x) for x in v]))
         return {"steps_per_pass": v[0].value, "rows": v[1].value, "planes": v[2].value, "active": bool(v[3].value)}
+
+
+def slab_exchange(lo: "Simulation", hi: "Simulation") -> None:
+    """virs_slab_exchange: adjacent slab handles pull each other's edge plane
+    of p^n into their ghost planes, on their own streams."""
+    check(lib().virs_slab_exchange(lo.handle, hi.handle))
+
+
+def slab_run(sims, steps: int) -> None:
+    """virs_slab_run: `steps` steps of the slabs sims (in order, covering the
+    grid), exchanging ghost planes before every step."""
+    arr = (C.c_void_p * len(sims))(*[s.handle.value for s in sims])
+    check(lib().virs_slab_run(arr, len(sims), steps))
 
 
 class Batch:

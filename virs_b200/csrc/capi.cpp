@@ -1660,6 +1660,89 @@ VIRS_EXPORT virs_status virs_run(virs_sim *s, uint64_t steps, void *stream)
     return run_steps(s, steps, st);
 }
 
+namespace {
+
+// lo and hi are adjacent slabs of one grid at the same step
+virs_status check_slab_pair(const virs_sim *lo, const virs_sim *hi)
+{
+    if (!lo->slab || !hi->slab) return fail(VIRS_E_STATE, "slab exchange: a handle is not a slab (virs_set_grid_slab)");
+    if (!started(lo) || !started(hi)) return fail(VIRS_E_STATE, "slab exchange: call virs_start_simulation first");
+    if (lo->nx != hi->nx || lo->ny != hi->ny || lo->global_nz != hi->global_nz ||
+        lo->prm.storage != hi->prm.storage)
+        return fail(VIRS_E_ARG, "slab exchange: the slabs belong to different grids or storages");
+    if (lo->slab_hi != hi->slab_lo)
+        return fail(VIRS_E_ARG, "slab exchange: the slabs are not adjacent (lo owns planes up to " +
+                                    std::to_string(lo->slab_hi) + ", hi starts at " + std::to_string(hi->slab_lo) + ")");
+    if (lo->steps_done != hi->steps_done || lo->cur != hi->cur)
+        return fail(VIRS_E_STATE, "slab exchange: the slabs are not at the same step");
+    if (!lo->fields_valid || !hi->fields_valid)
+        return fail(VIRS_E_STATE, "slab exchange: the fields were consumed by virs_adjoint");
+    return VIRS_OK;
+}
+
+// p^n plane k of a slab's current buffer
+char *slab_plane(const virs_sim *s, uint64_t k)
+{
+    return s->field[s->cur].as<char>() + k * (size_t)s->px * s->ny * s->storage_bytes();
+}
+
+// each handle pulls its ghost plane from the other on its own stream, after
+// the other's last queued work; then each handle's completion event follows
+// the copy into its ghost plane
+virs_status slab_exchange(virs_sim *lo, virs_sim *hi)
+{
+    const size_t pb = (size_t)lo->px * lo->ny * lo->storage_bytes();
+    VIRS_TRY(use_device(lo));
+    VIRS_CUDA(cudaStreamWaitEvent(lo->stream, hi->done, 0));
+    VIRS_TRY(use_device(hi));
+    VIRS_CUDA(cudaStreamWaitEvent(hi->stream, lo->done, 0));
+    VIRS_TRY(use_device(lo));
+    VIRS_CUDA(cudaMemcpyAsync(slab_plane(lo, lo->nz - 1), slab_plane(hi, 1), pb, cudaMemcpyDefault, lo->stream));
+    VIRS_CUDA(cudaEventRecord(lo->done, lo->stream));
+    VIRS_TRY(use_device(hi));
+    VIRS_CUDA(cudaMemcpyAsync(slab_plane(hi, 0), slab_plane(lo, lo->nz - 2), pb, cudaMemcpyDefault, hi->stream));
+    VIRS_CUDA(cudaEventRecord(hi->done, hi->stream));
+    return VIRS_OK;
+}
+
+} // namespace
+
+VIRS_EXPORT virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi)
+{
+    if (!lo || !hi) return fail(VIRS_E_ARG, "virs_slab_exchange: null argument");
+    VIRS_TRY(check_slab_pair(lo, hi));
+    return slab_exchange(lo, hi);
+}
+
+VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps)
+{
+    if (!slabs || n == 0) return fail(VIRS_E_ARG, "virs_slab_run: no slabs");
+    for (uint32_t k = 0; k < n; ++k) {
+        if (!slabs[k]) return fail(VIRS_E_ARG, "virs_slab_run: null slab");
+        if (slabs[k]->stop_rule) return fail(VIRS_E_STATE, "virs_slab_run: the device stop rule is not for slabs");
+    }
+    if (n == 1) {
+        const virs_sim *s = slabs[0];
+        if (!s->slab || !started(s)) return fail(VIRS_E_STATE, "virs_slab_run: a started slab handle is needed");
+    }
+    for (uint32_t k = 0; k + 1 < n; ++k) VIRS_TRY(check_slab_pair(slabs[k], slabs[k + 1]));
+    if (slabs[0]->slab_lo != 1 || slabs[n - 1]->slab_hi != slabs[0]->global_nz - 1)
+        return fail(VIRS_E_ARG, "virs_slab_run: the slabs must cover the grid's interior planes, in order");
+    if (slabs[0]->steps_done + steps >= (1ull << 32)) return fail(VIRS_E_ARG, "step counter would pass 2^32");
+    for (uint64_t i = 0; i < steps; ++i) {
+        // every exchange before any step: a slab's step writes the buffer
+        // its neighbours pulled from one step later, and each pull follows
+        // the neighbour's previous step
+        for (uint32_t k = 0; k + 1 < n; ++k) VIRS_TRY(slab_exchange(slabs[k], slabs[k + 1]));
+        for (uint32_t k = 0; k < n; ++k) {
+            virs_sim *s = slabs[k];
+            VIRS_TRY(use_device(s));
+            VIRS_TRY(run_steps(s, 1, s->stream));
+        }
+    }
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_synchronize(virs_sim *s)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_synchronize: null");
