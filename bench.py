@@ -324,6 +324,45 @@ def bench_batch(storage, args, stream, dev, dist=None):
 CPU_CROP_PLANES = 16   # planes of the hall crop both CPU figures time
 
 
+def bench_adjoint(args, stream, dev):
+    """The inverse-design configuration: 128x128x96, 6 materials x 2
+    sections, 4 receivers, 4000 steps, checkpoints every 64.  The forward
+    pass (virs_forward_checkpointed) is timed with CUDA events; the reverse
+    pass (virs_adjoint: recomputation of every segment, the adjoint steps,
+    the FP64 gradient sums, gradients copied to the host) by the host clock
+    around the synchronous call."""
+    import torch
+    from virs_b200 import scenes
+    sc, guess = scenes.inverse_design()
+    every = 64
+    sim, _ = scenes.build_simulation(sc)
+    nvox = int(np.prod(sim.shape))
+    sim.forward_checkpointed(256, every)             # warm-up: both passes once on a short run
+    sim.adjoint(np.zeros((len(sc.rcv_pos), 256), np.float32), sc.n_materials, sc.n_sections)
+    sim.start(sc.steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.forward_checkpointed(sc.steps, every, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    ir = sim.ir(0, sc.steps)
+    dl = (2.0 * ir / ir.size).astype(np.float32)
+    t0 = time.perf_counter()
+    gc, gs = sim.adjoint(dl, sc.n_materials, sc.n_sections)
+    adj_ms = (time.perf_counter() - t0) * 1e3
+    sim.close()
+    return {"workload": "inverse design 128x128x96, 6 materials x 2 sections, 4 receivers, %d steps, "
+                        "checkpoint every %d" % (sc.steps, every),
+            "forward_ms": round(fwd_ms, 2), "adjoint_ms": round(adj_ms, 2),
+            "forward_value": round(nvox * sc.steps / (fwd_ms * 1e-3) / 1e9, 3),
+            "gradient_value": round(nvox * sc.steps / ((fwd_ms + adj_ms) * 1e-3) / 1e9, 3),
+            "unit": "Gvoxel-updates/s (forward; forward + reverse for the gradient)",
+            "grad_finite": bool(np.isfinite(gc).all() and np.isfinite(gs).all())}
+
+
 def cpu_sample(shape, steps_budget_s, threads):
     """The oracle's FP32 step on a crop of the hall (same x, y extent,
     CPU_CROP_PLANES planes), timed on the host in chunks of about a second
@@ -405,6 +444,8 @@ def run_virs(args):
             "kernel_ms": rs.get("kernel_ms"), "kernel_ms_nearest": rb.get("kernel_ms"),
             "boundary_ms": rs.get("boundary_ms"),
         }
+    if args.adjoint:
+        variants["adjoint_inverse_design"] = bench_adjoint(args, stream, dev)
     if args.batch_steps:
         for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):
             rb = bench_batch(st, args, stream, dev, dist)
@@ -579,6 +620,8 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=4, help="steps per candidate of virs_autotune (0 = no tuning)")
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the inverse-design (adjoint) variant")
     ap.add_argument("--batch-steps", type=int, default=60, help="timed steps of the batched workload (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--storage", choices=list(STORAGE_NAMES), default="f32",

@@ -473,6 +473,23 @@ virs_status virs_design_chebyshev_lowpass(double fs, double fc, double fstop, do
 virs_status virs_postprocess_ir(virs_sim *sim, double rate, const double *sos, uint32_t n_sections, int normalize,
                                 float *out, uint64_t capacity, uint64_t *out_len);
 
+/* The same resampling with a band-limited interpolator instead of the
+ * Chebyshev cascade and linear interpolation, in the manner of the
+ * reference's kfr resampler (resample_quality::high, simulator.cpp:1056-1063;
+ * kfr is absent and its design unknown, so the output is not bit-equal to
+ * the reference's): output sample k sits at input position
+ * t = k * fs / rate (fs = 1/dt) and takes sum_n x[n] h(t - n) over the
+ * |t - n| < half_taps input samples around it, with the Kaiser-windowed sinc
+ * h(tau) = 2 fc sinc(2 fc tau) I0(beta sqrt(1 - (tau/half_taps)^2)) / I0(beta),
+ * fc = cutoff * min(fs, rate) / 2 / fs cycles per input sample, in FP64.
+ * Peak normalisation and the output length as virs_postprocess_ir.  For the
+ * reference's default cell (fs = 305.5 kHz) to 48 kHz, half_taps 245,
+ * beta 10.06 and cutoff 0.9167 give a 20-24 kHz transition band and about
+ * 100 dB of stop-band attenuation (the Kaiser design rules).
+ * half_taps 1..4096, beta 0..50, cutoff in (0, 1]. */
+virs_status virs_postprocess_ir_sinc(virs_sim *sim, double rate, uint32_t half_taps, double beta, double cutoff,
+                                     int normalize, float *out, uint64_t capacity, uint64_t *out_len);
+
 /* Failure-path self test (no reference counterpart): launches a kernel that
  * waits `limit` microseconds (1..2^20) on an mbarrier that nothing completes,
  * with the bounded wait of the step kernels; returns VIRS_E_TIMEOUT when the

@@ -407,6 +407,17 @@ def postprocess(ir, dt, rate=48000.0, sos=None, normalize=True):
     return out
 
 
+def resample_sinc(x, fs_in: float, rate: float, out_len: int, half: int, beta: float, cutoff: float,
+                  normalize: bool = False):
+    """One channel through the library's windowed-sinc resampler (FP64)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros(int(out_len), np.float32)
+    lib().vo_resample_sinc(C.c_void_p(x.ctypes.data), C.c_uint64(x.size), C.c_double(fs_in), C.c_double(rate),
+                           C.c_int(int(half)), C.c_double(beta), C.c_double(cutoff), C.c_void_p(out.ctypes.data),
+                           C.c_uint64(out.size), C.c_int(int(normalize)))
+    return out
+
+
 def audio_to_steps(x, rate: float, dt: float, steps: int):
     """An audio signal at `rate` read at step * dt (linear interpolation)."""
     x = np.ascontiguousarray(x, np.float32)

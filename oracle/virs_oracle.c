@@ -1307,6 +1307,52 @@ VO_API void vo_resample(const float *in, uint64_t len, double sim_rate, double r
  * design commented at simulator_gpu.cu:219-231 (float time and index, 0
  * once index + 1 reaches the end of the signal).  IEEE single, no
  * contraction. */
+/* The library's band-limited resampler (virs_postprocess_ir_sinc; no
+ * reference counterpart: the reference resamples with kfr, absent here):
+ * output sample k at input position t = k fs_in / rate is
+ * sum_n x[n] 2 fc sinc(2 fc (t - n)) w(t - n) over |t - n| < half, with
+ * fc = cutoff min(fs_in, rate) / 2 / fs_in, sinc(u) = sin(pi u) / (pi u) and
+ * the Kaiser window w(tau) = I0(beta sqrt(1 - (tau / half)^2)) / I0(beta), I0
+ * from its power series; FP64; then division by the peak if asked. */
+static double vo_bessel_i0(double x)
+{
+    const double q = 0.25 * x * x;
+    double t = 1.0, s = 1.0;
+    for (int k = 1; k < 500; ++k) {
+        t = t * q / ((double)k * (double)k);
+        s = s + t;
+        if (t < 1e-17 * s) break;
+    }
+    return s;
+}
+
+VO_API void vo_resample_sinc(const float *in, uint64_t len, double fs_in, double rate, int half, double beta,
+                             double cutoff, float *out, uint64_t out_len, int normalize)
+{
+    const double fc2 = cutoff * fmin(fs_in, rate) / fs_in, i0b = vo_bessel_i0(beta), ratio = fs_in / rate;
+#pragma omp parallel for schedule(static) num_threads(vo_get_threads())
+    for (int64_t k = 0; k < (int64_t)out_len; ++k) {
+        const double t = (double)k * ratio;
+        const double n0 = fmax(0.0, ceil(t - (double)half)), n1 = fmin((double)len - 1.0, floor(t + (double)half));
+        double acc = 0.0;
+        for (double n = n0; n <= n1; n += 1.0) {
+            const double tau = t - n, u = tau / (double)half;
+            if (!(fabs(u) < 1.0)) continue;
+            const double w = vo_bessel_i0(beta * sqrt(1.0 - u * u)) / i0b;
+            const double x = fc2 * tau;
+            const double sc = x == 0.0 ? 1.0 : sin(M_PI * x) / (M_PI * x);
+            acc += (double)in[(uint64_t)n] * (fc2 * sc * w);
+        }
+        out[k] = (float)acc;
+    }
+    if (normalize) {
+        float peak = 0.f;
+        for (uint64_t k = 0; k < out_len; ++k) peak = fmaxf(peak, fabsf(out[k]));
+        if (peak > 0.f)
+            for (uint64_t k = 0; k < out_len; ++k) out[k] = out[k] / peak;
+    }
+}
+
 VO_API void vo_audio_to_steps(const float *x, uint64_t len, float rate, float dt, uint64_t steps, float *out)
 {
     for (uint64_t n = 0; n < steps; ++n) {

@@ -44,3 +44,21 @@ def test_postprocess_many_receivers_and_sections():
     assert got.shape[0] == raw.shape[0] == 8
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     sim.close()
+
+
+@pytest.mark.parametrize("normalize", [True, False])
+def test_postprocess_sinc_matches_oracle(normalize):
+    """virs_postprocess_ir_sinc against the oracle's restatement of the same
+    windowed-sinc interpolation.  Both sum in FP64 with sin and sqrt of
+    their own libraries, so they agree to rounding: 1e-6 of the peak."""
+    sc = scenes.plain_small(steps=900)
+    sim, _ = scenes.build_simulation(sc)
+    sim.run(sc.steps)
+    raw = sim.ir()
+    dt = float(sim.info().dt)
+    got = sim.postprocess_ir_sinc(48000.0, 64, 8.0, 0.9, normalize)
+    n = int(48000.0 * (sc.steps * dt))
+    want = np.stack([oracle.resample_sinc(r, 1.0 / dt, 48000.0, n, 64, 8.0, 0.9, normalize) for r in raw])
+    assert got.shape == want.shape and np.abs(want).max() > 0
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
+    sim.close()

@@ -111,6 +111,8 @@ _SIGS = {
     "virs_set_tiling": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_set_time_blocking": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
     "virs_set_rounding": ([_P, C.c_int], C.c_int),
+    "virs_postprocess_ir_sinc": ([_P, C.c_double, C.c_uint32, C.c_double, C.c_double, C.c_int, _P, C.c_uint64,
+                                  C.POINTER(C.c_uint64)], C.c_int),
     "virs_slab_exchange": ([_P, _P], C.c_int),
     "virs_slab_run": ([_P, C.c_uint32, C.c_uint64], C.c_int),
     "virs_get_time_blocking": ([_P, _P, _P, _P, _P], C.c_int),
@@ -448,6 +450,19 @@ class Simulation:
         nr = getattr(self, "_nrcv", 0)
         out = np.zeros((max(nr, 1), n.value), np.float32)
         check(lib().virs_postprocess_ir(self._h, rate, _ptr(s6), ns, int(normalize), _ptr(out), out.size, C.byref(n)))
+        return out[:nr]
+
+    def postprocess_ir_sinc(self, rate: float = 48000.0, half_taps: int = 245, beta: float = 10.06,
+                            cutoff: float = 0.9167, normalize: bool = True) -> np.ndarray:
+        """The receiver traces resampled to `rate` by the Kaiser-windowed sinc
+        (virs_postprocess_ir_sinc), peak-normalised if asked."""
+        n = C.c_uint64(0)
+        check(lib().virs_postprocess_ir_sinc(self._h, rate, half_taps, beta, cutoff, int(normalize), None, 0,
+                                             C.byref(n)))
+        nr = getattr(self, "_nrcv", 0)
+        out = np.zeros((max(nr, 1), n.value), np.float32)
+        check(lib().virs_postprocess_ir_sinc(self._h, rate, half_taps, beta, cutoff, int(normalize), _ptr(out),
+                                             out.size, C.byref(n)))
         return out[:nr]
 
     def pressure(self, prev: bool = False):

@@ -1902,6 +1902,35 @@ VIRS_EXPORT virs_status virs_postprocess_ir(virs_sim *s, double rate, const doub
     return VIRS_OK;
 }
 
+VIRS_EXPORT virs_status virs_postprocess_ir_sinc(virs_sim *s, double rate, uint32_t half_taps, double beta,
+                                                 double cutoff, int normalize, float *out, uint64_t capacity,
+                                                 uint64_t *out_len)
+{
+    if (!s || !out_len) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: null argument");
+    if (!(rate > 0.0) || !std::isfinite(rate)) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: rate must be > 0");
+    if (half_taps < 1 || half_taps > 4096) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: half_taps must be 1..4096");
+    if (!(beta >= 0.0) || !(beta <= 50.0)) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: beta must be 0..50");
+    if (!(cutoff > 0.0) || !(cutoff <= 1.0)) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: cutoff must be in (0, 1]");
+    if (!(s->dt > 0.f)) return fail(VIRS_E_STATE, "virs_postprocess_ir_sinc: no grid");
+    const uint64_t steps = s->steps_done;
+    const uint64_t len = (uint64_t)(rate * ((double)steps * (double)s->dt));
+    *out_len = len;
+    if (!out || !len || !s->nrcv) return VIRS_OK;
+    if (capacity < len) return fail(VIRS_E_ARG, "virs_postprocess_ir_sinc: capacity smaller than the output length");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(wait_done(s));
+    VIRS_TRY(check_err(s));
+    cudaStream_t st = s->stream;
+    DevBuf res, peak;
+    VIRS_TRY(res.alloc((size_t)s->nrcv * len * sizeof(float), "resampled receiver traces"));
+    if (normalize) VIRS_TRY(peak.alloc((size_t)s->nrcv * sizeof(uint32_t), "receiver peaks"));
+    VIRS_CUDA(launch_ir_sinc(s->ir.as<float>(), s->ircap, steps, 1.0 / (double)s->dt, rate, (int)half_taps, beta,
+                             cutoff, res.as<float>(), len, normalize ? peak.as<uint32_t>() : nullptr, s->nrcv, st));
+    VIRS_CUDA(cudaMemcpyAsync(out, res.ptr, (size_t)s->nrcv * len * sizeof(float), cudaMemcpyDeviceToHost, st));
+    VIRS_CUDA(cudaStreamSynchronize(st));
+    return VIRS_OK;
+}
+
 VIRS_EXPORT virs_status virs_get_pressure(const virs_sim *s, float *cur, float *prev, size_t n)
 {
     if (!s || !cur) return fail(VIRS_E_ARG, "virs_get_pressure: null argument");

@@ -254,6 +254,9 @@ cudaError_t launch_voxelize(const float *verts, const uint32_t *tris, const int3
 // IR post-processing (kernels_ir.cu)
 cudaError_t launch_ir_sos(const float *in, uint64_t in_stride, uint64_t len, const double *sos, int ns, float *out,
                           uint64_t out_stride, uint32_t channels, cudaStream_t s);
+cudaError_t launch_ir_sinc(const float *in, uint64_t in_stride, uint64_t len, double fs_in, double rate, int half,
+                           double beta, double cutoff, float *out, uint64_t out_len, uint32_t *peak, uint32_t channels,
+                           cudaStream_t s);
 cudaError_t launch_ir_resample(const float *in, uint64_t in_stride, uint64_t len, double sim_rate, float rate,
                                float *out, uint64_t out_len, int normalize, uint32_t channels, cudaStream_t s);
 

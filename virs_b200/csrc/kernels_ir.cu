@@ -95,7 +95,79 @@ __global__ void __launch_bounds__(RB) k_ir_resample(const float *__restrict in, 
     for (uint64_t k = threadIdx.x; k < out_len; k += RB) o[k] = __fdiv_rn(o[k], peak);
 }
 
+// Band-limited resampling with a Kaiser-windowed sinc: output sample k is
+// at input position t = k * fs_in / rate; y_k = sum over the input samples
+// n with |t - n| < half of x[n] * 2 fc sinc(2 fc (t - n)) * w(t - n), with
+// fc = cutoff * min(fs_in, rate) / 2 / fs_in (cycles per input sample),
+// sinc(u) = sin(pi u) / (pi u) and the Kaiser window
+// w(tau) = I0(beta sqrt(1 - (tau / half)^2)) / I0(beta).  I0 is summed from
+// its power series, sum_k ((x / 2)^k / k!)^2.  FP64 throughout; one thread
+// per output sample of one channel (blockIdx.y).
+__device__ double bessel_i0(double x)
+{
+    const double q = 0.25 * x * x;
+    double t = 1.0, s = 1.0;
+    for (int k = 1; k < 500; ++k) {
+        t = t * q / ((double)k * (double)k);
+        s = s + t;
+        if (t < 1e-17 * s) break;
+    }
+    return s;
+}
+
+__global__ void __launch_bounds__(RB) k_ir_sinc(const float *__restrict in, uint64_t in_stride, uint64_t len,
+                                                double step_ratio, double fc2, int half, double beta, double i0b,
+                                                float *__restrict out, uint64_t out_len, uint32_t *__restrict peak)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * RB + threadIdx.x;
+    if (k >= out_len) return;
+    const float *f = in + blockIdx.y * in_stride;
+    const double t = (double)k * step_ratio;
+    const double n0 = fmax(0.0, ceil(t - (double)half)), n1 = fmin((double)len - 1.0, floor(t + (double)half));
+    double acc = 0.0;
+    for (double n = n0; n <= n1; n += 1.0) {
+        const double tau = t - n, u = tau / (double)half;
+        if (!(fabs(u) < 1.0)) continue;
+        const double w = bessel_i0(beta * sqrt(1.0 - u * u)) / i0b;
+        const double x = fc2 * tau;
+        const double sc = x == 0.0 ? 1.0 : sin(M_PI * x) / (M_PI * x);
+        acc += (double)f[(uint64_t)n] * (fc2 * sc * w);
+    }
+    const float v = (float)acc;
+    out[blockIdx.y * out_len + k] = v;
+    if (peak) atomicMax(peak + blockIdx.y, __float_as_uint(fabsf(v))); // non-negative floats order as integers
+}
+
+__global__ void k_ir_normalize(float *__restrict out, uint64_t out_len, const uint32_t *__restrict peak)
+{
+    const uint64_t k = (uint64_t)blockIdx.x * RB + threadIdx.x;
+    const float p = __uint_as_float(peak[blockIdx.y]);
+    if (k < out_len && p > 0.f) out[blockIdx.y * out_len + k] = __fdiv_rn(out[blockIdx.y * out_len + k], p);
+}
+
 } // namespace
+
+cudaError_t launch_ir_sinc(const float *in, uint64_t in_stride, uint64_t len, double fs_in, double rate, int half,
+                           double beta, double cutoff, float *out, uint64_t out_len, uint32_t *peak, uint32_t channels,
+                           cudaStream_t s)
+{
+    if (!channels || !out_len || !len) return cudaSuccess;
+    const double fc2 = cutoff * fmin(fs_in, rate) / fs_in;        // 2 fc
+    double i0b = 1.0, t = 1.0;
+    for (int k = 1; k < 500; ++k) {                                // I0(beta), as the kernel sums it
+        t = t * (0.25 * beta * beta) / ((double)k * (double)k);
+        i0b = i0b + t;
+        if (t < 1e-17 * i0b) break;
+    }
+    const dim3 g((unsigned)((out_len + RB - 1) / RB), channels);
+    if (peak) {
+        cudaError_t e = cudaMemsetAsync(peak, 0, channels * sizeof(uint32_t), s);
+        if (e != cudaSuccess) return e;
+    }
+    k_ir_sinc<<<g, RB, 0, s>>>(in, in_stride, len, fs_in / rate, fc2, half, beta, i0b, out, out_len, peak);
+    if (peak) k_ir_normalize<<<g, RB, 0, s>>>(out, out_len, peak);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_ir_sos(const float *in, uint64_t in_stride, uint64_t len, const double *sos, int ns, float *out,
                           uint64_t out_stride, uint32_t channels, cudaStream_t s)
