@@ -432,6 +432,8 @@ def run_virs(args):
             if rb.get("kernel_ms") else None,
             "bytes_per_voxel": BYTES_16,
             "kernel": bkern.split(" ")[0],
+            "kernel_ms": rb.get("kernel_ms"),
+            "boundary_ms": rb.get("boundary_ms"),
             "time_blocking": rb["time_blocking"],
         }
         # the same with stochastic rounding of the 16-bit stores: the cost of

@@ -5,8 +5,8 @@ must equal the oracle bit for bit, in every kernel variant, in batches and
 in z-slabs (whose voxels take the whole grid's keys).
 
 Accuracy on the 128^3 crop of the hall over 4000 steps against the FP64
-oracle, as measured with the oracle's identical rounding: FP16 5.1e-3 (7.2e-3
-to nearest), BF16 4.0e-2 (2.4e-1 to nearest).  Regression bound 1.25x that;
+oracle, as measured on a B200 (the library's automatic storage scale):
+FP16 5.2e-3 (5.8e-3 to nearest), BF16 4.0e-2 (2.4e-1 to nearest).  Regression bound 1.25x that;
 the 1e-3 target is a strict expected failure."""
 import dataclasses
 
@@ -156,7 +156,7 @@ def test_sr_slabs_equal_whole_grid():
 # ---- accuracy against FP64 on the hall crop -------------------------------------
 
 STEPS = 4000
-CROP_SR_MEASURED = {capi.STORAGE_F16: 5.1e-3, capi.STORAGE_BF16: 4.0e-2}
+CROP_SR_MEASURED = {capi.STORAGE_F16: 5.2e-3, capi.STORAGE_BF16: 4.0e-2}
 IR_TARGET = 1e-3
 
 
@@ -185,7 +185,7 @@ def test_sr_crop_error_regression(crop, storage):
     assert _crop_sr_error(crop, storage) <= 1.25 * CROP_SR_MEASURED[storage]
 
 
-@pytest.mark.xfail(strict=True, reason="stochastic rounding on the hall crop: measured FP16 5.1e-3, BF16 4.0e-2 "
+@pytest.mark.xfail(strict=True, reason="stochastic rounding on the hall crop: measured FP16 5.2e-3, BF16 4.0e-2 "
                                        "over 4000 steps against the 1e-3 target")
 @pytest.mark.parametrize("storage", [capi.STORAGE_F16, capi.STORAGE_BF16])
 def test_sr_crop_error_meets_target(crop, storage):

@@ -123,7 +123,7 @@ struct virs_sim {
 
     // boundary
     uint64_t nb = 0;
-    DevBuf bidx, bpos, bcode, bnrm, bmat, bw, state;
+    DevBuf bidx, bpos, bcode, bnrm, bmat, bw, brec, state;
     DevBuf hpos;                   // hard-source voxel positions
     uint32_t nhpos = 0;
 
@@ -371,7 +371,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->segnz, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos,
+                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->brec, &s->state, &s->side, &s->hpos,
                       &s->spare[0], &s->spare[1], &s->plist, &s->pzmask})
         b->release();
     const size_t ext = (size_t)s->px * ny * s->ext_nz;
@@ -629,6 +629,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.code = s->code.as<uint8_t>();
     a.normals = s->normals.as<uint8_t>();
     a.bpos = s->bpos.as<uint32_t>();
+    a.brec = s->brec.as<uint4>();
     a.l2 = s->l2;
     a.rigid = s->prm.rigid_walls ? 1 : 0;
     if (s->stop_rule) a.stop = s->stopbuf.as<uint32_t>();
@@ -643,6 +644,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.nb = s->nb;
     a.nhard = s->nhard;
     a.nsec = s->nsec;
+    a.ncoef = (uint32_t)(s->nmat * s->nsec * 5);
     a.nx = s->nx;
     a.ny = s->ny;
     a.nz = s->nz;
@@ -1332,6 +1334,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(s->bcode.alloc(std::max<uint64_t>(nb, 1), "boundary codes"));
         VIRS_TRY(s->bnrm.alloc(std::max<uint64_t>(nb, 1), "boundary normals"));
         VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
+        VIRS_TRY(s->brec.alloc(std::max<uint64_t>(nb, 1) * 16, "boundary slot records"));
         VIRS_TRY(s->side.alloc(std::max<uint64_t>(nb, 1) * sizeof(float4), "boundary records"));
         CompactArgs cp{};
         cp.flags = s->flags.as<uint8_t>();
@@ -1347,6 +1350,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         cp.bcode = s->bcode.as<uint8_t>();
         cp.bnrm = s->bnrm.as<uint8_t>();
         cp.bw = s->bw.as<float>();
+        cp.brec = s->brec.as<uint4>();
         cp.nx = s->nx;
         cp.ny = s->ny;
         cp.nz = s->nz;
@@ -2453,7 +2457,8 @@ cudaError_t batch_enqueue(const virs_batch *b, int parity, cudaStream_t st)
     const BatchMember *d = b->desc.as<BatchMember>();
     const uint32_t n = (uint32_t)b->mem.size();
     cudaError_t e =
-        launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->persistent, b->err.as<int>(), st);
+        launch_step_tma_batch(b->storage, b->rows, b->depth, d, n, b->ntiles, parity, b->persistent, b->err.as<int>(), st,
+                              sr_on(b->mem[0]));
     if (e != cudaSuccess) return e;
     e = launch_boundary_batch(b->storage, d, n, b->nbnd, parity, b->max_sections, st);
     if (e != cudaSuccess) return e;
@@ -2523,6 +2528,8 @@ VIRS_EXPORT virs_status virs_batch_create(virs_sim *const *sims, uint32_t n, vir
         if (!started(sims[i])) return fail(VIRS_E_STATE, "batch members must be started (virs_start_simulation)");
         if (sims[i]->prm.device != sims[0]->prm.device || sims[i]->prm.storage != sims[0]->prm.storage)
             return fail(VIRS_E_ARG, "batch members must share the device and the storage type");
+        if (sr_on(sims[i]) != sr_on(sims[0]))
+            return fail(VIRS_E_ARG, "batch members must share the rounding of their 16-bit stores");
         for (uint32_t j = 0; j < i; ++j)
             if (sims[j] == sims[i]) return fail(VIRS_E_ARG, "a simulation appears twice in the batch");
     }

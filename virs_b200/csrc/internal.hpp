@@ -76,6 +76,7 @@ struct StepArgs {
     const uint8_t *code;
     const uint8_t *normals; // air-neighbour mask (rigid-wall update)
     const uint32_t *bpos;   // [nb] padded device index of each boundary slot
+    const uint4 *brec;      // [nb] per slot {bpos, bcode | bnrm << 8 | bmat << 16, bw bits, 0}: one 16-byte load
     const uint8_t *bcode;   // [nb] cell code of each slot's voxel (read in slot order, not gathered)
     const uint8_t *bnrm;    // [nb] air-neighbour mask of each slot's voxel (rigid-wall update)
     const uint8_t *bmat;
@@ -87,6 +88,7 @@ struct StepArgs {
     uint64_t nb;
     uint32_t nhard;
     uint32_t nsec;
+    uint32_t ncoef;         // values in coef: materials x sections x 5
     uint32_t nx, ny, nz, px;
     int zc;                 // planes per block
     int form;               // VIRS_BOUNDARY_*
@@ -130,7 +132,7 @@ struct alignas(64) BatchMember {
     uint32_t gx, gy, gz;    // tile grid
 };
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
-                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s);
+                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s, bool sr);
 cudaError_t launch_boundary_batch(int storage, const BatchMember *mem, uint32_t nmem, uint64_t nbnd, int parity,
                                   uint32_t max_sections, cudaStream_t s);
 cudaError_t launch_post_batch(int storage, const BatchMember *mem, uint32_t nmem, int parity, cudaStream_t s);
@@ -220,6 +222,7 @@ struct CompactArgs {
     uint8_t *bcode, *bnrm;     // ... copied per slot
     uint8_t *bmat;
     float *bw;
+    uint4 *brec;               // the per-slot record the boundary pass reads
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);

@@ -207,8 +207,10 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bars, uint32_t j, int D, in
     return bounded_wait(bars + (j % D), (j / D) & 1u, WAIT_LIMIT_NS, err);
 }
 
-// The per-tile constants of the plane loop.
-template <typename T, int TY, int L> struct Tile {
+// The per-tile constants of the plane loop.  SR: the 16-bit stores round
+// stochastically (a compile-time choice, so that the default path carries
+// no trace of it).
+template <typename T, int TY, int L, bool SR = false> struct Tile {
     const StepArgs *a;
     unsigned char *smem;
     uint64_t *bars;
@@ -279,7 +281,7 @@ template <typename T, int TY, int L> struct Tile {
         float r[V];
         tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, r);
         if (act) {
-            if (a->sr) st_sr<T>(out, r, (uint64_t)(out - static_cast<T *>(a->q)), a->sr_base, srk);
+            if constexpr (SR) st_sr<T>(out, r, (uint64_t)(out - static_cast<T *>(a->q)), a->sr_base, srk);
             else IO::st(out, r);
         }
         out += plane;
@@ -299,7 +301,7 @@ template <typename T, int TY, int L> struct Tile {
 // stages: it continues across tiles so that the ring slot and mbarrier
 // phase of every stage stay consistent when a block processes several
 // tiles (the batched kernel).  Returns false when a bounded wait gave up.
-template <typename T, int TY, int L>
+template <typename T, int TY, int L, bool SR>
 __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *mP, const CUtensorMap *mQ,
                                           const CUtensorMap *mC, int bx, int by, int bz, int *err, unsigned char *smem,
                                           uint64_t *bars, uint32_t &jg)
@@ -311,7 +313,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     constexpr int D = L + 2;
     static_assert(IO::VEC == V && V % 2 == 0, "one 16-byte vector per thread, an even number of voxels");
 
-    Tile<T, TY, L> t;
+    Tile<T, TY, L, SR> t;
     const int lane = threadIdx.x, tid = threadIdx.y * 32 + lane;
     t.a = &a;
     t.smem = smem;
@@ -336,7 +338,7 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.t0 = t.row * TX + t.sl * V;            // ... and in a tile box
     t.c2dt2 = make_float2(a.c2dt2, a.c2dt2);
     t.inv_h2 = make_float2(a.inv_h2, a.inv_h2);
-    t.srk = a.sr ? sr_step_key(*a.ctr, 0u) : 0u;
+    t.srk = SR ? sr_step_key(*a.ctr, 0u) : 0u;
     t.plane = (size_t)a.px * a.ny;
     {
         const uint32_t gx = (a.px + TX - 1) / TX, gy = (a.ny + TY - 1) / TY;
@@ -387,7 +389,7 @@ template <typename T, int TY> constexpr int min_blocks()
     return block_threads<T, TY>() >= 768 ? 1 : 768 / block_threads<T, TY>();
 }
 
-template <typename T, int TY, int L>
+template <typename T, int TY, int L, bool SR>
 __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k_step_tma(const __grid_constant__ StepArgs a,
                                                                         const __grid_constant__ CUtensorMap mP,
                                                                         const __grid_constant__ CUtensorMap mQ,
@@ -399,14 +401,14 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + D * Stage<T, TY>::SB);
     init_bars<D>(bars);
     uint32_t jg = 0;
-    step_tile<T, TY, L>(a, &mP, &mQ, &mC, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
+    step_tile<T, TY, L, SR>(a, &mP, &mQ, &mC, blockIdx.x, blockIdx.y, blockIdx.z, err, smem, bars, jg);
 }
 
 // Many simulations in one launch: the blocks walk the concatenated tile
 // lists of all members (tiles of a member are consecutive, so neighbouring
 // tiles run at the same time and share the halo rows in L2), either one
 // tile per block or, persistent, a single wave of blocks striding over all.
-template <typename T, int TY, int L>
+template <typename T, int TY, int L, bool SR>
 __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k_step_tma_batch(const BatchMember *__restrict mem,
                                                                               uint32_t nmem, uint64_t ntiles,
                                                                               int parity, int *err)
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(block_threads<T, TY>(), min_blocks<T, TY>()) k
         const uint64_t local = w - b.first_tile;
         const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / ((uint64_t)b.gx * b.gy));
         __syncthreads(); // every thread is done with the previous tile's stages
-        if (!step_tile<T, TY, L>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, bx, by, bz, err, smem,
+        if (!step_tile<T, TY, L, SR>(b.step[parity], &b.mapP[parity], &b.mapQ[parity ^ 1], &b.mapC, bx, by, bz, err, smem,
                                  bars, jg))
             return;
     }
@@ -437,7 +439,8 @@ template <typename T, int TY, int L> constexpr size_t smem_bytes()
 template <typename T, int TY, int L>
 cudaError_t launch3(const StepArgs &a, const TmaMaps &m, int *err, cudaStream_t s)
 {
-    auto kern = k_step_tma<T, TY, L>;
+    // stochastic rounding of the stores only exists for 16-bit storage
+    auto kern = (sizeof(T) == 2 && a.sr) ? k_step_tma<T, TY, L, sizeof(T) == 2> : k_step_tma<T, TY, L, false>;
     constexpr size_t sm = smem_bytes<T, TY, L>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -484,9 +487,9 @@ __global__ void k_wait_probe(int *err, uint32_t limit_us)
 
 template <typename T, int TY, int L>
 cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity, bool persistent, int *err,
-                          cudaStream_t s)
+                          cudaStream_t s, bool mem_sr)
 {
-    auto kern = k_step_tma_batch<T, TY, L>;
+    auto kern = (sizeof(T) == 2 && mem_sr) ? k_step_tma_batch<T, TY, L, sizeof(T) == 2> : k_step_tma_batch<T, TY, L, false>;
     constexpr size_t sm = smem_bytes<T, TY, L>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -505,23 +508,23 @@ cudaError_t launch_batch3(const BatchMember *mem, uint32_t nmem, uint64_t ntiles
 
 template <typename T, int TY>
 cudaError_t launch_batch2(int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity,
-                          bool persistent, int *err, cudaStream_t s)
+                          bool persistent, int *err, cudaStream_t s, bool sr)
 {
     switch (depth) {
-    case 1: return launch_batch3<T, TY, 1>(mem, nmem, ntiles, parity, persistent, err, s);
-    case 3: return launch_batch3<T, TY, 3>(mem, nmem, ntiles, parity, persistent, err, s);
-    default: return launch_batch3<T, TY, 2>(mem, nmem, ntiles, parity, persistent, err, s);
+    case 1: return launch_batch3<T, TY, 1>(mem, nmem, ntiles, parity, persistent, err, s, sr);
+    case 3: return launch_batch3<T, TY, 3>(mem, nmem, ntiles, parity, persistent, err, s, sr);
+    default: return launch_batch3<T, TY, 2>(mem, nmem, ntiles, parity, persistent, err, s, sr);
     }
 }
 
 template <typename T>
 cudaError_t launch_batch1(int rows, int depth, const BatchMember *mem, uint32_t nmem, uint64_t ntiles, int parity,
-                          bool persistent, int *err, cudaStream_t s)
+                          bool persistent, int *err, cudaStream_t s, bool sr)
 {
     switch (rows) {
-    case 4: return launch_batch2<T, 4>(depth, mem, nmem, ntiles, parity, persistent, err, s);
-    case 16: return launch_batch2<T, 16>(depth, mem, nmem, ntiles, parity, persistent, err, s);
-    default: return launch_batch2<T, 8>(depth, mem, nmem, ntiles, parity, persistent, err, s);
+    case 4: return launch_batch2<T, 4>(depth, mem, nmem, ntiles, parity, persistent, err, s, sr);
+    case 16: return launch_batch2<T, 16>(depth, mem, nmem, ntiles, parity, persistent, err, s, sr);
+    default: return launch_batch2<T, 8>(depth, mem, nmem, ntiles, parity, persistent, err, s, sr);
     }
 }
 
@@ -819,15 +822,15 @@ cudaError_t pair1(int rows, const StepArgs &a, const TmaMaps &m, void *zout, voi
 } // namespace
 
 cudaError_t launch_step_tma_batch(int storage, int tile_rows, int depth, const BatchMember *mem, uint32_t nmem,
-                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s)
+                                  uint64_t ntiles, int parity, bool persistent, int *err, cudaStream_t s, bool sr)
 {
     if (ntiles == 0) return cudaSuccess;
     switch (storage) {
     case VIRS_STORAGE_F16:
-        return launch_batch1<__half>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
+        return launch_batch1<__half>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s, sr);
     case VIRS_STORAGE_BF16:
-        return launch_batch1<__nv_bfloat16>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
-    default: return launch_batch1<float>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s);
+        return launch_batch1<__nv_bfloat16>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s, sr);
+    default: return launch_batch1<float>(tile_rows, depth, mem, nmem, ntiles, parity, persistent, err, s, false);
     }
 }
 
