@@ -29,12 +29,15 @@ def test_committed_traffic_summaries():
     for f, storages in (("k_pair_tma_dram_traffic.txt", ["f32"]), ("k_step_tma_dram_traffic.txt", ["f32", "bf16"])):
         for st in storages:
             tr = bench.measured_traffic(ROOT / "profiles" / f, st, hall)
-            assert tr is not None and "captured on" not in tr["source"]
+            # captured on the 512x384x256 crop and scaled to the hall
+            assert tr is not None and "captured on 50331648 voxels and scaled by 8.000" in tr["source"]
             per_voxel = tr["bytes"] / hall
             # no re-reads: at or below the algorithmic bytes per voxel and launch
             want = {"k_pair_tma_dram_traffic.txt": 17.0}.get(f, 13.0 if st == "f32" else 7.0)
             assert 0.8 * want < per_voxel <= want
     # a smaller workload: scaled by the voxel count, and said so
     tr = bench.measured_traffic(ROOT / "profiles" / "k_pair_tma_dram_traffic.txt", "f32", hall // 2)
-    assert "scaled by 0.500" in tr["source"]
+    assert "scaled by 4.000" in tr["source"]
+    tr = bench.measured_traffic(ROOT / "profiles" / "k_pair_tma_dram_traffic.txt", "f32", 512 * 384 * 256)
+    assert "captured on" not in tr["source"]
     assert bench.measured_traffic(ROOT / "profiles" / "k_pair_tma_dram_traffic.txt", "bf16", hall) is None
