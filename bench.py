@@ -363,6 +363,30 @@ def bench_adjoint(args, stream, dev):
             "grad_finite": bool(np.isfinite(gc).all() and np.isfinite(gs).all())}
 
 
+def bench_slabs(sc, args, dev, parts=2, steps=100):
+    """The hall split into `parts` z-slabs on this GPU, advanced by
+    virs_slab_run (ghost planes exchanged by device copies before every
+    step, single steps, no graph): the cost of the slab machinery against
+    the whole grid.  Timed by the host clock around the queued run and a
+    synchronisation of every slab."""
+    from virs_b200 import capi, scenes
+    parts_, meta = scenes.build_slabs(sc, parts, device=dev)
+    sims = [p[0] for p in parts_]
+    nvox = int(np.prod(meta["shape"]))
+    capi.slab_run(sims, 8)                              # warm-up
+    for s in sims:
+        s.synchronize()
+    t0 = time.perf_counter()
+    capi.slab_run(sims, steps)
+    for s in sims:
+        s.synchronize()
+    secs = time.perf_counter() - t0
+    for s in sims:
+        s.close()
+    return {"parts": parts, "steps": steps, "value": round(nvox * steps / secs / 1e9, 3),
+            "ms_per_step": secs * 1e3 / steps, "timing": "host clock around virs_slab_run and the synchronisations"}
+
+
 def cpu_sample(shape, steps_budget_s, threads):
     """The oracle's FP32 step on a crop of the hall (same x, y extent,
     CPU_CROP_PLANES planes), timed on the host in chunks of about a second
@@ -448,6 +472,8 @@ def run_virs(args):
         }
     if args.adjoint:
         variants["adjoint_inverse_design"] = bench_adjoint(args, stream, dev)
+    if args.slabs and world == 1:
+        variants["slabs_2_one_gpu"] = bench_slabs(sc, args, dev)
     if args.batch_steps:
         for name, st in (("batched_f32", capi.STORAGE_F32), ("batched_bf16", capi.STORAGE_BF16)):
             rb = bench_batch(st, args, stream, dev, dist)
@@ -622,6 +648,8 @@ def main():
     ap.add_argument("--tune-steps", type=int, default=4, help="steps per candidate of virs_autotune (0 = no tuning)")
     ap.add_argument("--no-variants", dest="variants", action="store_false")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-slabs", dest="slabs", action="store_false",
+                    help="skip the variant that runs the hall as two z-slabs on one GPU")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the inverse-design (adjoint) variant")
     ap.add_argument("--batch-steps", type=int, default=60, help="timed steps of the batched workload (0 = skip)")
