@@ -577,13 +577,6 @@ template <typename T, int TY> struct PStage {
     static constexpr uint32_t RB = ((TY + 2) * TX * sizeof(T) + 127u) & ~127u;
 };
 
-// V values rounded to the storage type, as a store and a reload would give
-template <typename T> __device__ __forceinline__ void round_to(float (&r)[Lay<T>::V])
-{
-#pragma unroll
-    for (int k = 0; k < Lay<T>::V; ++k) r[k] = Io<T>::get(Io<T>::put(r[k]));
-}
-
 // a plain 16-byte store of V values (shared memory)
 __device__ __forceinline__ void put_vec(float *p, const float (&r)[4])
 {
@@ -666,9 +659,18 @@ template <typename T, int TY, int L> struct PairTile {
             if (sl == 0) left = IO::ld1(Ph + c0 - 1);
             if (sl == LPR - 1) right = IO::ld1(Ph + c0 + V);
             tile_update<T>(code, cc, left, right, yp, ym, zp, zm, qv, c2dt2, inv_h2, a->c2dt2, a->inv_h2, up);
-            round_to<T>(up);
-            put_vec(ring + (uint32_t)(i & 1) * (S::RB / sizeof(T)) + r0, up);
-            if (inner && z >= zs && z < z1) IO::st(zout, up);
+            T *rslot = ring + (uint32_t)(i & 1) * (S::RB / sizeof(T)) + r0;
+            if constexpr (sizeof(T) == 2) {
+                // rounded once: the packed vector goes to the ring and to
+                // p^{n+1}, and its values feed the second step
+                const uint4 pk = IO::pack(up);
+                IO::unpack(pk, up);
+                *reinterpret_cast<uint4 *>(rslot) = pk;
+                if (inner && z >= zs && z < z1) IO::st_packed(zout, pk);
+            } else {
+                put_vec(rslot, up);
+                if (inner && z >= zs && z < z1) IO::st(zout, up);
+            }
             zout += plane;
             // second step: p^{n+2}(z-1), from the ring plane written in the
             // previous iteration (visible since this iteration's barrier).

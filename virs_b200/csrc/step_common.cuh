@@ -61,6 +61,16 @@ template <> struct Io<__half> {
         for (int i = 0; i < 4; ++i) h[i] = __floats2half2_rn(r[2 * i], r[2 * i + 1]);
         __stcs(reinterpret_cast<uint4 *>(p), v);
     }
+    // V values rounded to FP16 in one 16-byte vector, and a streaming store of one
+    __device__ static uint4 pack(const float (&r)[VEC])
+    {
+        uint4 v;
+        __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2half2_rn(r[2 * i], r[2 * i + 1]);
+        return v;
+    }
+    __device__ static void st_packed(__half *p, uint4 v) { __stcs(reinterpret_cast<uint4 *>(p), v); }
     __device__ static float ld1(const __half *p) { return __half2float(*p); }
     __device__ static float get(__half v) { return __half2float(v); }
     __device__ static __half put(float v) { return __float2half_rn(v); }
@@ -91,6 +101,15 @@ template <> struct Io<__nv_bfloat16> {
         for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(r[2 * i], r[2 * i + 1]);
         __stcs(reinterpret_cast<uint4 *>(p), v);
     }
+    __device__ static uint4 pack(const float (&r)[VEC])
+    {
+        uint4 v;
+        __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(r[2 * i], r[2 * i + 1]);
+        return v;
+    }
+    __device__ static void st_packed(__nv_bfloat16 *p, uint4 v) { __stcs(reinterpret_cast<uint4 *>(p), v); }
     __device__ static float ld1(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
     __device__ static float get(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ static __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
