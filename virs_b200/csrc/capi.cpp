@@ -123,7 +123,7 @@ struct virs_sim {
 
     // boundary
     uint64_t nb = 0;
-    DevBuf bidx, bpos, bcode, bnrm, bmat, bw, brec, state;
+    DevBuf bidx, bpos, bcode, bnrm, bmat, bw, state;
     DevBuf hpos;                   // hard-source voxel positions
     uint32_t nhpos = 0;
 
@@ -371,7 +371,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     compute_constants(s);
     // release the old grid first so that peak memory stays at one grid
     for (DevBuf *b : {&s->flags_raw, &s->wall_mat, &s->flags, &s->code, &s->normals, &s->bseg, &s->segnz, &s->field[0],
-                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->brec, &s->state, &s->side, &s->hpos,
+                      &s->field[1], &s->bidx, &s->bpos, &s->bcode, &s->bnrm, &s->bmat, &s->bw, &s->state, &s->side, &s->hpos,
                       &s->spare[0], &s->spare[1], &s->plist, &s->pzmask})
         b->release();
     const size_t ext = (size_t)s->px * ny * s->ext_nz;
@@ -629,7 +629,6 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.code = s->code.as<uint8_t>();
     a.normals = s->normals.as<uint8_t>();
     a.bpos = s->bpos.as<uint32_t>();
-    a.brec = s->brec.as<uint4>();
     a.l2 = s->l2;
     a.rigid = s->prm.rigid_walls ? 1 : 0;
     if (s->stop_rule) a.stop = s->stopbuf.as<uint32_t>();
@@ -644,7 +643,6 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.nb = s->nb;
     a.nhard = s->nhard;
     a.nsec = s->nsec;
-    a.ncoef = (uint32_t)(s->nmat * s->nsec * 5);
     a.nx = s->nx;
     a.ny = s->ny;
     a.nz = s->nz;
@@ -1334,7 +1332,6 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         VIRS_TRY(s->bcode.alloc(std::max<uint64_t>(nb, 1), "boundary codes"));
         VIRS_TRY(s->bnrm.alloc(std::max<uint64_t>(nb, 1), "boundary normals"));
         VIRS_TRY(s->bw.alloc(std::max<uint64_t>(nb, 1) * 4, "boundary weights"));
-        VIRS_TRY(s->brec.alloc(std::max<uint64_t>(nb, 1) * 16, "boundary slot records"));
         VIRS_TRY(s->side.alloc(std::max<uint64_t>(nb, 1) * sizeof(float4), "boundary records"));
         CompactArgs cp{};
         cp.flags = s->flags.as<uint8_t>();
@@ -1350,7 +1347,6 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
         cp.bcode = s->bcode.as<uint8_t>();
         cp.bnrm = s->bnrm.as<uint8_t>();
         cp.bw = s->bw.as<float>();
-        cp.brec = s->brec.as<uint4>();
         cp.nx = s->nx;
         cp.ny = s->ny;
         cp.nz = s->nz;

@@ -76,7 +76,6 @@ struct StepArgs {
     const uint8_t *code;
     const uint8_t *normals; // air-neighbour mask (rigid-wall update)
     const uint32_t *bpos;   // [nb] padded device index of each boundary slot
-    const uint4 *brec;      // [nb] per slot {bpos, bcode | bnrm << 8 | bmat << 16, bw bits, 0}: one 16-byte load
     const uint8_t *bcode;   // [nb] cell code of each slot's voxel (read in slot order, not gathered)
     const uint8_t *bnrm;    // [nb] air-neighbour mask of each slot's voxel (rigid-wall update)
     const uint8_t *bmat;
@@ -88,7 +87,6 @@ struct StepArgs {
     uint64_t nb;
     uint32_t nhard;
     uint32_t nsec;
-    uint32_t ncoef;         // values in coef: materials x sections x 5
     uint32_t nx, ny, nz, px;
     int zc;                 // planes per block
     int form;               // VIRS_BOUNDARY_*
@@ -222,7 +220,6 @@ struct CompactArgs {
     uint8_t *bcode, *bnrm;     // ... copied per slot
     uint8_t *bmat;
     float *bw;
-    uint4 *brec;               // the per-slot record the boundary pass reads
     uint32_t nx, ny, nz, px, spr;
 };
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);

@@ -180,10 +180,7 @@ __global__ void k_compact(const CompactArgs a)
     a.bcode[slot] = a.code[i];
     a.bnrm[slot] = a.normals[i];
     a.bmat[slot] = a.bmat_full[i];
-    const float w = a.wtab[a.bd2_full[i]];
-    a.bw[slot] = w;
-    a.brec[slot] = make_uint4((uint32_t)i, (uint32_t)a.code[i] | ((uint32_t)a.normals[i] << 8) |
-                                               ((uint32_t)a.bmat_full[i] << 16), __float_as_uint(w), 0u);
+    a.bw[slot] = a.wtab[a.bd2_full[i]];
 }
 
 // ---- exclusive scan (three phases) -------------------------------------------

@@ -183,16 +183,13 @@ template <typename T, int MODE, int MAXS>
 __device__ __forceinline__ void bvox_load(const StepArgs &a, uint64_t slot, BVox<T, MAXS> &v)
 {
     using IO = Io<T>;
-    // the slot's record: position, code, air-neighbour mask, material and
-    // sponge weight in one 16-byte load
-    const uint4 rec = __ldg(a.brec + slot);
-    const size_t i = rec.x;
+    const size_t i = __ldg(a.bpos + slot);
     const size_t sy = a.px, sz = (size_t)a.px * a.ny;
     const T *P = static_cast<const T *>(a.p);
     const T *Q = static_cast<const T *>(a.q);
     v.i = i;
-    v.c = (uint8_t)(rec.y & 0xffu);
-    v.nm = a.rigid ? (uint8_t)((rec.y >> 8) & 0xffu) : 0;
+    v.c = __ldg(a.bcode + slot);
+    v.nm = a.rigid ? __ldg(a.bnrm + slot) : 0;
     v.ce = IO::get(P[i]);
     v.qv = IO::get(Q[i]);
     v.nb[0] = IO::get(P[i + 1]);
@@ -201,15 +198,11 @@ __device__ __forceinline__ void bvox_load(const StepArgs &a, uint64_t slot, BVox
     v.nb[3] = IO::get(P[i - sy]);
     v.nb[4] = IO::get(P[i + sz]);
     v.nb[5] = IO::get(P[i - sz]);
-    if (MODE != BND_RECORD && MAXS > 0) {
-        v.st.m = rec.y >> 16;
-        v.st.wf = __uint_as_float(rec.z);
-        bload_states<MAXS>(a, slot, v.st);
-    }
+    if (MODE != BND_RECORD && MAXS > 0) bload<MAXS>(a, slot, v.st);
 }
 
 template <typename T, int MODE, int MAXS>
-__device__ __forceinline__ void bvox_update(const StepArgs &a, const float *coef, uint64_t slot, const BVox<T, MAXS> &v)
+__device__ __forceinline__ void bvox_update(const StepArgs &a, uint64_t slot, const BVox<T, MAXS> &v)
 {
     float r;
     if (a.rigid) {
@@ -226,7 +219,7 @@ __device__ __forceinline__ void bvox_update(const StepArgs &a, const float *coef
     }
     if (MODE != BND_UPDATE) a.side[slot] = make_float4(r, v.ce, v.qv, 0.f);
     if (MODE == BND_RECORD) return;
-    r = MAXS > 0 ? bcompute<MAXS>(a, coef, r, v.ce, v.qv, slot, v.st) : boundary_loop(a, r, v.ce, v.qv, slot);
+    r = MAXS > 0 ? bcompute<MAXS>(a, r, v.ce, v.qv, slot, v.st) : boundary_loop(a, r, v.ce, v.qv, slot);
     static_cast<T *>(a.q)[v.i] =
         put_rounded<T>(r, a.sr, v.i, a.sr_base, a.sr ? sr_step_key(*a.ctr, 0u) : 0u);
 }
@@ -247,32 +240,18 @@ __device__ __forceinline__ void bvox_update(const StepArgs &a, const float *coef
 //   BND_RECORD  the record only: no filters, nothing written to the fields
 //               (the adjoint step, on adjoint fields)
 constexpr int BT = 256;
-// The coefficient table ([materials][sections][5]) is copied to shared
-// memory when it holds at most MAXC values, so the cascade's coefficient
-// loads stay off the global load path that the gathers use.
-constexpr uint32_t MAXC = 1280;
-
-__device__ __forceinline__ const float *stage_coefs(const StepArgs &a, float *sh, uint32_t ncoef)
-{
-    if (ncoef > MAXC) return a.coef;
-    for (uint32_t k = threadIdx.x; k < ncoef; k += blockDim.x) sh[k] = __ldg(a.coef + k);
-    __syncthreads();
-    return sh;
-}
 
 template <typename T, int MODE, int MAXS>
-__global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArgs a, uint32_t ncoef)
+__global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArgs a)
 {
     if (a.stop && *a.stop) return; // the stop rule fired at an earlier step
-    __shared__ float csh[MAXC];
-    const float *coef = MODE != BND_RECORD && MAXS > 0 ? stage_coefs(a, csh, ncoef) : a.coef;
     const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
     const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
     BVox<T, MAXS> v0, v1;
     if (h0) bvox_load<T, MODE, MAXS>(a, s0, v0);
     if (h1) bvox_load<T, MODE, MAXS>(a, s1, v1);
-    if (h0) bvox_update<T, MODE, MAXS>(a, coef, s0, v0);
-    if (h1) bvox_update<T, MODE, MAXS>(a, coef, s1, v1);
+    if (h0) bvox_update<T, MODE, MAXS>(a, s0, v0);
+    if (h1) bvox_update<T, MODE, MAXS>(a, s1, v1);
 }
 
 // The second step of a two-step pass (kernels_step_tma.cu, k_pair_tma):
@@ -319,20 +298,17 @@ template <typename T> __device__ __forceinline__ void fix_store(const StepArgs &
 
 template <typename T, int MAXS>
 __global__ void __launch_bounds__(BT) k_boundary_fix(const __grid_constant__ StepArgs a, const void *pn,
-                                                     const uint32_t *__restrict list, uint32_t nlist, uint32_t gb,
-                                                     uint32_t ncoef)
+                                                     const uint32_t *__restrict list, uint32_t nlist, uint32_t gb)
 {
     if (a.stop && *a.stop) return;
     if (blockIdx.x < gb) {
-        __shared__ float csh[MAXC];
-        const float *coef = MAXS > 0 ? stage_coefs(a, csh, ncoef) : a.coef;
         const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
         const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
         BVox<T, MAXS> v0, v1;
         if (h0) bvox_load<T, BND_UPDATE, MAXS>(a, s0, v0);
         if (h1) bvox_load<T, BND_UPDATE, MAXS>(a, s1, v1);
-        if (h0) bvox_update<T, BND_UPDATE, MAXS>(a, coef, s0, v0);
-        if (h1) bvox_update<T, BND_UPDATE, MAXS>(a, coef, s1, v1);
+        if (h0) bvox_update<T, BND_UPDATE, MAXS>(a, s0, v0);
+        if (h1) bvox_update<T, BND_UPDATE, MAXS>(a, s1, v1);
         return;
     }
     const uint32_t f0 = (blockIdx.x - gb) * (2 * BT) + threadIdx.x, f1 = f0 + BT;
@@ -369,7 +345,7 @@ __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__res
     const BatchMember &b = mem[lo];
     BVox<T, MAXS> v;
     bvox_load<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
-    bvox_update<T, BND_UPDATE, MAXS>(b.step[parity], b.step[parity].coef, g - b.first_bnd, v);
+    bvox_update<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
 }
 
 // The reference's stop rule (simulator_gpu.cu:303-330) on receiver 0's
@@ -478,21 +454,20 @@ cudaError_t launch_step(int storage, int tile_rows, const StepArgs &a, cudaStrea
 namespace {
 
 template <typename T, int MODE>
-void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, uint32_t nc, cudaStream_t s)
+void boundary_by_sections(uint32_t ns, unsigned g, const StepArgs &a, cudaStream_t s)
 {
-    if (MODE == BND_RECORD || ns <= 1) k_boundary<T, MODE, 1><<<g, BT, 0, s>>>(a, nc);
-    else if (ns == 2) k_boundary<T, MODE, 2><<<g, BT, 0, s>>>(a, nc);
-    else if (ns <= 4) k_boundary<T, MODE, 4><<<g, BT, 0, s>>>(a, nc);
-    else k_boundary<T, MODE, 0><<<g, BT, 0, s>>>(a, nc);
+    if (MODE == BND_RECORD || ns <= 1) k_boundary<T, MODE, 1><<<g, BT, 0, s>>>(a);
+    else if (ns == 2) k_boundary<T, MODE, 2><<<g, BT, 0, s>>>(a);
+    else if (ns <= 4) k_boundary<T, MODE, 4><<<g, BT, 0, s>>>(a);
+    else k_boundary<T, MODE, 0><<<g, BT, 0, s>>>(a);
 }
 
 template <typename T> void boundary_by_mode(int mode, uint32_t ns, unsigned g, const StepArgs &a, cudaStream_t s)
 {
-    const uint32_t nc = a.ncoef;
     switch (mode) {
-    case BND_KEEP: boundary_by_sections<T, BND_KEEP>(ns, g, a, nc, s); break;
-    case BND_RECORD: boundary_by_sections<T, BND_RECORD>(ns, g, a, nc, s); break;
-    default: boundary_by_sections<T, BND_UPDATE>(ns, g, a, nc, s); break;
+    case BND_KEEP: boundary_by_sections<T, BND_KEEP>(ns, g, a, s); break;
+    case BND_RECORD: boundary_by_sections<T, BND_RECORD>(ns, g, a, s); break;
+    default: boundary_by_sections<T, BND_UPDATE>(ns, g, a, s); break;
     }
 }
 
@@ -512,11 +487,11 @@ void boundary_fix_t(const StepArgs &a, const void *pn, const uint32_t *list, uin
 {
     const unsigned gb = (unsigned)((a.nb + 2 * BT - 1) / (2 * BT));
     const unsigned g = gb + (nlist + 2 * BT - 1) / (2 * BT);
-    const uint32_t ns = a.nsec, nc = a.ncoef;
-    if (ns <= 1) k_boundary_fix<T, 1><<<g, BT, 0, s>>>(a, pn, list, nlist, gb, nc);
-    else if (ns == 2) k_boundary_fix<T, 2><<<g, BT, 0, s>>>(a, pn, list, nlist, gb, nc);
-    else if (ns <= 4) k_boundary_fix<T, 4><<<g, BT, 0, s>>>(a, pn, list, nlist, gb, nc);
-    else k_boundary_fix<T, 0><<<g, BT, 0, s>>>(a, pn, list, nlist, gb, nc);
+    const uint32_t ns = a.nsec;
+    if (ns <= 1) k_boundary_fix<T, 1><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else if (ns == 2) k_boundary_fix<T, 2><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else if (ns <= 4) k_boundary_fix<T, 4><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
+    else k_boundary_fix<T, 0><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
 }
 } // namespace
 

@@ -326,21 +326,21 @@ __device__ __forceinline__ float correct(const StepArgs &a, float r, float d, fl
 
 // up to MAXS sections, fully unrolled, in two parts so that a caller can
 // issue the loads of several voxels before any arithmetic: bload reads the
-// material, the weight and every state of a slot (bload_states the states
-// only, for a caller that has the material and weight from the slot's
-// record); bcompute reads the coefficients from `coef` (global memory, or a
-// copy in shared memory), runs the cascade, writes the states and returns
-// the corrected value.
+// material, the weight and every state of a slot; bcompute reads the
+// coefficients (they depend on the material), runs the cascade, writes the
+// states and returns the corrected value.
 template <int MAXS> struct BState {
     uint32_t m;
     float wf;
     float h[MAXS + 1][2];
 };
 
-template <int MAXS> __device__ __forceinline__ void bload_states(const StepArgs &a, uint64_t slot, BState<MAXS> &b)
+template <int MAXS> __device__ __forceinline__ void bload(const StepArgs &a, uint64_t slot, BState<MAXS> &b)
 {
     const uint32_t ns = a.nsec;
     const float *st = a.state + slot;
+    b.m = __ldg(a.bmat + slot);
+    b.wf = __ldg(a.bw + slot);
 #pragma unroll
     for (int q = 0; q <= MAXS; ++q)
         if (q <= (int)ns)
@@ -348,31 +348,24 @@ template <int MAXS> __device__ __forceinline__ void bload_states(const StepArgs 
             for (int j = 0; j < 2; ++j) b.h[q][j] = st[(uint64_t)(2 * q + j) * a.nb];
 }
 
-template <int MAXS> __device__ __forceinline__ void bload(const StepArgs &a, uint64_t slot, BState<MAXS> &b)
-{
-    b.m = __ldg(a.bmat + slot);
-    b.wf = __ldg(a.bw + slot);
-    bload_states<MAXS>(a, slot, b);
-}
-
 template <int MAXS>
-__device__ __forceinline__ float bcompute(const StepArgs &a, const float *coef, float r, float ce, float qv,
-                                          uint64_t slot, const BState<MAXS> &b)
+__device__ __forceinline__ float bcompute(const StepArgs &a, float r, float ce, float qv, uint64_t slot,
+                                          const BState<MAXS> &b)
 {
     const uint32_t ns = a.nsec;
     const uint64_t nb = a.nb;
     float *st = a.state + slot;
-    const float *kc = coef + (uint64_t)b.m * ns * 5;
+    const float *kc = a.coef + (uint64_t)b.m * ns * 5;
     const float d = __fsub_rn(ce, qv);
     float in = d, last = b.h[0][0];
 #pragma unroll
     for (int q = 0; q < MAXS; ++q) {
         if (q < (int)ns) {
             const float *kq = kc + 5 * q;
-            float y = __fmaf_rn(kq[0], in, __fmul_rn(kq[1], b.h[q][0]));
-            y = __fmaf_rn(kq[2], b.h[q][1], y);
-            y = __fmaf_rn(-kq[3], b.h[q + 1][0], y);
-            y = __fmaf_rn(-kq[4], b.h[q + 1][1], y);
+            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), b.h[q][0]));
+            y = __fmaf_rn(__ldg(kq + 2), b.h[q][1], y);
+            y = __fmaf_rn(-__ldg(kq + 3), b.h[q + 1][0], y);
+            y = __fmaf_rn(-__ldg(kq + 4), b.h[q + 1][1], y);
             st[(uint64_t)(2 * q + 0) * nb] = in;
             st[(uint64_t)(2 * q + 1) * nb] = b.h[q][0];
             in = y;
