@@ -489,14 +489,15 @@ def run_virs(args):
     interior = int(np.prod([d - 2 for d in args.size]))
     kernel_ms = r32.get("kernel_ms")
     bpv, steps_per_launch, kernel_name, traffic_file = stencil_roofline(r32, args.storage)
-    # algorithmic bytes per launch: 13 B (7 B in 16-bit storage) per voxel
-    # update times the updates one launch makes (two per voxel with time
-    # blocking, an effective bandwidth that exceeds the DRAM bytes); the
-    # kernel's own bytes per voxel and launch (17 / 9 with time blocking)
-    # and the measured DRAM traffic are reported beside it
+    # achieved: the launch's own algorithmic bytes (13 / 7 B per voxel for a
+    # single step; 17 / 9 B per voxel for a two-step launch, which reads p^n,
+    # p^{n-1} and the code once and writes p^{n+1} and p^{n+2}) over its
+    # CUDA-event duration.  The per-update basis (13 / 7 B per voxel update
+    # times the updates a launch makes) is reported beside it as an
+    # effective bandwidth: with time blocking it exceeds the bytes moved.
     upd = BYTES_F32 if args.storage == "f32" else BYTES_16
-    achieved = nvox * upd * steps_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
-    own = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    effective = nvox * upd * steps_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
+    achieved = nvox * bpv / (kernel_ms * 1e-3) / 1e9 if kernel_ms else None
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -545,10 +546,13 @@ def run_virs(args):
             "kernel": kernel_name,
             "kernel_ms": kernel_ms,
             "steps_per_launch": steps_per_launch,
-            "basis": "%g B per voxel update x %d update(s) per voxel per launch" % (upd, steps_per_launch),
-            "bytes_per_voxel": upd,
-            "launch_bytes_per_voxel": bpv,
-            "launch_frac": round(own / peak, 4) if own else None,
+            "basis": "%g B per voxel per launch (the launch's own algorithmic bytes)" % bpv,
+            "bytes_per_voxel": bpv,
+            "updates_per_launch": steps_per_launch,
+            "effective_achieved": round(effective, 1) if effective else None,
+            "effective_frac": round(effective / peak, 4) if effective else None,
+            "effective_basis": "%g B per voxel update x %d update(s) per voxel per launch: with time blocking an "
+                               "effective bandwidth above the bytes moved" % (upd, steps_per_launch),
             "boundary_pass_ms": r32.get("boundary_ms"),
             "boundary_pass_note": ("per step: a two-step pass's two boundary launches (the second also recomputes "
                                    "the voxels next to boundary voxels and sources), halved" if steps_per_launch == 2
