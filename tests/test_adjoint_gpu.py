@@ -74,6 +74,6 @@ def test_torch_autograd_descends():
         loss.backward()
         assert coef.grad is not None and torch.isfinite(coef.grad).all()
         opt.step()
-        losses.append(float(loss))
+        losses.append(float(loss.detach()))
     assert losses[-1] < losses[0]
     sim.close()
