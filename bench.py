@@ -337,8 +337,10 @@ def bench_adjoint(args, stream, dev):
     every = 64
     sim, _ = scenes.build_simulation(sc)
     nvox = int(np.prod(sim.shape))
-    sim.forward_checkpointed(256, every)             # warm-up: both passes once on a short run
-    sim.adjoint(np.zeros((len(sc.rcv_pos), 256), np.float32), sc.n_materials, sc.n_sections)
+    # warm-up: both passes once at the full length, so that the checkpoint
+    # and segment buffers exist before the timed passes
+    sim.forward_checkpointed(sc.steps, every)
+    sim.adjoint(np.zeros((len(sc.rcv_pos), sc.steps), np.float32), sc.n_materials, sc.n_sections)
     sim.start(sc.steps)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
