@@ -583,7 +583,11 @@ def run_virs(args):
                     "(sw_power_cap) engages within about a second",
         }
     if "batched_bf16" in variants:
+        # against the headline FP32 hall, and against FP32 storage on the same
+        # batched workload
         variants["bf16_batched_vs_f32_plain"] = round(variants["batched_bf16"]["value"] / value, 3)
+        variants["bf16_batched_vs_f32_batched"] = round(variants["batched_bf16"]["value"] /
+                                                        variants["batched_f32"]["value"], 3)
     tr = measured_traffic(Path(args.traffic) if args.traffic else traffic_file, args.storage, nvox)
     if tr:
         line["roofline"]["traffic"] = tr["bytes"]
