@@ -191,11 +191,14 @@ virs_status virs_slab_planes(const virs_sim *sim, void **first, void **last, voi
 virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi);
 
 /* `steps` steps of a grid split into the n slabs slabs[0..n-1] (in order,
- * covering planes 1..nz-2): per step every adjacent pair exchanges
- * (virs_slab_exchange), then every slab takes one step on its own stream.
- * Slabs on different GPUs of this process run concurrently.  Returns when
- * the work is queued (virs_synchronize each handle to wait).  Single steps,
- * no CUDA graph; the device stop rule is refused. */
+ * covering planes 1..nz-2).  Per step and slab: the stencil over the slab's
+ * interior planes (which read no ghost plane) on its own stream, while a
+ * second stream of the handle pulls its two ghost planes from the
+ * neighbours (after their previous step); then the two edge planes, the
+ * boundary pass and the sources and receivers.  The copies overlap the
+ * interior work; slabs on different GPUs of this process run concurrently.
+ * Returns when the work is queued (virs_synchronize each handle to wait).
+ * Single steps, no CUDA graph; the device stop rule is refused. */
 virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps);
 
 virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);

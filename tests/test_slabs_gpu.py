@@ -199,3 +199,35 @@ def test_slab_exchange_arguments_checked():
     assert e.value.status == capi.E_STATE
     for s in (a, b, c):
         s.close()
+
+
+@pytest.mark.parametrize("parts", [3, 7])
+def test_slab_run_thin_slabs_match_whole_grid(parts):
+    """virs_slab_run on slabs that own one to three planes: the interior
+    launch (planes 2 .. nz-3) is empty or a single plane, and the edge planes
+    are one plane or two.  A 64x48x9 hall: 7 interior planes."""
+    sc = scenes.large_hall(steps=80, size=(64, 48, 9))
+    whole, meta = scenes.build_simulation(sc)
+    whole.run(sc.steps)
+    want_ir = whole.ir()
+    want_p, want_pp = whole.pressure(prev=True)
+    nx, ny, _ = meta["shape"]
+    plane = nx * ny
+    parts_, _ = scenes.build_slabs(sc, parts)
+    sims = [p[0] for p in parts_]
+    capi.slab_run(sims, 50)
+    capi.slab_run(sims, 30)
+    ir = np.zeros_like(want_ir)
+    for s, z_lo, z_hi, own_r in parts_:
+        s.synchronize()
+        if own_r.any():
+            ir[own_r] = s.ir()
+        p, pp = s.pressure(prev=True)
+        gown = slice(z_lo * plane, z_hi * plane)
+        assert np.array_equal(p[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_p[gown].view(np.uint32))
+        assert np.array_equal(pp[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_pp[gown].view(np.uint32))
+    assert np.abs(want_ir).max() > 0
+    assert np.array_equal(ir.view(np.uint32), want_ir.view(np.uint32))
+    for s in sims:
+        s.close()
+    whole.close()

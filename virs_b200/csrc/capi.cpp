@@ -117,6 +117,8 @@ struct virs_sim {
     // the owned planes and a ghost plane each side) starts slab_drop planes
     // into them.  For a whole grid ext_nz == nz and slab_drop == 0.
     bool slab = false;
+    cudaStream_t xstream = nullptr;    // virs_slab_run: the ghost-plane pulls, beside the interior stencil
+    cudaEvent_t xdone = nullptr;       // ... and their completion
     int rounding = VIRS_ROUND_NEAREST; // of the 16-bit stores (virs_set_rounding)
     uint32_t ext_nz = 0, slab_drop = 0;
     uint64_t slab_lo = 0, slab_hi = 0, global_nz = 0; // owned global planes and the global grid's planes
@@ -220,6 +222,8 @@ struct virs_sim {
     {
         drop_graphs();
         if (done) cudaEventDestroy(done);
+        if (xdone) cudaEventDestroy(xdone);
+        if (xstream) cudaStreamDestroy(xstream);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -648,6 +652,8 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.nz = s->nz;
     a.px = s->px;
     a.zc = s->zc;
+    a.zb = 1;
+    a.ze = (int)s->nz - 1;
     a.c2dt2 = s->c2dt2;
     a.inv_h2 = s->inv_h2;
     a.K = (double)s->K;
@@ -688,6 +694,19 @@ cudaError_t launch_stencil(const virs_sim *s, int parity, cudaStream_t st)
     if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, step_args(s, parity), st);
     const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
     return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, step_args(s, parity), m, s->err.as<int>(), st);
+}
+
+// the stencil over planes [zb, ze) only (the all-zero code masks belong to
+// the whole-step tiling and are not used)
+cudaError_t launch_stencil_range(const virs_sim *s, int parity, cudaStream_t st, int zb, int ze)
+{
+    StepArgs a = step_args(s, parity);
+    a.zb = zb;
+    a.ze = ze;
+    a.tzmask = nullptr;
+    if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, a, st);
+    const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
+    return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
 }
 
 cudaError_t enqueue_step(const virs_sim *s, int parity, cudaStream_t st)
@@ -1724,20 +1743,65 @@ VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64
     if (n == 1) {
         const virs_sim *s = slabs[0];
         if (!s->slab || !started(s)) return fail(VIRS_E_STATE, "virs_slab_run: a started slab handle is needed");
+        if (!s->fields_valid) return fail(VIRS_E_STATE, "virs_slab_run: the fields were consumed by virs_adjoint");
     }
     for (uint32_t k = 0; k + 1 < n; ++k) VIRS_TRY(check_slab_pair(slabs[k], slabs[k + 1]));
     if (slabs[0]->slab_lo != 1 || slabs[n - 1]->slab_hi != slabs[0]->global_nz - 1)
         return fail(VIRS_E_ARG, "virs_slab_run: the slabs must cover the grid's interior planes, in order");
     if (slabs[0]->steps_done + steps >= (1ull << 32)) return fail(VIRS_E_ARG, "step counter would pass 2^32");
+    for (uint32_t k = 0; k < n; ++k) {
+        virs_sim *s = slabs[k];
+        VIRS_TRY(use_device(s));
+        if (s->stop_rule && s->stopped) return fail(VIRS_E_STATE, "virs_slab_run: the stop rule fired");
+        VIRS_TRY(ready_to_run(s));
+        VIRS_TRY(ensure_ir(s, s->steps_done + steps));
+        if (!s->xstream) VIRS_CUDA(cudaStreamCreateWithFlags(&s->xstream, cudaStreamNonBlocking));
+        if (!s->xdone) VIRS_CUDA(cudaEventCreateWithFlags(&s->xdone, cudaEventDisableTiming));
+    }
+    // Per step and slab: the interior planes 2 .. nz-3 (they read no ghost
+    // plane) on the slab's stream; meanwhile, on its exchange stream, the
+    // pulls of its two ghost planes, after its own and its neighbours'
+    // previous steps; then, after the pulls, the edge planes 1 and nz-2, the
+    // boundary pass and the post kernel.  The pulls write the ghost planes of
+    // p^n, which this step's kernels do not write, and a slab overwrites the
+    // planes its neighbours pulled from only two steps later, after waiting
+    // for their previous step, which waited for those pulls.
+    const size_t pb = (size_t)slabs[0]->px * slabs[0]->ny * slabs[0]->storage_bytes();
     for (uint64_t i = 0; i < steps; ++i) {
-        // every exchange before any step: a slab's step writes the buffer
-        // its neighbours pulled from one step later, and each pull follows
-        // the neighbour's previous step
-        for (uint32_t k = 0; k + 1 < n; ++k) VIRS_TRY(slab_exchange(slabs[k], slabs[k + 1]));
         for (uint32_t k = 0; k < n; ++k) {
             virs_sim *s = slabs[k];
             VIRS_TRY(use_device(s));
-            VIRS_TRY(run_steps(s, 1, s->stream));
+            const int nz = (int)s->nz;
+            if (nz - 2 > 2) VIRS_CUDA(launch_stencil_range(s, s->cur, s->stream, 2, nz - 2));
+        }
+        for (uint32_t k = 0; k < n; ++k) {
+            virs_sim *s = slabs[k];
+            VIRS_TRY(use_device(s));
+            VIRS_CUDA(cudaStreamWaitEvent(s->xstream, s->done, 0));
+            if (k > 0) {
+                VIRS_CUDA(cudaStreamWaitEvent(s->xstream, slabs[k - 1]->done, 0));
+                VIRS_CUDA(cudaMemcpyAsync(slab_plane(s, 0), slab_plane(slabs[k - 1], slabs[k - 1]->nz - 2), pb,
+                                          cudaMemcpyDefault, s->xstream));
+            }
+            if (k + 1 < n) {
+                VIRS_CUDA(cudaStreamWaitEvent(s->xstream, slabs[k + 1]->done, 0));
+                VIRS_CUDA(cudaMemcpyAsync(slab_plane(s, s->nz - 1), slab_plane(slabs[k + 1], 1), pb, cudaMemcpyDefault,
+                                          s->xstream));
+            }
+            VIRS_CUDA(cudaEventRecord(s->xdone, s->xstream));
+        }
+        for (uint32_t k = 0; k < n; ++k) {
+            virs_sim *s = slabs[k];
+            VIRS_TRY(use_device(s));
+            const int nz = (int)s->nz, par = s->cur;
+            VIRS_CUDA(cudaStreamWaitEvent(s->stream, s->xdone, 0));
+            VIRS_CUDA(launch_stencil_range(s, par, s->stream, 1, 2));
+            if (nz - 2 > 1) VIRS_CUDA(launch_stencil_range(s, par, s->stream, nz - 2, nz - 1));
+            VIRS_CUDA(launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, s->stream));
+            VIRS_CUDA(launch_post(s->prm.storage, post_args(s, par), s->stream));
+            s->cur ^= 1;
+            s->steps_done += 1;
+            VIRS_CUDA(cudaEventRecord(s->done, s->stream));
         }
     }
     return VIRS_OK;

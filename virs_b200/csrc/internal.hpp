@@ -89,6 +89,7 @@ struct StepArgs {
     uint32_t nsec;
     uint32_t nx, ny, nz, px;
     int zc;                 // planes per block
+    int zb, ze;             // the stencil updates planes [zb, ze): 1 and nz - 1 for a whole step
     int form;               // VIRS_BOUNDARY_*
     float c2dt2, inv_h2;
     float l2;               // (c dt / h)^2 of the rigid-wall update

@@ -48,8 +48,8 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY)) k_step(const __grid
     const int y0 = blockIdx.y * TY;
     const int y = y0 + ty;
     if (a.stop && *a.stop) return; // the stop rule fired at an earlier step
-    const int z0 = 1 + blockIdx.z * a.zc;
-    const int z1 = min(z0 + a.zc, (int)a.nz - 1);
+    const int z0 = a.zb + blockIdx.z * a.zc;
+    const int z1 = min(z0 + a.zc, a.ze);
     if (z0 >= z1) return; // uniform over the block
 
     const int px = (int)a.px, ny = (int)a.ny;
@@ -425,7 +425,8 @@ cudaError_t launch_step_t(int tile_rows, const StepArgs &a, cudaStream_t s)
     StepArgs b = a;
     b.zc = zc;
     const unsigned gx = (a.px + TX - 1) / TX;
-    const unsigned gz = (a.nz - 2 + zc - 1) / zc;
+    if (a.ze <= a.zb) return cudaSuccess;
+    const unsigned gz = (unsigned)((a.ze - a.zb + zc - 1) / zc);
     switch (tile_rows) {
     case 4: k_step<T, 4><<<dim3(gx, (a.ny + 3) / 4, gz), dim3(32, 4), 0, s>>>(b); break;
     case 16: k_step<T, 16><<<dim3(gx, (a.ny + 15) / 16, gz), dim3(32, 16), 0, s>>>(b); break;

@@ -326,8 +326,8 @@ __device__ __forceinline__ bool step_tile(const StepArgs &a, const CUtensorMap *
     t.sl = lane % LPR;                         // lane within the row
     t.x0 = bx * TX;
     t.y0 = by * TY;
-    t.z0 = 1 + bz * a.zc;
-    const int z1 = min(t.z0 + a.zc, (int)a.nz - 1);
+    t.z0 = a.zb + bz * a.zc;
+    const int z1 = min(t.z0 + a.zc, a.ze);
     if (t.z0 >= z1) return true;
     t.nst = z1 - t.z0 + 2; // stages: planes z0-1 .. z1
     const int x = t.x0 + t.sl * V, y = t.y0 + t.row;
@@ -444,8 +444,9 @@ cudaError_t launch3(const StepArgs &a, const TmaMaps &m, int *err, cudaStream_t 
     constexpr size_t sm = smem_bytes<T, TY, L>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
+    if (a.ze <= a.zb) return cudaSuccess;
     const unsigned gx = (a.px + TX - 1) / TX;
-    const unsigned gz = (a.nz - 2 + a.zc - 1) / a.zc;
+    const unsigned gz = (unsigned)((a.ze - a.zb + a.zc - 1) / a.zc);
     kern<<<dim3(gx, (a.ny + TY - 1) / TY, gz), dim3(32, block_threads<T, TY>() / 32), sm, s>>>(a, *m.p, *m.q, *m.c,
                                                                                              err);
     return cudaGetLastError();
