@@ -167,6 +167,9 @@ struct virs_sim {
     // built for zm_rows x zm_zc tiles (0 = none)
     DevBuf zmask;
     int zm_rows = 0, zm_zc = 0;
+    // the same for the slab-interior launch of virs_slab_run (planes 2 .. nz-3)
+    DevBuf zmask_in;
+    int zmi_rows = 0, zmi_zc = 0;
     DevBuf err;                    // device error flag of bounded waits
 
     // two steps per pass (virs_set_time_blocking).  spare[k] is the partner
@@ -391,6 +394,7 @@ virs_status install_grid(virs_sim *s, uint64_t nx, uint64_t ny, uint64_t nz, flo
     s->steps_done = 0;
     s->maps_rows = 0;
     s->zm_rows = s->zm_zc = 0;
+    s->zmi_rows = s->zmi_zc = 0;
     s->pm_rows = 0;
     s->pl_ok = false;
     s->pair_nomem = false;
@@ -574,14 +578,19 @@ int eff_planes(const virs_sim *s) { return s->zc > 0 ? s->zc : default_planes(s-
 
 // per tile of a rows x zc tiling of the TMA stencil, the stages whose codes
 // are all zero (kernels_classify.cu::k_tile_zero_mask)
-virs_status build_zero_masks(const virs_sim *s, int rows, int zc, DevBuf &mask)
+// (planes [zb, ze); 0, 0 = the whole step's planes 1 .. nz-2)
+virs_status build_zero_masks(const virs_sim *s, int rows, int zc, DevBuf &mask, uint32_t zb = 0, uint32_t ze = 0)
 {
+    if (zb == 0 && ze == 0) {
+        zb = 1;
+        ze = s->nz - 1;
+    }
     const uint32_t gx = (s->px + (uint32_t)tma_tile_x() - 1) / (uint32_t)tma_tile_x();
     const uint32_t gy = (s->ny + (uint32_t)rows - 1) / (uint32_t)rows;
-    const uint32_t gz = (s->nz - 2 + (uint32_t)zc - 1) / (uint32_t)zc;
-    VIRS_TRY(mask.alloc((size_t)gx * gy * gz * 8, "zero-code masks"));
+    const uint32_t gz = (ze - zb + (uint32_t)zc - 1) / (uint32_t)zc;
+    VIRS_TRY(mask.alloc(std::max<size_t>((size_t)gx * gy * gz, 1) * 8, "zero-code masks"));
     VIRS_CUDA(launch_tile_zero_masks(s->segnz.as<uint8_t>(), s->ny, s->nz, s->spr, (uint32_t)rows, (uint32_t)zc, gx,
-                                     gy, gz, mask.as<uint64_t>(), s->stream));
+                                     gy, gz, zb, ze, mask.as<uint64_t>(), s->stream));
     VIRS_CUDA(cudaStreamSynchronize(s->stream));
     return VIRS_OK;
 }
@@ -703,7 +712,9 @@ cudaError_t launch_stencil_range(const virs_sim *s, int parity, cudaStream_t st,
     StepArgs a = step_args(s, parity);
     a.zb = zb;
     a.ze = ze;
-    a.tzmask = nullptr;
+    const bool inner = zb == 2 && ze == (int)s->nz - 2 && s->depth > 0 && s->zmi_rows == s->tile_rows &&
+                       s->zmi_zc == eff_planes(s);
+    a.tzmask = inner ? s->zmask_in.as<uint64_t>() : nullptr;
     if (s->depth == 0) return launch_step(s->prm.storage, s->tile_rows, a, st);
     const TmaMaps m{&s->tmP[parity], &s->tmQ[parity ^ 1], &s->tmC};
     return launch_step_tma(s->prm.storage, s->tile_rows, s->depth, a, m, s->err.as<int>(), st);
@@ -1378,6 +1389,7 @@ VIRS_EXPORT virs_status virs_classify(virs_sim *s)
     if (s->filters_set) VIRS_TRY(alloc_states(s));
     s->maps_rows = 0;
     s->zm_rows = s->zm_zc = 0;
+    s->zmi_rows = s->zmi_zc = 0;
     s->pm_rows = 0;
     s->pzm_zc = -1;
     s->pl_ok = false;
@@ -1755,6 +1767,13 @@ VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64
         if (s->stop_rule && s->stopped) return fail(VIRS_E_STATE, "virs_slab_run: the stop rule fired");
         VIRS_TRY(ready_to_run(s));
         VIRS_TRY(ensure_ir(s, s->steps_done + steps));
+        if (s->depth > 0 && zero_masks_useful(s) && s->nz > 5 &&
+            (s->zmi_rows != s->tile_rows || s->zmi_zc != eff_planes(s))) {
+            s->zmi_rows = s->zmi_zc = 0;
+            VIRS_TRY(build_zero_masks(s, s->tile_rows, eff_planes(s), s->zmask_in, 2, s->nz - 2));
+            s->zmi_rows = s->tile_rows;
+            s->zmi_zc = eff_planes(s);
+        }
         if (!s->xstream) VIRS_CUDA(cudaStreamCreateWithFlags(&s->xstream, cudaStreamNonBlocking));
         if (!s->xdone) VIRS_CUDA(cudaEventCreateWithFlags(&s->xdone, cudaEventDisableTiming));
     }

@@ -226,8 +226,10 @@ struct CompactArgs {
 cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s);
 // per tile of a rows x zc tiling of the TMA stencil: bit j set when the codes
 // of the plane in stage j are all zero (kernels_classify.cu)
+// (planes [zb, ze) in chunks of zc: 1 and nz - 1 for a whole step)
 cudaError_t launch_tile_zero_masks(const uint8_t *segnz, uint32_t ny, uint32_t nz, uint32_t spr, uint32_t rows,
-                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint64_t *mask, cudaStream_t s);
+                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint32_t zb, uint32_t ze,
+                                   uint64_t *mask, cudaStream_t s);
 cudaError_t launch_hard_list(const uint8_t *code, uint64_t n, uint32_t *count, uint32_t *out, uint32_t cap,
                              cudaStream_t s);
 

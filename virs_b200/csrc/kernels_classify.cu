@@ -331,12 +331,13 @@ cudaError_t launch_compact(const CompactArgs &a, cudaStream_t s)
 namespace {
 __global__ void __launch_bounds__(64) k_tile_zero_mask(const uint8_t *__restrict segnz, uint32_t ny, uint32_t nz,
                                                        uint32_t spr, uint32_t rows, uint32_t zc, uint32_t gx,
-                                                       uint32_t gy, uint64_t *__restrict mask)
+                                                       uint32_t gy, uint32_t zb, uint32_t ze,
+                                                       uint64_t *__restrict mask)
 {
     __shared__ unsigned w[2];
     const uint32_t t = blockIdx.x, j = threadIdx.x;
     const uint32_t bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
-    const uint32_t z0 = 1 + bz * zc, z1 = min(z0 + zc, nz - 1);
+    const uint32_t z0 = zb + bz * zc, z1 = min(z0 + zc, ze);
     const uint32_t k = z0 - 1 + j;
     bool zero = false;
     if (k >= z0 && k < z1) {
@@ -352,11 +353,12 @@ __global__ void __launch_bounds__(64) k_tile_zero_mask(const uint8_t *__restrict
 } // namespace
 
 cudaError_t launch_tile_zero_masks(const uint8_t *segnz, uint32_t ny, uint32_t nz, uint32_t spr, uint32_t rows,
-                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint64_t *mask, cudaStream_t s)
+                                   uint32_t zc, uint32_t gx, uint32_t gy, uint32_t gz, uint32_t zb, uint32_t ze,
+                                   uint64_t *mask, cudaStream_t s)
 {
     const uint64_t ntiles = (uint64_t)gx * gy * gz;
     if (ntiles == 0) return cudaSuccess;
-    k_tile_zero_mask<<<(unsigned)ntiles, 64, 0, s>>>(segnz, ny, nz, spr, rows, zc, gx, gy, mask);
+    k_tile_zero_mask<<<(unsigned)ntiles, 64, 0, s>>>(segnz, ny, nz, spr, rows, zc, gx, gy, zb, ze, mask);
     return cudaGetLastError();
 }
 
