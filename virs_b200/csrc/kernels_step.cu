@@ -230,10 +230,10 @@ __device__ __forceinline__ void bvox_update(const StepArgs &a, uint64_t slot, co
 // the step) and p^{n-1}, reads the voxel's code from the per-slot copy made
 // at classification (in slot order: no 32-byte sector fetched for one
 // byte), computes the leapfrog update with the wall mirror (or the
-// rigid-wall update), then the filter correction, and writes p^{n+1}.  A
-// thread takes two slots, BT apart, and
-// issues all loads of both before any arithmetic: the pass is bound by the
-// latency of its gathers, and two independent voxels in flight hide it.
+// rigid-wall update), then the filter correction, and writes p^{n+1}.  One
+// slot per thread: on the hall, two, three and four slots per thread (all
+// loads issued before any arithmetic) measured 3, 8 and 16 % slower, and
+// staging the loads of later slots in shared memory slower still.
 //   BND_UPDATE  the step
 //   BND_KEEP    the same, and the record {free value, p, p^{n-1}} of the
 //               slot kept in a.side (the adjoint's recomputation)
@@ -245,13 +245,11 @@ template <typename T, int MODE, int MAXS>
 __global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArgs a)
 {
     if (a.stop && *a.stop) return; // the stop rule fired at an earlier step
-    const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
-    const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
-    BVox<T, MAXS> v0, v1;
-    if (h0) bvox_load<T, MODE, MAXS>(a, s0, v0);
-    if (h1) bvox_load<T, MODE, MAXS>(a, s1, v1);
-    if (h0) bvox_update<T, MODE, MAXS>(a, s0, v0);
-    if (h1) bvox_update<T, MODE, MAXS>(a, s1, v1);
+    const uint64_t s0 = (uint64_t)blockIdx.x * BT + threadIdx.x;
+    if (s0 >= a.nb) return;
+    BVox<T, MAXS> v;
+    bvox_load<T, MODE, MAXS>(a, s0, v);
+    bvox_update<T, MODE, MAXS>(a, s0, v);
 }
 
 // The second step of a two-step pass (kernels_step_tma.cu, k_pair_tma):
@@ -264,8 +262,7 @@ __global__ void __launch_bounds__(BT) k_boundary(const __grid_constant__ StepArg
 // p^n (pn) with leapfrog(code, ...), which is bit-identical to the air
 // update for code 0 and is the mirror update for the others.  Both parts
 // read p^{n+1} and write disjoint voxels of p^{n+2} (a.q): boundary voxels,
-// and air or mirror voxels.  Two entries per thread, loads first, as in the
-// boundary pass.
+// and air or mirror voxels.  One entry per thread, as in the boundary pass.
 template <typename T> struct FixVox {
     size_t i;
     uint8_t c;
@@ -302,23 +299,18 @@ __global__ void __launch_bounds__(BT) k_boundary_fix(const __grid_constant__ Ste
 {
     if (a.stop && *a.stop) return;
     if (blockIdx.x < gb) {
-        const uint64_t s0 = (uint64_t)blockIdx.x * (2 * BT) + threadIdx.x, s1 = s0 + BT;
-        const bool h0 = s0 < a.nb, h1 = s1 < a.nb;
-        BVox<T, MAXS> v0, v1;
-        if (h0) bvox_load<T, BND_UPDATE, MAXS>(a, s0, v0);
-        if (h1) bvox_load<T, BND_UPDATE, MAXS>(a, s1, v1);
-        if (h0) bvox_update<T, BND_UPDATE, MAXS>(a, s0, v0);
-        if (h1) bvox_update<T, BND_UPDATE, MAXS>(a, s1, v1);
+        const uint64_t s0 = (uint64_t)blockIdx.x * BT + threadIdx.x;
+        if (s0 >= a.nb) return;
+        BVox<T, MAXS> v;
+        bvox_load<T, BND_UPDATE, MAXS>(a, s0, v);
+        bvox_update<T, BND_UPDATE, MAXS>(a, s0, v);
         return;
     }
-    const uint32_t f0 = (blockIdx.x - gb) * (2 * BT) + threadIdx.x, f1 = f0 + BT;
-    const bool h0 = f0 < nlist, h1 = f1 < nlist;
-    const T *P0 = static_cast<const T *>(pn);
-    FixVox<T> v0, v1;
-    if (h0) fix_load<T>(a, P0, __ldg(list + f0), v0);
-    if (h1) fix_load<T>(a, P0, __ldg(list + f1), v1);
-    if (h0) fix_store<T>(a, v0);
-    if (h1) fix_store<T>(a, v1);
+    const uint32_t f0 = (blockIdx.x - gb) * BT + threadIdx.x;
+    if (f0 >= nlist) return;
+    FixVox<T> v;
+    fix_load<T>(a, static_cast<const T *>(pn), __ldg(list + f0), v);
+    fix_store<T>(a, v);
 }
 
 // batched: thread g belongs to the last member whose first boundary index
@@ -486,8 +478,8 @@ namespace {
 template <typename T>
 void boundary_fix_t(const StepArgs &a, const void *pn, const uint32_t *list, uint32_t nlist, cudaStream_t s)
 {
-    const unsigned gb = (unsigned)((a.nb + 2 * BT - 1) / (2 * BT));
-    const unsigned g = gb + (nlist + 2 * BT - 1) / (2 * BT);
+    const unsigned gb = (unsigned)((a.nb + BT - 1) / BT);
+    const unsigned g = gb + (nlist + BT - 1) / BT;
     const uint32_t ns = a.nsec;
     if (ns <= 1) k_boundary_fix<T, 1><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
     else if (ns == 2) k_boundary_fix<T, 2><<<g, BT, 0, s>>>(a, pn, list, nlist, gb);
@@ -511,7 +503,7 @@ cudaError_t launch_boundary_fix(int storage, const StepArgs &a, const void *pn, 
 cudaError_t launch_boundary(int storage, const StepArgs &a, int mode, cudaStream_t s)
 {
     if (a.nb == 0) return cudaSuccess;
-    const unsigned g = (unsigned)((a.nb + 2 * BT - 1) / (2 * BT));
+    const unsigned g = (unsigned)((a.nb + BT - 1) / BT);
     switch (storage) {
     case VIRS_STORAGE_F16: boundary_by_mode<__half>(mode, a.nsec, g, a, s); break;
     case VIRS_STORAGE_BF16: boundary_by_mode<__nv_bfloat16>(mode, a.nsec, g, a, s); break;
