@@ -367,15 +367,16 @@ def bench_adjoint(args, stream, dev):
 
 def bench_slabs(sc, args, dev, parts=2, steps=100):
     """The hall split into `parts` z-slabs on this GPU, advanced by
-    virs_slab_run (ghost planes exchanged by device copies before every
-    step, single steps, no graph): the cost of the slab machinery against
-    the whole grid.  Timed by the host clock around the queued run and a
+    virs_slab_run (ghost planes pulled by device copies every step beside
+    the interior stencil, single steps, the 16-step slab graph): the cost of
+    the slab machinery against the whole grid.  The warm-up captures the
+    graph.  Timed by the host clock around the queued run and a
     synchronisation of every slab."""
     from virs_b200 import capi, scenes
     parts_, meta = scenes.build_slabs(sc, parts, device=dev)
     sims = [p[0] for p in parts_]
     nvox = int(np.prod(meta["shape"]))
-    capi.slab_run(sims, 8)                              # warm-up
+    capi.slab_run(sims, 32)                             # warm-up: captures the graph
     for s in sims:
         s.synchronize()
     t0 = time.perf_counter()

@@ -198,7 +198,12 @@ virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi);
  * boundary pass and the sources and receivers.  The copies overlap the
  * interior work; slabs on different GPUs of this process run concurrently.
  * Returns when the work is queued (virs_synchronize each handle to wait).
- * Single steps, no CUDA graph; the device stop rule is refused. */
+ * Single steps (no two-step passes).  When every slab is on one GPU, runs of
+ * 16 steps or more replay a CUDA graph of 16 steps of all slabs (captured
+ * at the first such call and kept by slabs[0] while the same unchanged
+ * slabs run) and take the remaining steps as direct launches; slabs on
+ * several GPUs always take direct launches.  The device stop rule is
+ * refused. */
 virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps);
 
 virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);

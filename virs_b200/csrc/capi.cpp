@@ -8,6 +8,7 @@
 //   -> virs_start_simulation -> virs_run (graph) or virs_step (per step)
 //   -> virs_get_ir -> virs_destroy
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -92,10 +93,37 @@ cudaError_t zero_on(cudaStream_t st, void *p, size_t n)
 
 using namespace virs;
 
+namespace virs {
+namespace {
+// a number no other handle of this process carries
+uint64_t next_handle_id()
+{
+    static std::atomic<uint64_t> n{0};
+    return ++n;
+}
+} // namespace
+} // namespace virs
+
+// the step graph of a virs_slab_run over the same slabs (kept by the first
+// slab): valid while every slab is the same handle, unchanged (gen), and
+// at the buffer parity it was captured for
+struct SlabGraph {
+    std::vector<const virs_sim *> mem;
+    std::vector<uint64_t> id, gen;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    ~SlabGraph()
+    {
+        for (cudaGraphExec_t g : exec)
+            if (g) cudaGraphExecDestroy(g);
+    }
+};
+
 struct virs_sim {
+    const uint64_t id = virs::next_handle_id();
     virs_params prm{};
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    std::unique_ptr<SlabGraph> slab_graph;
 
     // geometry
     bool has_grid = false, classified = false;
@@ -224,6 +252,7 @@ struct virs_sim {
     ~virs_sim()
     {
         drop_graphs();
+        slab_graph.reset();
         if (done) cudaEventDestroy(done);
         if (xdone) cudaEventDestroy(xdone);
         if (xstream) cudaStreamDestroy(xstream);
@@ -1745,6 +1774,169 @@ VIRS_EXPORT virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi)
     return slab_exchange(lo, hi);
 }
 
+namespace {
+
+// steps per graph of a slab run (even: the graph leaves every slab's buffer
+// parity as it found it)
+constexpr int SLAB_GRAPH_STEPS = 16;
+
+// One step of every slab.  Per slab: the interior planes 2 .. nz-3 (they
+// read no ghost plane) on the slab's stream; meanwhile, on its exchange
+// stream, the pulls of its two ghost planes, after its own and its
+// neighbours' previous steps; then, after the pulls, the edge planes 1 and
+// nz-2, the boundary pass and the post kernel.  The pulls write the ghost
+// planes of p^n, which this step's kernels do not write, and a slab
+// overwrites the planes its neighbours pulled from only two steps later,
+// after waiting for their previous step, which waited for those pulls.
+cudaError_t slab_step(virs_sim *const *slabs, uint32_t n, size_t pb)
+{
+    cudaError_t e = cudaSuccess;
+    for (uint32_t k = 0; k < n && e == cudaSuccess; ++k) {
+        virs_sim *s = slabs[k];
+        e = cudaSetDevice(s->prm.device);
+        const int nz = (int)s->nz;
+        if (e == cudaSuccess && nz - 2 > 2) e = launch_stencil_range(s, s->cur, s->stream, 2, nz - 2);
+    }
+    for (uint32_t k = 0; k < n && e == cudaSuccess; ++k) {
+        virs_sim *s = slabs[k];
+        e = cudaSetDevice(s->prm.device);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s->xstream, s->done, 0);
+        if (e == cudaSuccess && k > 0) {
+            e = cudaStreamWaitEvent(s->xstream, slabs[k - 1]->done, 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(slab_plane(s, 0), slab_plane(slabs[k - 1], slabs[k - 1]->nz - 2), pb,
+                                    cudaMemcpyDefault, s->xstream);
+        }
+        if (e == cudaSuccess && k + 1 < n) {
+            e = cudaStreamWaitEvent(s->xstream, slabs[k + 1]->done, 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(slab_plane(s, s->nz - 1), slab_plane(slabs[k + 1], 1), pb, cudaMemcpyDefault,
+                                    s->xstream);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(s->xdone, s->xstream);
+    }
+    for (uint32_t k = 0; k < n && e == cudaSuccess; ++k) {
+        virs_sim *s = slabs[k];
+        e = cudaSetDevice(s->prm.device);
+        const int nz = (int)s->nz, par = s->cur;
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, s->xdone, 0);
+        if (e == cudaSuccess) e = launch_stencil_range(s, par, s->stream, 1, 2);
+        if (e == cudaSuccess && nz - 2 > 1) e = launch_stencil_range(s, par, s->stream, nz - 2, nz - 1);
+        if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, s->stream);
+        if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, par), s->stream);
+        if (e == cudaSuccess) {
+            s->cur ^= 1;
+            s->steps_done += 1;
+            e = cudaEventRecord(s->done, s->stream);
+        }
+    }
+    return e;
+}
+
+// events that live for one call
+struct EventSet {
+    std::vector<cudaEvent_t> ev;
+    ~EventSet()
+    {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    cudaError_t make(cudaEvent_t *out)
+    {
+        const cudaError_t e = cudaEventCreateWithFlags(out, cudaEventDisableTiming);
+        if (e == cudaSuccess) ev.push_back(*out);
+        return e;
+    }
+};
+
+// SLAB_GRAPH_STEPS steps of all slabs (one device) captured in one graph
+// from the first slab's stream: the other streams join the capture through
+// an event recorded on it and leave it through events it waits for; each
+// slab records its completion event inside the capture before any wait on
+// it.  The steps are enqueued as slab_step does; the handles' step state is
+// put back after the capture (the graph's launches advance it), and so are
+// their events.
+virs_status slab_graph(virs_sim *const *slabs, uint32_t n, size_t pb, cudaGraphExec_t *exec)
+{
+    VIRS_TRY(use_device(slabs[0]));
+    cudaStream_t o = slabs[0]->stream;
+    EventSet evs;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join(2 * n, nullptr);
+    VIRS_CUDA(evs.make(&fork));
+    for (auto &j : join) VIRS_CUDA(evs.make(&j));
+    std::vector<int> cur(n);
+    std::vector<uint64_t> done(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        cur[k] = slabs[k]->cur;
+        done[k] = slabs[k]->steps_done;
+    }
+    VIRS_CUDA(cudaStreamBeginCapture(o, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaEventRecord(fork, o);
+    for (uint32_t k = 0; k < n && e == cudaSuccess; ++k) {
+        virs_sim *s = slabs[k];
+        if (k > 0) e = cudaStreamWaitEvent(s->stream, fork, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s->xstream, fork, 0);
+        if (e == cudaSuccess) e = cudaEventRecord(s->done, s->stream);
+    }
+    for (int i = 0; i < SLAB_GRAPH_STEPS && e == cudaSuccess; ++i) e = slab_step(slabs, n, pb);
+    for (uint32_t k = 0; k < n && e == cudaSuccess; ++k) {
+        virs_sim *s = slabs[k];
+        if (k > 0) {
+            e = cudaEventRecord(join[2 * k], s->stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(o, join[2 * k], 0);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(join[2 * k + 1], s->xstream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(o, join[2 * k + 1], 0);
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        slabs[k]->cur = cur[k];
+        slabs[k]->steps_done = done[k];
+    }
+    cudaSetDevice(slabs[0]->prm.device);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(o, &g);
+    if (e == cudaSuccess) e = ee;
+    // the events recorded during the capture stand for graph nodes: record
+    // them again on their streams, whose queued work the capture left as it
+    // was
+    for (uint32_t k = 0; k < n; ++k) {
+        const cudaError_t er = cudaEventRecord(slabs[k]->done, slabs[k]->stream);
+        const cudaError_t ex = cudaEventRecord(slabs[k]->xdone, slabs[k]->xstream);
+        if (e == cudaSuccess) e = er != cudaSuccess ? er : ex;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "slab step graph");
+    }
+    return VIRS_OK;
+}
+
+// `times` launches of the graph on the first slab's stream, after every
+// slab's queued work; every slab's stream then follows the last launch
+virs_status slab_graph_run(virs_sim *const *slabs, uint32_t n, cudaGraphExec_t exec, uint64_t times)
+{
+    VIRS_TRY(use_device(slabs[0]));
+    cudaStream_t o = slabs[0]->stream;
+    EventSet evs;
+    cudaEvent_t after = nullptr;
+    VIRS_CUDA(evs.make(&after));
+    for (uint32_t k = 1; k < n; ++k) VIRS_CUDA(cudaStreamWaitEvent(o, slabs[k]->done, 0));
+    for (uint64_t r = 0; r < times; ++r) VIRS_CUDA(cudaGraphLaunch(exec, o));
+    VIRS_CUDA(cudaEventRecord(after, o));
+    for (uint32_t k = 0; k < n; ++k) {
+        virs_sim *s = slabs[k];
+        if (k > 0) VIRS_CUDA(cudaStreamWaitEvent(s->stream, after, 0));
+        VIRS_CUDA(cudaStreamWaitEvent(s->xstream, after, 0));
+        VIRS_CUDA(cudaEventRecord(s->done, s->stream));
+        s->steps_done += times * SLAB_GRAPH_STEPS;
+    }
+    return VIRS_OK;
+}
+
+} // namespace
+
 VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps)
 {
     if (!slabs || n == 0) return fail(VIRS_E_ARG, "virs_slab_run: no slabs");
@@ -1777,52 +1969,29 @@ VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64
         if (!s->xstream) VIRS_CUDA(cudaStreamCreateWithFlags(&s->xstream, cudaStreamNonBlocking));
         if (!s->xdone) VIRS_CUDA(cudaEventCreateWithFlags(&s->xdone, cudaEventDisableTiming));
     }
-    // Per step and slab: the interior planes 2 .. nz-3 (they read no ghost
-    // plane) on the slab's stream; meanwhile, on its exchange stream, the
-    // pulls of its two ghost planes, after its own and its neighbours'
-    // previous steps; then, after the pulls, the edge planes 1 and nz-2, the
-    // boundary pass and the post kernel.  The pulls write the ghost planes of
-    // p^n, which this step's kernels do not write, and a slab overwrites the
-    // planes its neighbours pulled from only two steps later, after waiting
-    // for their previous step, which waited for those pulls.
     const size_t pb = (size_t)slabs[0]->px * slabs[0]->ny * slabs[0]->storage_bytes();
-    for (uint64_t i = 0; i < steps; ++i) {
-        for (uint32_t k = 0; k < n; ++k) {
-            virs_sim *s = slabs[k];
-            VIRS_TRY(use_device(s));
-            const int nz = (int)s->nz;
-            if (nz - 2 > 2) VIRS_CUDA(launch_stencil_range(s, s->cur, s->stream, 2, nz - 2));
-        }
-        for (uint32_t k = 0; k < n; ++k) {
-            virs_sim *s = slabs[k];
-            VIRS_TRY(use_device(s));
-            VIRS_CUDA(cudaStreamWaitEvent(s->xstream, s->done, 0));
-            if (k > 0) {
-                VIRS_CUDA(cudaStreamWaitEvent(s->xstream, slabs[k - 1]->done, 0));
-                VIRS_CUDA(cudaMemcpyAsync(slab_plane(s, 0), slab_plane(slabs[k - 1], slabs[k - 1]->nz - 2), pb,
-                                          cudaMemcpyDefault, s->xstream));
+    bool one_device = true;
+    for (uint32_t k = 1; k < n; ++k) one_device = one_device && slabs[k]->prm.device == slabs[0]->prm.device;
+    uint64_t i = 0;
+    if (one_device && n > 1 && steps >= SLAB_GRAPH_STEPS) {
+        std::unique_ptr<SlabGraph> &c = slabs[0]->slab_graph;
+        bool same = c && c->mem.size() == n;
+        for (uint32_t k = 0; same && k < n; ++k)
+            same = c->mem[k] == slabs[k] && c->id[k] == slabs[k]->id && c->gen[k] == slabs[k]->gen;
+        if (!same) {
+            c.reset(new SlabGraph);
+            for (uint32_t k = 0; k < n; ++k) {
+                c->mem.push_back(slabs[k]);
+                c->id.push_back(slabs[k]->id);
+                c->gen.push_back(slabs[k]->gen);
             }
-            if (k + 1 < n) {
-                VIRS_CUDA(cudaStreamWaitEvent(s->xstream, slabs[k + 1]->done, 0));
-                VIRS_CUDA(cudaMemcpyAsync(slab_plane(s, s->nz - 1), slab_plane(slabs[k + 1], 1), pb, cudaMemcpyDefault,
-                                          s->xstream));
-            }
-            VIRS_CUDA(cudaEventRecord(s->xdone, s->xstream));
         }
-        for (uint32_t k = 0; k < n; ++k) {
-            virs_sim *s = slabs[k];
-            VIRS_TRY(use_device(s));
-            const int nz = (int)s->nz, par = s->cur;
-            VIRS_CUDA(cudaStreamWaitEvent(s->stream, s->xdone, 0));
-            VIRS_CUDA(launch_stencil_range(s, par, s->stream, 1, 2));
-            if (nz - 2 > 1) VIRS_CUDA(launch_stencil_range(s, par, s->stream, nz - 2, nz - 1));
-            VIRS_CUDA(launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, s->stream));
-            VIRS_CUDA(launch_post(s->prm.storage, post_args(s, par), s->stream));
-            s->cur ^= 1;
-            s->steps_done += 1;
-            VIRS_CUDA(cudaEventRecord(s->done, s->stream));
-        }
+        const int par = slabs[0]->cur;
+        if (!c->exec[par]) VIRS_TRY(slab_graph(slabs, n, pb, &c->exec[par]));
+        VIRS_TRY(slab_graph_run(slabs, n, c->exec[par], steps / SLAB_GRAPH_STEPS));
+        i = steps / SLAB_GRAPH_STEPS * SLAB_GRAPH_STEPS;
     }
+    for (; i < steps; ++i) VIRS_CUDA(slab_step(slabs, n, pb));
     return VIRS_OK;
 }
 
