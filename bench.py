@@ -324,6 +324,39 @@ def bench_batch(storage, args, stream, dev, dist=None):
 CPU_CROP_PLANES = 16   # planes of the hall crop both CPU figures time
 
 
+def bench_ir_postprocess(dev, steps=4000, reps=5):
+    """The end of a simulation on the GPU: the 8 receiver traces of a
+    4000-step run of the 128^3 hall crop resampled to 48 kHz, by the
+    reference's Chebyshev-I cascade plus linear interpolation
+    (virs_postprocess_ir) and by the Kaiser-windowed sinc
+    (virs_postprocess_ir_sinc), each peak-normalised.  Host clock around a
+    whole call (size query, kernels, copy of the result to the host), best
+    of `reps` after one untimed call."""
+    from virs_b200 import capi, scenes
+    sc = scenes.large_hall(steps=steps, size=(128, 128, 128))
+    sim, _ = scenes.build_simulation(sc, device=dev)
+    sim.run(steps)
+    sim.synchronize()
+    dt = float(sim.info().dt)
+    fs = float(np.float32(1.0) / np.float32(dt))
+    band = min(fs, 48000.0)
+    sos = capi.design_chebyshev_lowpass(fs, 0.45 * band, 0.5 * band)
+    out = {"receivers": int(sim.ir().shape[0]), "samples_in": steps, "rate_in_hz": round(fs, 1),
+           "sections": int(sos.shape[0])}
+    for name, call in (("chebyshev_linear", lambda: sim.postprocess_ir(48000.0, sos, True)),
+                       ("kaiser_sinc", lambda: sim.postprocess_ir_sinc(48000.0))):
+        y = call()
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            call()
+            best = min(best, time.perf_counter() - t0)
+        out[name + "_ms"] = round(best * 1e3, 3)
+        out["samples_out"] = int(y.shape[1])
+    sim.close()
+    return out
+
+
 def bench_adjoint(args, stream, dev):
     """The inverse-design configuration: 128x128x96, 6 materials x 2
     sections, 4 receivers, 4000 steps, checkpoints every 64.  The forward
@@ -475,6 +508,8 @@ def run_virs(args):
         }
     if args.adjoint:
         variants["adjoint_inverse_design"] = bench_adjoint(args, stream, dev)
+    if args.variants:
+        variants["ir_postprocess"] = bench_ir_postprocess(dev)
     if args.slabs and world == 1:
         variants["slabs_2_one_gpu"] = bench_slabs(sc, args, dev)
     if args.batch_steps:

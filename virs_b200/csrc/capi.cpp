@@ -324,8 +324,8 @@ virs_status default_filters(virs_sim *s)
     return VIRS_OK;
 }
 
-// the filter states, [2(S+1)][nb] (see step_common.cuh)
-size_t state_bytes(const virs_sim *s) { return std::max<uint64_t>(s->nb, 1) * (s->nsec + 1) * 2 * sizeof(float); }
+// the filter states: state_groups vectors of four floats per slot (internal.hpp)
+size_t state_bytes(const virs_sim *s) { return std::max<uint64_t>(s->nb, 1) * state_groups(s->nsec) * 4 * sizeof(float); }
 
 virs_status alloc_states(virs_sim *s)
 {

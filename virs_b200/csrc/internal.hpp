@@ -31,6 +31,19 @@ virs_status cuda_fail(cudaError_t e, const char *what);
         if (s_ != VIRS_OK) return s_;        \
     } while (0)
 
+// ---- filter states ----------------------------------------------------------
+//
+// The 2(S+1) filter states of each boundary slot (step_common.cuh) come in
+// groups of four, one 16-byte vector per group; group g of every slot is
+// one array of vectors, so a warp's consecutive slots read consecutive
+// vectors and a slot's states take one vector load per group.  Entry e of
+// slot s sits at float index state_index(e, s, nb).
+__host__ __device__ inline uint64_t state_index(uint32_t e, uint64_t s, uint64_t nb)
+{
+    return ((uint64_t)(e >> 2) * nb + s) * 4u + (e & 3u);
+}
+inline uint32_t state_groups(uint32_t nsec) { return (2u * (nsec + 1u) + 3u) / 4u; }
+
 // ---- device buffer -----------------------------------------------------------
 
 struct DevBuf {
@@ -80,7 +93,7 @@ struct StepArgs {
     const uint8_t *bnrm;    // [nb] air-neighbour mask of each slot's voxel (rigid-wall update)
     const uint8_t *bmat;
     const float *bw;
-    float *state;           // [2(S+1)][nb]: X_q[n-1], X_q[n-2] of the cascade's input and section outputs
+    float *state;           // X_q[n-1], X_q[n-2] of the cascade's input and section outputs (state_index)
     const float *coef;      // [M][S][5]
     const float *hard;      // per-step hard source values (scaled)
     const uint32_t *ctr;    // device step counter

@@ -47,7 +47,7 @@ struct AdjArgs {
     const float *bw;
     const float *coef;         // [M][S][5]
     const float4 *rec;         // forward records of this step {free, p, q, 0}
-    const float *fst;          // forward states before this step [2(S+1)][nb] (shared cascade layout)
+    const float *fst;          // forward states before this step (the cascade's layout, state_index)
     float *ast;                // state adjoints, four per section [S][4][nb]
     float *dbar, *cq;          // per slot
     double *grad;              // [M][S][5]
@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
         float in = __fsub_rn(rec.y, rec.z);
         for (uint32_t q = 0; q < S; ++q) {
             const float *kq = kc + 5 * q;
-            const float s0 = a.fst[(uint64_t)(2 * q + 0) * a.nb + b], s1 = a.fst[(uint64_t)(2 * q + 1) * a.nb + b];
-            const float s2 = a.fst[(uint64_t)(2 * q + 2) * a.nb + b], s3 = a.fst[(uint64_t)(2 * q + 3) * a.nb + b];
+            const float s0 = a.fst[state_index(2 * q + 0, b, a.nb)], s1 = a.fst[state_index(2 * q + 1, b, a.nb)];
+            const float s2 = a.fst[state_index(2 * q + 2, b, a.nb)], s3 = a.fst[state_index(2 * q + 3, b, a.nb)];
             xin[q] = in;
             float yv = __fmaf_rn(kq[0], in, __fmul_rn(kq[1], s0));
             yv = __fmaf_rn(kq[2], s1, yv);
@@ -106,9 +106,8 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
             const uint64_t o0 = (uint64_t)(4 * q + 0) * a.nb, o1 = (uint64_t)(4 * q + 1) * a.nb;
             const uint64_t o2 = (uint64_t)(4 * q + 2) * a.nb, o3 = (uint64_t)(4 * q + 3) * a.nb;
             const double yt = yb + (double)aq[o2];
-            const uint64_t f0 = (uint64_t)(2 * q) * a.nb;
-            const double s0 = a.fst[f0 + b], s1 = a.fst[f0 + a.nb + b], s2 = a.fst[f0 + 2 * a.nb + b],
-                         s3 = a.fst[f0 + 3 * a.nb + b];
+            const double s0 = a.fst[state_index(2 * q, b, a.nb)], s1 = a.fst[state_index(2 * q + 1, b, a.nb)],
+                         s2 = a.fst[state_index(2 * q + 2, b, a.nb)], s3 = a.fst[state_index(2 * q + 3, b, a.nb)];
             double *g = gsm + (uint64_t)(m * S + q) * 5;
             atomicAdd(g + 0, yt * (double)xin[q]);
             atomicAdd(g + 1, yt * s0);

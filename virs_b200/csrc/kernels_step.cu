@@ -21,7 +21,8 @@
 //     and updated by k_boundary, one thread per entry of the compacted,
 //     ascending boundary list: the leapfrog and the biquad correction
 //     together, with no divergence in the stencil kernel; the filter states
-//     are stored [2(S+1)][slot] so a warp touches consecutive words.
+//     are stored in 16-byte groups per slot (state_index in internal.hpp) so
+//     a warp touches consecutive vectors.
 //
 // Arithmetic order is fixed with _rn intrinsics so that the result is
 // bit-identical to the CPU oracle: the reference CUDA build contracts

@@ -319,62 +319,77 @@ __device__ __forceinline__ float correct(const StepArgs &a, float r, float d, fl
 // section q+1, so the two past outputs a DF1 section keeps (y[n-1], y[n-2])
 // are the two past inputs of the next one: S sections need 2(S+1) values,
 // X_q[n-1] and X_q[n-2] for the input X_0 = p - p^{n-1} and the outputs
-// X_{q+1} = y_q.  They are stored [2(S+1)][nb] (entry 2q holds X_q[n-1],
-// 2q+1 holds X_q[n-2]).  This is the reference's four states per section
-// (simulator_gpu.cu:126-146) without the copies, so every value, and the
-// result, is the same.
+// X_{q+1} = y_q (entry 2q holds X_q[n-1], 2q+1 holds X_q[n-2]).  This is
+// the reference's four states per section (simulator_gpu.cu:126-146)
+// without the copies, so every value, and the result, is the same.  They
+// are stored in groups of four entries per slot (state_index in
+// internal.hpp): one 16-byte load and store per group.
 
 // up to MAXS sections, fully unrolled, in two parts so that a caller can
-// issue the loads of several voxels before any arithmetic: bload reads the
+// issue the loads of a voxel before any arithmetic: bload reads the
 // material, the weight and every state of a slot; bcompute reads the
 // coefficients (they depend on the material), runs the cascade, writes the
 // states and returns the corrected value.
 template <int MAXS> struct BState {
+    static constexpr int NG = (2 * (MAXS + 1) + 3) / 4; // vector groups
     uint32_t m;
     float wf;
-    float h[MAXS + 1][2];
+    float h[4 * NG];                                    // entry e = 2q + j
 };
 
 template <int MAXS> __device__ __forceinline__ void bload(const StepArgs &a, uint64_t slot, BState<MAXS> &b)
 {
-    const uint32_t ns = a.nsec;
-    const float *st = a.state + slot;
+    const uint32_t ng = (2u * (a.nsec + 1u) + 3u) / 4u;
+    const float4 *st = reinterpret_cast<const float4 *>(a.state) + slot;
     b.m = __ldg(a.bmat + slot);
     b.wf = __ldg(a.bw + slot);
 #pragma unroll
-    for (int q = 0; q <= MAXS; ++q)
-        if (q <= (int)ns)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) b.h[q][j] = st[(uint64_t)(2 * q + j) * a.nb];
+    for (int g = 0; g < BState<MAXS>::NG; ++g)
+        if ((uint32_t)g < ng) {
+            const float4 v = st[(uint64_t)g * a.nb];
+            b.h[4 * g] = v.x;
+            b.h[4 * g + 1] = v.y;
+            b.h[4 * g + 2] = v.z;
+            b.h[4 * g + 3] = v.w;
+        }
 }
 
 template <int MAXS>
 __device__ __forceinline__ float bcompute(const StepArgs &a, float r, float ce, float qv, uint64_t slot,
                                           const BState<MAXS> &b)
 {
-    const uint32_t ns = a.nsec;
-    const uint64_t nb = a.nb;
-    float *st = a.state + slot;
+    const uint32_t ns = a.nsec, ng = (2u * (ns + 1u) + 3u) / 4u;
+    float4 *st = reinterpret_cast<float4 *>(a.state) + slot;
     const float *kc = a.coef + (uint64_t)b.m * ns * 5;
     const float d = __fsub_rn(ce, qv);
-    float in = d, last = b.h[0][0];
+    float in = d, last = b.h[0];
+    float nv[4 * BState<MAXS>::NG]; // the states after this step
+#pragma unroll
+    for (int e = 0; e < 4 * BState<MAXS>::NG; ++e) nv[e] = 0.f;
 #pragma unroll
     for (int q = 0; q < MAXS; ++q) {
         if (q < (int)ns) {
             const float *kq = kc + 5 * q;
-            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), b.h[q][0]));
-            y = __fmaf_rn(__ldg(kq + 2), b.h[q][1], y);
-            y = __fmaf_rn(-__ldg(kq + 3), b.h[q + 1][0], y);
-            y = __fmaf_rn(-__ldg(kq + 4), b.h[q + 1][1], y);
-            st[(uint64_t)(2 * q + 0) * nb] = in;
-            st[(uint64_t)(2 * q + 1) * nb] = b.h[q][0];
+            float y = __fmaf_rn(__ldg(kq), in, __fmul_rn(__ldg(kq + 1), b.h[2 * q]));
+            y = __fmaf_rn(__ldg(kq + 2), b.h[2 * q + 1], y);
+            y = __fmaf_rn(-__ldg(kq + 3), b.h[2 * q + 2], y);
+            y = __fmaf_rn(-__ldg(kq + 4), b.h[2 * q + 3], y);
+            nv[2 * q] = in;
+            nv[2 * q + 1] = b.h[2 * q];
             in = y;
-            last = b.h[q + 1][0];
+            last = b.h[2 * q + 2];
         }
     }
-    // the history of the last output
-    st[(uint64_t)(2 * ns + 0) * nb] = in;
-    st[(uint64_t)(2 * ns + 1) * nb] = last;
+    // the history of the last output, entries 2S and 2S+1
+#pragma unroll
+    for (int q = 0; q <= MAXS; ++q)
+        if (q == (int)ns) {
+            nv[2 * q] = in;
+            nv[2 * q + 1] = last;
+        }
+#pragma unroll
+    for (int g = 0; g < BState<MAXS>::NG; ++g)
+        if ((uint32_t)g < ng) st[(uint64_t)g * a.nb] = make_float4(nv[4 * g], nv[4 * g + 1], nv[4 * g + 2], nv[4 * g + 3]);
     return correct(a, r, d, in, qv, b.wf);
 }
 
@@ -385,22 +400,22 @@ __device__ __noinline__ float boundary_loop(const StepArgs &a, float r, float ce
     float in = d;
     const uint64_t nb = a.nb;
     const float *kc = a.coef + (uint64_t)__ldg(a.bmat + slot) * a.nsec * 5;
-    float *st = a.state + slot;
-    float x1 = st[0], x2 = st[nb];
-    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5, st += 2 * nb) {
-        const float y1 = st[2 * nb], y2 = st[3 * nb];
+    float *st = a.state;
+    float x1 = st[state_index(0, slot, nb)], x2 = st[state_index(1, slot, nb)];
+    for (uint32_t q = 0; q < a.nsec; ++q, kc += 5) {
+        const float y1 = st[state_index(2 * q + 2, slot, nb)], y2 = st[state_index(2 * q + 3, slot, nb)];
         float y = __fmaf_rn(__ldg(kc), in, __fmul_rn(__ldg(kc + 1), x1));
         y = __fmaf_rn(__ldg(kc + 2), x2, y);
         y = __fmaf_rn(-__ldg(kc + 3), y1, y);
         y = __fmaf_rn(-__ldg(kc + 4), y2, y);
-        st[0] = in;
-        st[nb] = x1;
+        st[state_index(2 * q, slot, nb)] = in;
+        st[state_index(2 * q + 1, slot, nb)] = x1;
         in = y;
         x1 = y1;
         x2 = y2;
     }
-    st[0] = in;
-    st[nb] = x1;
+    st[state_index(2 * a.nsec, slot, nb)] = in;
+    st[state_index(2 * a.nsec + 1, slot, nb)] = x1;
     return correct(a, r, d, in, qv, __ldg(a.bw + slot));
 }
 
