@@ -2990,15 +2990,15 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
         VIRS_CUDA(cudaMemcpyAsync(s->field[0].ptr, A.ckp.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
         VIRS_CUDA(cudaMemcpyAsync(s->field[1].ptr, A.ckq.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
         VIRS_CUDA(cudaMemcpyAsync(s->state.ptr, A.cks.as<char>() + c * sb, sb, cudaMemcpyDeviceToDevice, st));
-        const uint32_t c0 = (uint32_t)n0;
-        VIRS_CUDA(cudaMemcpyAsync(s->ctr.ptr, &c0, 4, cudaMemcpyHostToDevice, st));
-        VIRS_CUDA(cudaStreamSynchronize(st));
+        VIRS_CUDA(launch_set_u32(s->ctr.as<uint32_t>(), (uint32_t)n0, st));
         for (uint64_t n = n0; n < n1; ++n) {
             const uint64_t k = n - n0;
             VIRS_CUDA(cudaMemcpyAsync(A.segst.as<char>() + k * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
             cudaError_t e = launch_stencil(s, s->cur, st);
-            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, step_args(s, s->cur), BND_KEEP, st);
-            if (e == cudaSuccess) e = launch_keep_records(s->side.as<float4>(), A.segrec.as<float4>() + k * nb, nb, st);
+            // the boundary pass keeps its records straight in the segment's slot k
+            StepArgs ka = step_args(s, s->cur);
+            ka.side = A.segrec.as<float4>() + k * nb;
+            if (e == cudaSuccess) e = launch_boundary(s->prm.storage, ka, BND_KEEP, st);
             if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, s->cur), st);
             if (e != cudaSuccess) return cuda_fail(e, "adjoint recomputation");
             s->cur ^= 1;

@@ -256,7 +256,7 @@ cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *b
                                 int form, double K, double mix_y, double mix_d, double gain, cudaStream_t s);
 cudaError_t launch_adj_fix(float *Tn, float *Tb, const uint32_t *bidx, const float4 *rec, const float *dbar,
                            const float *cq, uint64_t nb, uint32_t nx, uint32_t ny, uint32_t px, cudaStream_t s);
-cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s);
+cudaError_t launch_set_u32(uint32_t *p, uint32_t v, cudaStream_t s);
 cudaError_t launch_zero_at(float *f, const uint32_t *pos, uint32_t n, cudaStream_t s);
 
 // mesh voxelisation (kernels_voxelize.cu)

@@ -59,6 +59,13 @@ struct AdjArgs {
 
 constexpr int AB = 256;
 
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
 {
     extern __shared__ double gsm[]; // block partial sums of the coefficient gradients
@@ -99,6 +106,10 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
             yv = __fmaf_rn(-kq[3], s2, yv);
             in = __fmaf_rn(-kq[4], s3, yv);
         }
+        // every lane of this warp holds a slot of one material (the loops
+        // over the sections are uniform: S is the same for every slot)
+        const unsigned act = __activemask();
+        const bool uni = act == 0xffffffffu && __all_sync(act, m == __shfl_sync(act, m, 0));
         double yb = ybar;
         for (int q = (int)S - 1; q >= 0; --q) {
             const float *kq = kc + 5 * q;
@@ -109,11 +120,19 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
             const double s0 = a.fst[state_index(2 * q, b, a.nb)], s1 = a.fst[state_index(2 * q + 1, b, a.nb)],
                          s2 = a.fst[state_index(2 * q + 2, b, a.nb)], s3 = a.fst[state_index(2 * q + 3, b, a.nb)];
             double *g = gsm + (uint64_t)(m * S + q) * 5;
-            atomicAdd(g + 0, yt * (double)xin[q]);
-            atomicAdd(g + 1, yt * s0);
-            atomicAdd(g + 2, yt * s1);
-            atomicAdd(g + 3, -yt * s2);
-            atomicAdd(g + 4, -yt * s3);
+            const double gv[5] = {yt * (double)xin[q], yt * s0, yt * s1, -yt * s2, -yt * s3};
+            if (uni) {
+                // a full warp of one material: one shared-memory add per
+                // coefficient instead of 32 contending ones
+#pragma unroll
+                for (int j = 0; j < 5; ++j) {
+                    const double v = warp_sum(gv[j]);
+                    if ((threadIdx.x & 31u) == 0) atomicAdd(g + j, v);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 5; ++j) atomicAdd(g + j, gv[j]);
+            }
             const double xbar = (double)kq[0] * yt + (double)aq[o0];
             const double x1 = (double)kq[1] * yt + (double)aq[o1];
             const double x2 = (double)kq[2] * yt;
@@ -148,13 +167,6 @@ __global__ void k_adj_fix(float *Tn, float *Tb, const uint32_t *__restrict bidx,
     const size_t i = ((size_t)z * ny + y) * px + x;
     Tn[i] = rec[b].x + dbar[b];
     Tb[i] = Tb[i] + dbar[b] - cq[b];
-}
-
-// the boundary data the reverse pass needs from one forward step
-__global__ void k_keep_records(const float4 *__restrict side, float4 *__restrict out, uint64_t nb)
-{
-    const uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < nb) out[b] = side[b];
 }
 
 } // namespace
@@ -205,10 +217,14 @@ cudaError_t launch_zero_at(float *f, const uint32_t *pos, uint32_t n, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_keep_records(const float4 *side, float4 *out, uint64_t nb, cudaStream_t s)
+namespace {
+__global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
+} // namespace
+
+// one device word set in stream order (no host staging buffer)
+cudaError_t launch_set_u32(uint32_t *p, uint32_t v, cudaStream_t s)
 {
-    if (nb == 0) return cudaSuccess;
-    k_keep_records<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(side, out, nb);
+    k_set_u32<<<1, 1, 0, s>>>(p, v);
     return cudaGetLastError();
 }
 
