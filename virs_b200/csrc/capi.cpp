@@ -603,7 +603,37 @@ virs_status check_err(virs_sim *s)
     return VIRS_OK;
 }
 
-int eff_planes(const virs_sim *s) { return s->zc > 0 ? s->zc : default_planes(s->nz); }
+// the SMs of a device (looked up once per device)
+int sm_count(int dev)
+{
+    static std::atomic<int> cache[64];
+    if (dev < 0 || dev >= 64) return 148;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+        cache[dev].store(n, std::memory_order_relaxed);
+        v = n;
+    }
+    return v;
+}
+
+// planes per block of a single simulation's stencil when none is set: the
+// batch default (32), or fewer, down to 4, on grids whose 32-plane tiling
+// would give the device fewer than about eight blocks per SM (a 128^3 grid
+// has 16 tiles of 128 x 8 voxels per plane: 48 blocks with 32 planes, 384
+// with 4)
+int eff_planes(const virs_sim *s)
+{
+    if (s->zc > 0) return s->zc;
+    const uint64_t tiles = (uint64_t)((s->px + 127) / 128) * ((s->ny + s->tile_rows - 1) / s->tile_rows);
+    const uint64_t want = 8ull * (uint64_t)sm_count(s->prm.device);
+    const uint64_t zc = (uint64_t)(s->nz > 2 ? s->nz - 2 : 1) * tiles / want;
+    return (int)std::min<uint64_t>(std::max<uint64_t>(zc, 4), (uint64_t)default_planes(s->nz));
+}
 
 // per tile of a rows x zc tiling of the TMA stencil, the stages whose codes
 // are all zero (kernels_classify.cu::k_tile_zero_mask)
@@ -689,7 +719,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.ny = s->ny;
     a.nz = s->nz;
     a.px = s->px;
-    a.zc = s->zc;
+    a.zc = eff_planes(s);
     a.zb = 1;
     a.ze = (int)s->nz - 1;
     a.c2dt2 = s->c2dt2;
