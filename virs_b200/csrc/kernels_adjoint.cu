@@ -59,10 +59,24 @@ struct AdjArgs {
 
 constexpr int AB = 256;
 
-__device__ __forceinline__ double warp_sum(double v)
+// The sum of v over the lanes of a full warp that share this lane's key
+// (peers = __match_any_sync of the key), complete at the group's lowest
+// lane: a tree over each group's ranks, every lane taking part in every
+// shuffle.  Lanes of a mixed warp (boundary slots of two or more
+// materials) then make one shared-memory add per group instead of one
+// each.
+__device__ __forceinline__ double peer_sum(unsigned peers, double v)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned rank = __popc(peers & ((1u << lane) - 1u));
+    peers &= 0xfffffffeu << lane; // the peers above this lane
+    while (__any_sync(0xffffffffu, peers != 0u)) {
+        const int next = __ffs(peers);
+        const double u = __shfl_sync(0xffffffffu, v, next > 0 ? next - 1 : 0);
+        if (next > 0) v += u;
+        peers &= __ballot_sync(0xffffffffu, (rank & 1u) == 0u);
+        rank >>= 1;
+    }
     return v;
 }
 
@@ -108,8 +122,10 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
         }
         // every lane of this warp holds a slot of one material (the loops
         // over the sections are uniform: S is the same for every slot)
-        const unsigned act = __activemask();
-        const bool uni = act == 0xffffffffu && __all_sync(act, m == __shfl_sync(act, m, 0));
+        // full warps sum over the lanes of each material first
+        const bool full = __activemask() == 0xffffffffu;
+        const unsigned peers = full ? __match_any_sync(0xffffffffu, m) : 0u;
+        const bool lead = full && (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
         double yb = ybar;
         for (int q = (int)S - 1; q >= 0; --q) {
             const float *kq = kc + 5 * q;
@@ -121,13 +137,11 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
                          s2 = a.fst[state_index(2 * q + 2, b, a.nb)], s3 = a.fst[state_index(2 * q + 3, b, a.nb)];
             double *g = gsm + (uint64_t)(m * S + q) * 5;
             const double gv[5] = {yt * (double)xin[q], yt * s0, yt * s1, -yt * s2, -yt * s3};
-            if (uni) {
-                // a full warp of one material: one shared-memory add per
-                // coefficient instead of 32 contending ones
+            if (full) {
 #pragma unroll
                 for (int j = 0; j < 5; ++j) {
-                    const double v = warp_sum(gv[j]);
-                    if ((threadIdx.x & 31u) == 0) atomicAdd(g + j, v);
+                    const double v = peer_sum(peers, gv[j]);
+                    if (lead) atomicAdd(g + j, v);
                 }
             } else {
 #pragma unroll
@@ -144,6 +158,108 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
             aq[o3] = (float)y2;
             yb = xbar;
         }
+        db += yb;
+        a.T[i] = (float)fr;
+        a.dbar[b] = (float)db;
+        a.cq[b] = (float)cqv;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB)
+        if (gsm[k] != 0.0) atomicAdd(a.grad + k, gsm[k]);
+}
+
+// The same for cascades of up to MAXS sections, unrolled: the forward
+// section inputs and the filter states stay in registers (the states are
+// read once, as the 16-byte groups of the cascade's layout).
+template <int MAXS> __global__ void __launch_bounds__(AB) k_adj_boundary_s(const AdjArgs a)
+{
+    constexpr int NG = (2 * (MAXS + 1) + 3) / 4;
+    extern __shared__ double gsm[]; // block partial sums of the coefficient gradients
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB) gsm[k] = 0.0;
+    __syncthreads();
+    const uint64_t b = (uint64_t)blockIdx.x * AB + threadIdx.x;
+    if (b < a.nb) {
+        const uint32_t ref = a.bidx[b];
+        const uint32_t S = a.nsec, m = a.bmat[b];
+        const float4 rec = a.rec[b];
+        const double w = (double)a.bw[b];
+        float h[4 * NG];
+        const float4 *st = reinterpret_cast<const float4 *>(a.fst) + b;
+        const uint32_t ng = (2u * (S + 1u) + 3u) / 4u;
+#pragma unroll
+        for (int g = 0; g < NG; ++g)
+            if ((uint32_t)g < ng) {
+                const float4 v = st[(uint64_t)g * a.nb];
+                h[4 * g] = v.x;
+                h[4 * g + 1] = v.y;
+                h[4 * g + 2] = v.z;
+                h[4 * g + 3] = v.w;
+            }
+        const uint32_t x = ref % a.nx, t = ref / a.nx, y = t % a.ny, z = t / a.ny;
+        const size_t i = ((size_t)z * a.ny + y) * a.px + x;
+        const float f = a.T[i];
+        const double kgw = a.K * a.gain * w;
+        double fr, ybar, db = 0.0, cqv = 0.0;
+        if (a.form == VIRS_BOUNDARY_REFERENCE) {
+            fr = f;
+            ybar = -kgw * a.mix_y * f;
+            db = -kgw * a.mix_d * f;
+        } else {
+            const double ac = kgw * a.mix_d * 0.5;
+            fr = f / (1.0 + ac);
+            ybar = -kgw * a.mix_y * fr;
+            cqv = ac * fr;
+        }
+        // forward inputs of every section at this step
+        const float *kc = a.coef + (uint64_t)m * S * 5;
+        float xin[MAXS];
+        float in = __fsub_rn(rec.y, rec.z);
+#pragma unroll
+        for (int q = 0; q < MAXS; ++q)
+            if (q < (int)S) {
+                const float *kq = kc + 5 * q;
+                xin[q] = in;
+                float yv = __fmaf_rn(kq[0], in, __fmul_rn(kq[1], h[2 * q]));
+                yv = __fmaf_rn(kq[2], h[2 * q + 1], yv);
+                yv = __fmaf_rn(-kq[3], h[2 * q + 2], yv);
+                in = __fmaf_rn(-kq[4], h[2 * q + 3], yv);
+            }
+        const bool full = __activemask() == 0xffffffffu;
+        const unsigned peers = full ? __match_any_sync(0xffffffffu, m) : 0u;
+        const bool lead = full && (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
+        double yb = ybar;
+#pragma unroll
+        for (int q = MAXS - 1; q >= 0; --q)
+            if (q < (int)S) {
+                const float *kq = kc + 5 * q;
+                float *aq = a.ast + b;
+                const uint64_t o0 = (uint64_t)(4 * q + 0) * a.nb, o1 = (uint64_t)(4 * q + 1) * a.nb;
+                const uint64_t o2 = (uint64_t)(4 * q + 2) * a.nb, o3 = (uint64_t)(4 * q + 3) * a.nb;
+                const double yt = yb + (double)aq[o2];
+                double *g = gsm + (uint64_t)(m * S + q) * 5;
+                const double gv[5] = {yt * (double)xin[q], yt * (double)h[2 * q], yt * (double)h[2 * q + 1],
+                                      -yt * (double)h[2 * q + 2], -yt * (double)h[2 * q + 3]};
+                if (full) {
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) {
+                        const double v = peer_sum(peers, gv[j]);
+                        if (lead) atomicAdd(g + j, v);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) atomicAdd(g + j, gv[j]);
+                }
+                const double xbar = (double)kq[0] * yt + (double)aq[o0];
+                const double x1 = (double)kq[1] * yt + (double)aq[o1];
+                const double x2 = (double)kq[2] * yt;
+                const double y1 = -(double)kq[3] * yt + (double)aq[o3];
+                const double y2 = -(double)kq[4] * yt;
+                aq[o0] = (float)x1;
+                aq[o1] = (float)x2;
+                aq[o2] = (float)y1;
+                aq[o3] = (float)y2;
+                yb = xbar;
+            }
         db += yb;
         a.T[i] = (float)fr;
         a.dbar[b] = (float)db;
@@ -188,7 +304,11 @@ cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *b
     AdjArgs a{T, bidx, bmat, bw, coef, rec, fst, ast, dbar, cq, grad, nb, nx, ny, px, nsec, nmat * nsec * 5, form,
               K, mix_y, mix_d, gain};
     const size_t sm = (size_t)a.ncoef * sizeof(double);
-    k_adj_boundary<<<(unsigned)((nb + AB - 1) / AB), AB, sm, s>>>(a);
+    const unsigned g = (unsigned)((nb + AB - 1) / AB);
+    if (nsec <= 1) k_adj_boundary_s<1><<<g, AB, sm, s>>>(a);
+    else if (nsec == 2) k_adj_boundary_s<2><<<g, AB, sm, s>>>(a);
+    else if (nsec <= 4) k_adj_boundary_s<4><<<g, AB, sm, s>>>(a);
+    else k_adj_boundary<<<g, AB, sm, s>>>(a);
     return cudaGetLastError();
 }
 
