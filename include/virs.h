@@ -206,6 +206,26 @@ virs_status virs_slab_exchange(virs_sim *lo, virs_sim *hi);
  * refused. */
 virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64_t steps);
 
+/* One step of a slab in two parts, for hosts that exchange the ghost planes
+ * themselves (no reference counterpart; one process per GPU, the planes
+ * sent with NCCL or MPI between the parts):
+ *   virs_slab_step_begin  the stencil over the slab's interior planes 2 ..
+ *                         nz-3, which read no ghost plane, on `stream`
+ *                         (NULL: the handle's stream) after the handle's
+ *                         last queued work;
+ *   virs_slab_step_end    the edge planes 1 and nz-2, the boundary pass and
+ *                         the sources and receivers, then the step count
+ *                         and buffer parity advance.
+ * Between the two the host sends the slab's first and last owned planes of
+ * p^n (virs_slab_planes, before this step) and receives its ghost planes:
+ * the interior launch reads neither and writes only p^{n+1}, so the
+ * exchange can run beside it.  virs_slab_step_end must follow, in stream
+ * order, both virs_slab_step_begin and the receives.  A second begin
+ * before the end, or virs_run / virs_slab_run in between, is refused
+ * (VIRS_E_STATE).  The device stop rule is refused. */
+virs_status virs_slab_step_begin(virs_sim *sim, void *stream);
+virs_status virs_slab_step_end(virs_sim *sim, void *stream);
+
 virs_status virs_get_grid_info(const virs_sim *sim, virs_grid_info *out);
 
 /* Replaces buildSpongeLayer / buildSpongeLayerGPU (simulator_dispatch.cpp:83-91,

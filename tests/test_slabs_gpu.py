@@ -235,3 +235,98 @@ def test_slab_run_thin_slabs_match_whole_grid(parts):
     for s in sims:
         s.close()
     whole.close()
+
+
+@pytest.mark.parametrize("nparts,storage", [(2, capi.STORAGE_F32), (3, capi.STORAGE_BF16)])
+def test_split_slab_step_matches_whole_grid(nparts, storage):
+    """virs_slab_step_begin / virs_slab_step_end with the ghost planes
+    exchanged between the two parts (the form a multi-process host uses,
+    here with device copies in one process): the interior launches of
+    every slab run on a side stream while the copies run on the main one;
+    receivers and owned planes equal the whole grid's bit for bit."""
+    import torch
+    sc = _scene(150)
+    scale = 64.0 if storage else 0.0
+    whole, meta = scenes.build_simulation(sc, storage=storage, storage_scale=scale)
+    nx, ny, _ = meta["shape"]
+    plane = nx * ny
+    whole.run(sc.steps)
+    want_ir = whole.ir()
+    want_p, want_pp = whole.pressure(prev=True)
+    parts, _ = scenes.build_slabs(sc, nparts, storage=storage, storage_scale=scale)
+    sims = [p[0] for p in parts]
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream()
+    for _ in range(sc.steps):
+        side.wait_stream(main)
+        for s in sims:
+            s.slab_step_begin(side.cuda_stream)
+        slabs.exchange_local(sims)
+        main.wait_stream(side)
+        for s in sims:
+            s.slab_step_end(main.cuda_stream)
+    torch.cuda.synchronize()
+    ir = np.zeros_like(want_ir)
+    for s, z_lo, z_hi, own_r in parts:
+        if own_r.any():
+            ir[own_r] = s.ir()
+        p, pp = s.pressure(prev=True)
+        gown = slice(z_lo * plane, z_hi * plane)
+        assert np.array_equal(p[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_p[gown].view(np.uint32))
+        assert np.array_equal(pp[plane:(z_hi - z_lo + 1) * plane].view(np.uint32), want_pp[gown].view(np.uint32))
+    assert np.abs(want_ir).max() > 0
+    assert np.array_equal(ir.view(np.uint32), want_ir.view(np.uint32))
+    for s in sims:
+        s.close()
+    whole.close()
+
+
+def test_split_slab_step_order_checked():
+    """A second begin, a run, or an end without a begin is refused, and the
+    handle stays usable."""
+    import torch
+    st = torch.cuda.current_stream().cuda_stream
+    sc = _scene(20)
+    parts, _ = scenes.build_slabs(sc, 2)
+    a, b = (p[0] for p in parts)
+    with pytest.raises(capi.VirsError) as e:
+        a.slab_step_end(st)
+    assert e.value.status == capi.E_STATE
+    a.slab_step_begin(st)
+    with pytest.raises(capi.VirsError) as e:
+        a.slab_step_begin(st)
+    assert e.value.status == capi.E_STATE
+    with pytest.raises(capi.VirsError) as e:
+        a.run(1)
+    assert e.value.status == capi.E_STATE
+    with pytest.raises(capi.VirsError) as e:
+        capi.slab_run([a, b], 1)
+    assert e.value.status == capi.E_STATE
+    b.slab_step_begin(st)
+    slabs.exchange_local([a, b])
+    a.slab_step_end(st)
+    b.slab_step_end(st)
+    capi.slab_run([a, b], 3)
+    for s in (a, b):
+        s.synchronize()
+        assert s.info().steps_done == 4
+        s.close()
+
+
+def test_slab_run_class_single_rank_matches_whole_grid():
+    """slabs.SlabRun on one rank (the grid as one slab, no neighbours, so no
+    collective): the interior launch on its side stream and the end of the
+    step on the current stream give the whole grid's results bit for bit."""
+    sc = _scene(80)
+    whole, _ = scenes.build_simulation(sc)
+    whole.run(sc.steps)
+    want_ir = whole.ir()
+    parts, _ = scenes.build_slabs(sc, 1)
+    sim = parts[0][0]
+    slabs.SlabRun(sim, 0, 1).run(sc.steps)
+    sim.synchronize()
+    got = sim.ir()
+    assert np.abs(want_ir).max() > 0
+    assert np.array_equal(got.view(np.uint32), want_ir.view(np.uint32))
+    sim.close()
+    whole.close()

@@ -115,6 +115,8 @@ _SIGS = {
                                   C.POINTER(C.c_uint64)], C.c_int),
     "virs_slab_exchange": ([_P, _P], C.c_int),
     "virs_slab_run": ([_P, C.c_uint32, C.c_uint64], C.c_int),
+    "virs_slab_step_begin": ([_P, _P], C.c_int),
+    "virs_slab_step_end": ([_P, _P], C.c_int),
     "virs_get_time_blocking": ([_P, _P, _P, _P, _P], C.c_int),
     "virs_check_bounded_wait": ([_P, C.c_uint32], C.c_int),
     "virs_autotune": ([_P, C.c_uint32, _P], C.c_int),
@@ -410,6 +412,16 @@ class Simulation:
 
     def run(self, steps: int, stream: int | None = None):
         check(lib().virs_run(self._h, steps, _stream(stream)))
+
+    def slab_step_begin(self, stream: int | None = None):
+        """virs_slab_step_begin: the stencil over this slab's interior planes
+        (no ghost plane read), on `stream` after the handle's queued work."""
+        check(lib().virs_slab_step_begin(self._h, _stream(stream)))
+
+    def slab_step_end(self, stream: int | None = None):
+        """virs_slab_step_end: the edge planes, the boundary pass and the
+        sources and receivers, once the ghost planes are filled."""
+        check(lib().virs_slab_step_end(self._h, _stream(stream)))
 
     def run_host(self, steps: int, signal=None, ir_out=None, stream: int | None = None):
         s = None if signal is None else _c(signal, np.float32)

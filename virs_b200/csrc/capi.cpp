@@ -248,6 +248,7 @@ struct virs_sim {
         CUtensorMap mapP[2], mapQ[2];
     } adj;
     bool fields_valid = true;      // false after virs_adjoint until the next start
+    bool slab_open = false;        // virs_slab_step_begin ran, virs_slab_step_end not yet
 
     ~virs_sim()
     {
@@ -1722,6 +1723,7 @@ VIRS_EXPORT virs_status virs_start_simulation(virs_sim *s, uint64_t steps)
     VIRS_CUDA(zero_on(s->stream, s->ctr.ptr, 4));
     if (s->stopbuf.ptr) VIRS_CUDA(zero_on(s->stream, s->stopbuf.ptr, s->stopbuf.bytes));
     s->stopped = false;
+    s->slab_open = false;
     s->cur = 0;
     s->steps_done = 0;
     s->out0.clear();
@@ -1741,6 +1743,7 @@ VIRS_EXPORT virs_status virs_run(virs_sim *s, uint64_t steps, void *stream)
 {
     if (!s) return fail(VIRS_E_ARG, "virs_run: null");
     if (!started(s)) return fail(VIRS_E_STATE, "call virs_start_simulation first");
+    if (s->slab_open) return fail(VIRS_E_STATE, "virs_run: a step begun by virs_slab_step_begin has not ended");
     VIRS_TRY(use_device(s));
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     if (steps == 0) return VIRS_OK;
@@ -1972,6 +1975,8 @@ VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64
     if (!slabs || n == 0) return fail(VIRS_E_ARG, "virs_slab_run: no slabs");
     for (uint32_t k = 0; k < n; ++k) {
         if (!slabs[k]) return fail(VIRS_E_ARG, "virs_slab_run: null slab");
+        if (slabs[k]->slab_open)
+            return fail(VIRS_E_STATE, "virs_slab_run: a step begun by virs_slab_step_begin has not ended");
         if (slabs[k]->stop_rule) return fail(VIRS_E_STATE, "virs_slab_run: the device stop rule is not for slabs");
     }
     if (n == 1) {
@@ -2022,6 +2027,59 @@ VIRS_EXPORT virs_status virs_slab_run(virs_sim *const *slabs, uint32_t n, uint64
         i = steps / SLAB_GRAPH_STEPS * SLAB_GRAPH_STEPS;
     }
     for (; i < steps; ++i) VIRS_CUDA(slab_step(slabs, n, pb));
+    return VIRS_OK;
+}
+
+namespace {
+// a slab handle ready for one more step of the split form
+virs_status slab_step_ready(virs_sim *s, const char *who)
+{
+    if (!s->slab || !started(s)) return fail(VIRS_E_STATE, std::string(who) + ": a started slab handle is needed");
+    if (!s->fields_valid) return fail(VIRS_E_STATE, std::string(who) + ": the fields were consumed by virs_adjoint");
+    if (s->stop_rule) return fail(VIRS_E_STATE, std::string(who) + ": the device stop rule is not for slabs");
+    if (s->steps_done + 1 >= (1ull << 32)) return fail(VIRS_E_ARG, "step counter would pass 2^32");
+    VIRS_TRY(use_device(s));
+    VIRS_TRY(ready_to_run(s));
+    VIRS_TRY(ensure_ir(s, s->steps_done + 1));
+    if (s->depth > 0 && zero_masks_useful(s) && s->nz > 5 &&
+        (s->zmi_rows != s->tile_rows || s->zmi_zc != eff_planes(s))) {
+        s->zmi_rows = s->zmi_zc = 0;
+        VIRS_TRY(build_zero_masks(s, s->tile_rows, eff_planes(s), s->zmask_in, 2, s->nz - 2));
+        s->zmi_rows = s->tile_rows;
+        s->zmi_zc = eff_planes(s);
+    }
+    return VIRS_OK;
+}
+} // namespace
+
+VIRS_EXPORT virs_status virs_slab_step_begin(virs_sim *s, void *stream)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_slab_step_begin: null");
+    if (s->slab_open) return fail(VIRS_E_STATE, "virs_slab_step_begin: the step begun before has not ended");
+    VIRS_TRY(slab_step_ready(s, "virs_slab_step_begin"));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    VIRS_CUDA(cudaStreamWaitEvent(st, s->done, 0));
+    const int nz = (int)s->nz;
+    if (nz - 2 > 2) VIRS_CUDA(launch_stencil_range(s, s->cur, st, 2, nz - 2));
+    s->slab_open = true;
+    return VIRS_OK;
+}
+
+VIRS_EXPORT virs_status virs_slab_step_end(virs_sim *s, void *stream)
+{
+    if (!s) return fail(VIRS_E_ARG, "virs_slab_step_end: null");
+    if (!s->slab_open) return fail(VIRS_E_STATE, "virs_slab_step_end: no step begun (virs_slab_step_begin)");
+    VIRS_TRY(use_device(s));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    const int nz = (int)s->nz, par = s->cur;
+    s->slab_open = false;
+    VIRS_CUDA(launch_stencil_range(s, par, st, 1, 2));
+    if (nz - 2 > 1) VIRS_CUDA(launch_stencil_range(s, par, st, nz - 2, nz - 1));
+    VIRS_CUDA(launch_boundary(s->prm.storage, step_args(s, par), BND_UPDATE, st));
+    VIRS_CUDA(launch_post(s->prm.storage, post_args(s, par), st));
+    s->cur ^= 1;
+    s->steps_done += 1;
+    VIRS_CUDA(cudaEventRecord(s->done, st));
     return VIRS_OK;
 }
 

@@ -113,25 +113,35 @@ def exchange_local(sims) -> None:
 
 
 class SlabRun:
-    """Drives one slab of a distributed grid: per step, the halo exchange
-    with the neighbouring ranks, then the step on the current torch stream.
+    """Drives one slab of a distributed grid.  Per step: the stencil over
+    the slab's interior planes (virs_slab_step_begin) on a side stream,
+    meanwhile the halo exchange with the neighbouring ranks on the current
+    torch stream, then, after both, the edge planes, the boundary pass and
+    the sources and receivers (virs_slab_step_end) on the current stream.
+    The interior launch reads no ghost plane and the exchange sends planes
+    of p^n that no kernel of the step writes, so the two run side by side.
 
     `sim` is a capi.Simulation set up with `setup_slab`, classified,
     configured and started; every rank runs the same number of steps."""
 
     def __init__(self, sim, rank: int, world: int, group=None):
         self.sim, self.rank, self.world, self.group = sim, rank, world, group
+        self._side = None
 
     def run(self, steps: int) -> None:
         import torch
-        stream = torch.cuda.current_stream().cuda_stream
+        d = int(self.sim.params.device)
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=d)
+        main = torch.cuda.current_stream(d)
         for _ in range(steps):
             first, last, glo, ghi, nb = self.sim.slab_planes()
-            d = int(self.sim.params.device)
+            self._side.wait_stream(main)
+            self.sim.slab_step_begin(self._side.cuda_stream)
             exchange(device_bytes(first, nb, d), device_bytes(last, nb, d), device_bytes(glo, nb, d),
-                     device_bytes(ghi, nb, d),
-                     self.rank, self.world, self.group)
-            self.sim.run(1, stream=stream)
+                     device_bytes(ghi, nb, d), self.rank, self.world, self.group)
+            main.wait_stream(self._side)
+            self.sim.slab_step_end(main.cuda_stream)
 
 
 def setup_slab(sim, shape, cell_size: float, flags, wall_material, rank: int, world: int, sponge_width: int):
