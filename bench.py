@@ -366,7 +366,7 @@ def bench_adjoint(args, stream, dev):
     around the synchronous call."""
     import torch
     from virs_b200 import scenes
-    sc, guess = scenes.inverse_design()
+    sc, guess = scenes.inverse_design(steps=args.adjoint_steps)
     every = 64
     sim, _ = scenes.build_simulation(sc)
     nvox = int(np.prod(sim.shape))
@@ -698,6 +698,8 @@ def main():
                     help="skip the variant that runs the hall as two z-slabs on one GPU")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the inverse-design (adjoint) variant")
+    ap.add_argument("--adjoint-steps", type=int, default=4000,
+                    help="steps of the inverse-design leg (4000: the configuration; fewer for profiling)")
     ap.add_argument("--batch-steps", type=int, default=60, help="timed steps of the batched workload (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--storage", choices=list(STORAGE_NAMES), default="f32",
