@@ -331,7 +331,10 @@ def bench_ir_postprocess(dev, steps=4000, reps=5):
     (virs_postprocess_ir) and by the Kaiser-windowed sinc
     (virs_postprocess_ir_sinc), each peak-normalised.  Host clock around a
     whole call (size query, kernels, copy of the result to the host), best
-    of `reps` after one untimed call."""
+    of `reps` after one untimed call.  The hall's simulation rate (38 kHz)
+    is below 48 kHz: the step upsamples, and the anti-alias design for that
+    rate, with its stop band at the simulation's Nyquist frequency, is one
+    section."""
     from virs_b200 import capi, scenes
     sc = scenes.large_hall(steps=steps, size=(128, 128, 128))
     sim, _ = scenes.build_simulation(sc, device=dev)
