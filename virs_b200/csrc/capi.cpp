@@ -710,6 +710,7 @@ StepArgs step_args(const virs_sim *s, int parity)
     a.bnrm = s->bnrm.as<uint8_t>();
     a.bw = s->bw.as<float>();
     a.state = s->state.as<float>();
+    a.state_out = nullptr;
     a.coef = s->coef.as<float>();
     a.hard = s->hard.as<float>();
     a.ctr = s->ctr.as<uint32_t>();
@@ -3077,15 +3078,20 @@ VIRS_EXPORT virs_status virs_adjoint(virs_sim *s, const float *dl_dir, double *g
         s->cur = 0;
         VIRS_CUDA(cudaMemcpyAsync(s->field[0].ptr, A.ckp.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
         VIRS_CUDA(cudaMemcpyAsync(s->field[1].ptr, A.ckq.as<char>() + c * fb, fb, cudaMemcpyDeviceToDevice, st));
-        VIRS_CUDA(cudaMemcpyAsync(s->state.ptr, A.cks.as<char>() + c * sb, sb, cudaMemcpyDeviceToDevice, st));
+        VIRS_CUDA(cudaMemcpyAsync(A.segst.ptr, A.cks.as<char>() + c * sb, sb, cudaMemcpyDeviceToDevice, st));
         VIRS_CUDA(launch_set_u32(s->ctr.as<uint32_t>(), (uint32_t)n0, st));
         for (uint64_t n = n0; n < n1; ++n) {
             const uint64_t k = n - n0;
-            VIRS_CUDA(cudaMemcpyAsync(A.segst.as<char>() + k * sb, s->state.ptr, sb, cudaMemcpyDeviceToDevice, st));
             cudaError_t e = launch_stencil(s, s->cur, st);
-            // the boundary pass keeps its records straight in the segment's slot k
+            // the boundary pass keeps its records straight in the segment's
+            // slot k, and reads the states before the step from slot k and
+            // writes those after it to slot k + 1 (the last step's to the
+            // handle's own states)
             StepArgs ka = step_args(s, s->cur);
             ka.side = A.segrec.as<float4>() + k * nb;
+            ka.state = reinterpret_cast<float *>(A.segst.as<char>() + k * sb);
+            ka.state_out = k + 1 < every ? reinterpret_cast<float *>(A.segst.as<char>() + (k + 1) * sb)
+                                         : s->state.as<float>();
             if (e == cudaSuccess) e = launch_boundary(s->prm.storage, ka, BND_KEEP, st);
             if (e == cudaSuccess) e = launch_post(s->prm.storage, post_args(s, s->cur), st);
             if (e != cudaSuccess) return cuda_fail(e, "adjoint recomputation");

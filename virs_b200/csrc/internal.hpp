@@ -94,6 +94,7 @@ struct StepArgs {
     const uint8_t *bmat;
     const float *bw;
     float *state;           // X_q[n-1], X_q[n-2] of the cascade's input and section outputs (state_index)
+    float *state_out;       // where the pass writes the states after the step (nullptr: in place, `state`)
     const float *coef;      // [M][S][5]
     const float *hard;      // per-step hard source values (scaled)
     const uint32_t *ctr;    // device step counter

@@ -359,7 +359,7 @@ __device__ __forceinline__ float bcompute(const StepArgs &a, float r, float ce, 
                                           const BState<MAXS> &b)
 {
     const uint32_t ns = a.nsec, ng = (2u * (ns + 1u) + 3u) / 4u;
-    float4 *st = reinterpret_cast<float4 *>(a.state) + slot;
+    float4 *st = reinterpret_cast<float4 *>(a.state_out ? a.state_out : a.state) + slot;
     const float *kc = a.coef + (uint64_t)b.m * ns * 5;
     const float d = __fsub_rn(ce, qv);
     float in = d, last = b.h[0];
@@ -400,10 +400,11 @@ __device__ __noinline__ float boundary_loop(const StepArgs &a, float r, float ce
     float in = d;
     const uint64_t nb = a.nb;
     const float *kc = a.coef + (uint64_t)__ldg(a.bmat + slot) * a.nsec * 5;
-    float *st = a.state;
-    float x1 = st[state_index(0, slot, nb)], x2 = st[state_index(1, slot, nb)];
+    const float *si = a.state;
+    float *st = a.state_out ? a.state_out : a.state;
+    float x1 = si[state_index(0, slot, nb)], x2 = si[state_index(1, slot, nb)];
     for (uint32_t q = 0; q < a.nsec; ++q, kc += 5) {
-        const float y1 = st[state_index(2 * q + 2, slot, nb)], y2 = st[state_index(2 * q + 3, slot, nb)];
+        const float y1 = si[state_index(2 * q + 2, slot, nb)], y2 = si[state_index(2 * q + 3, slot, nb)];
         float y = __fmaf_rn(__ldg(kc), in, __fmul_rn(__ldg(kc + 1), x1));
         y = __fmaf_rn(__ldg(kc + 2), x2, y);
         y = __fmaf_rn(-__ldg(kc + 3), y1, y);
