@@ -59,6 +59,53 @@ struct AdjArgs {
 
 constexpr int AB = 256;
 
+// The shuffle schedule of peer_sum for one lane, worked out once and used
+// for every sum of a slot: in round r the lane takes the value of lane
+// src[r] and adds it when bit r of `use` is set; `rounds` (at most five,
+// for a group of 32) is the same on every lane.
+struct PeerPlan {
+    int src[5];
+    unsigned use;
+    int rounds;
+};
+
+__device__ __forceinline__ PeerPlan peer_plan(unsigned peers)
+{
+    PeerPlan p;
+    p.use = 0u;
+    p.rounds = 0;
+    const int lane = (int)(threadIdx.x & 31u);
+    unsigned rank = __popc(peers & ((1u << lane) - 1u));
+    peers &= 0xfffffffeu << lane;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        p.src[r] = lane;
+        if (__any_sync(0xffffffffu, peers != 0u)) {
+            const int next = __ffs(peers);
+            if (next > 0) {
+                p.src[r] = next - 1;
+                p.use |= 1u << r;
+            }
+            peers &= __ballot_sync(0xffffffffu, (rank & 1u) == 0u);
+            rank >>= 1;
+            p.rounds = r + 1;
+        }
+    }
+    return p;
+}
+
+// peer_sum with a schedule from peer_plan
+__device__ __forceinline__ double plan_sum(const PeerPlan &p, double v)
+{
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+        if (r < p.rounds) {
+            const double u = __shfl_sync(0xffffffffu, v, p.src[r]);
+            if ((p.use >> r) & 1u) v += u;
+        }
+    return v;
+}
+
 // The sum of v over the lanes of a full warp that share this lane's key
 // (peers = __match_any_sync of the key), complete at the group's lowest
 // lane: a tree over each group's ranks, every lane taking part in every
@@ -168,16 +215,18 @@ __global__ void __launch_bounds__(AB) k_adj_boundary(const AdjArgs a)
         if (gsm[k] != 0.0) atomicAdd(a.grad + k, gsm[k]);
 }
 
+constexpr int ABS = 128; // threads per block of k_adj_boundary_s: a few slots per SM at small sizes still fill it
+
 // The same for cascades of up to MAXS sections, unrolled: the forward
 // section inputs and the filter states stay in registers (the states are
 // read once, as the 16-byte groups of the cascade's layout).
-template <int MAXS> __global__ void __launch_bounds__(AB) k_adj_boundary_s(const AdjArgs a)
+template <int MAXS> __global__ void __launch_bounds__(ABS) k_adj_boundary_s(const AdjArgs a)
 {
     constexpr int NG = (2 * (MAXS + 1) + 3) / 4;
     extern __shared__ double gsm[]; // block partial sums of the coefficient gradients
-    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB) gsm[k] = 0.0;
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += ABS) gsm[k] = 0.0;
     __syncthreads();
-    const uint64_t b = (uint64_t)blockIdx.x * AB + threadIdx.x;
+    const uint64_t b = (uint64_t)blockIdx.x * ABS + threadIdx.x;
     if (b < a.nb) {
         const uint32_t ref = a.bidx[b];
         const uint32_t S = a.nsec, m = a.bmat[b];
@@ -227,6 +276,7 @@ template <int MAXS> __global__ void __launch_bounds__(AB) k_adj_boundary_s(const
         const bool full = __activemask() == 0xffffffffu;
         const unsigned peers = full ? __match_any_sync(0xffffffffu, m) : 0u;
         const bool lead = full && (int)(threadIdx.x & 31u) == __ffs(peers) - 1;
+        const PeerPlan plan = full ? peer_plan(peers) : PeerPlan{};
         double yb = ybar;
 #pragma unroll
         for (int q = MAXS - 1; q >= 0; --q)
@@ -242,7 +292,7 @@ template <int MAXS> __global__ void __launch_bounds__(AB) k_adj_boundary_s(const
                 if (full) {
 #pragma unroll
                     for (int j = 0; j < 5; ++j) {
-                        const double v = peer_sum(peers, gv[j]);
+                        const double v = plan_sum(plan, gv[j]);
                         if (lead) atomicAdd(g + j, v);
                     }
                 } else {
@@ -266,7 +316,7 @@ template <int MAXS> __global__ void __launch_bounds__(AB) k_adj_boundary_s(const
         a.cq[b] = (float)cqv;
     }
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < a.ncoef; k += AB)
+    for (uint32_t k = threadIdx.x; k < a.ncoef; k += ABS)
         if (gsm[k] != 0.0) atomicAdd(a.grad + k, gsm[k]);
 }
 
@@ -304,11 +354,11 @@ cudaError_t launch_adj_boundary(float *T, const uint32_t *bidx, const uint8_t *b
     AdjArgs a{T, bidx, bmat, bw, coef, rec, fst, ast, dbar, cq, grad, nb, nx, ny, px, nsec, nmat * nsec * 5, form,
               K, mix_y, mix_d, gain};
     const size_t sm = (size_t)a.ncoef * sizeof(double);
-    const unsigned g = (unsigned)((nb + AB - 1) / AB);
-    if (nsec <= 1) k_adj_boundary_s<1><<<g, AB, sm, s>>>(a);
-    else if (nsec == 2) k_adj_boundary_s<2><<<g, AB, sm, s>>>(a);
-    else if (nsec <= 4) k_adj_boundary_s<4><<<g, AB, sm, s>>>(a);
-    else k_adj_boundary<<<g, AB, sm, s>>>(a);
+    const unsigned gs = (unsigned)((nb + ABS - 1) / ABS);
+    if (nsec <= 1) k_adj_boundary_s<1><<<gs, ABS, sm, s>>>(a);
+    else if (nsec == 2) k_adj_boundary_s<2><<<gs, ABS, sm, s>>>(a);
+    else if (nsec <= 4) k_adj_boundary_s<4><<<gs, ABS, sm, s>>>(a);
+    else k_adj_boundary<<<(unsigned)((nb + AB - 1) / AB), AB, sm, s>>>(a);
     return cudaGetLastError();
 }
 
