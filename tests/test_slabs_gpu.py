@@ -237,17 +237,21 @@ def test_slab_run_thin_slabs_match_whole_grid(parts):
     whole.close()
 
 
-@pytest.mark.parametrize("nparts,storage", [(2, capi.STORAGE_F32), (3, capi.STORAGE_BF16)])
-def test_split_slab_step_matches_whole_grid(nparts, storage):
+@pytest.mark.parametrize("nparts,storage,rounding", [(2, capi.STORAGE_F32, capi.ROUND_NEAREST),
+                                                    (3, capi.STORAGE_BF16, capi.ROUND_NEAREST),
+                                                    (2, capi.STORAGE_F16, capi.ROUND_STOCHASTIC)])
+def test_split_slab_step_matches_whole_grid(nparts, storage, rounding):
     """virs_slab_step_begin / virs_slab_step_end with the ghost planes
     exchanged between the two parts (the form a multi-process host uses,
     here with device copies in one process): the interior launches of
     every slab run on a side stream while the copies run on the main one;
-    receivers and owned planes equal the whole grid's bit for bit."""
+    receivers and owned planes equal the whole grid's bit for bit (with
+    stochastic rounding too: a slab's voxels take the whole grid's keys)."""
     import torch
     sc = _scene(150)
     scale = 64.0 if storage else 0.0
     whole, meta = scenes.build_simulation(sc, storage=storage, storage_scale=scale)
+    whole.set_rounding(rounding)
     nx, ny, _ = meta["shape"]
     plane = nx * ny
     whole.run(sc.steps)
@@ -255,6 +259,8 @@ def test_split_slab_step_matches_whole_grid(nparts, storage):
     want_p, want_pp = whole.pressure(prev=True)
     parts, _ = scenes.build_slabs(sc, nparts, storage=storage, storage_scale=scale)
     sims = [p[0] for p in parts]
+    for s in sims:
+        s.set_rounding(rounding)
     main = torch.cuda.current_stream()
     side = torch.cuda.Stream()
     for _ in range(sc.steps):
