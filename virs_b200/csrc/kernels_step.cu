@@ -314,28 +314,53 @@ __global__ void __launch_bounds__(BT) k_boundary_fix(const __grid_constant__ Ste
     fix_store<T>(a, v);
 }
 
-// batched: thread g belongs to the last member whose first boundary index
-// is <= g (members without boundary voxels are skipped by that rule); the
-// members' first indices are searched in shared memory
+// batched: slot g belongs to the last member whose first boundary index is
+// <= g (members without boundary voxels are skipped by that rule).  A
+// block's 256 slots nearly always belong to one member: two threads find
+// the members of the block's first and last slot (binary searches over the
+// members' first indices), and when they agree the block copies that
+// member's step arguments into shared memory once, so that no thread
+// searches or reads its arguments from the descriptor array; a block that
+// straddles members searches per thread between the two.
+__device__ __forceinline__ uint32_t batch_member_of(const BatchMember *__restrict mem, uint32_t lo, uint32_t hi,
+                                                    uint64_t g)
+{
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) / 2;
+        if (mem[mid].first_bnd <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename T, int MAXS>
 __global__ void __launch_bounds__(256) k_boundary_batch(const BatchMember *__restrict mem, uint32_t nmem,
                                                         uint64_t ntotal, int parity)
 {
-    constexpr uint32_t CACHE = 1024;
-    __shared__ uint64_t first[CACHE];
-    const bool cached = nmem <= CACHE;
-    if (cached)
-        for (uint32_t m = threadIdx.x; m < nmem; m += blockDim.x) first[m] = mem[m].first_bnd;
-    __syncthreads();
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ntotal) return;
-    uint32_t lo = 0, hi = nmem - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) / 2;
-        if ((cached ? first[mid] : mem[mid].first_bnd) <= g) lo = mid;
-        else hi = mid - 1;
+    __shared__ StepArgs sa;
+    __shared__ uint32_t sm[2];
+    __shared__ uint64_t sfirst;
+    const uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x, g = g0 + threadIdx.x;
+    if (threadIdx.x < 2) {
+        const uint64_t last = min(g0 + blockDim.x, ntotal) - 1;
+        sm[threadIdx.x] = batch_member_of(mem, 0, nmem - 1, threadIdx.x == 0 ? g0 : last);
     }
-    const BatchMember &b = mem[lo];
+    __syncthreads();
+    const uint32_t m0 = sm[0], m1 = sm[1];
+    if (m0 == m1) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(&mem[m0].step[parity]);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&sa);
+        for (uint32_t k = threadIdx.x; k < (uint32_t)(sizeof(StepArgs) / 4); k += blockDim.x) dst[k] = src[k];
+        if (threadIdx.x == 0) sfirst = mem[m0].first_bnd;
+        __syncthreads();
+        if (g >= ntotal) return;
+        BVox<T, MAXS> v;
+        bvox_load<T, BND_UPDATE, MAXS>(sa, g - sfirst, v);
+        bvox_update<T, BND_UPDATE, MAXS>(sa, g - sfirst, v);
+        return;
+    }
+    if (g >= ntotal) return;
+    const BatchMember &b = mem[batch_member_of(mem, m0, m1, g)];
     BVox<T, MAXS> v;
     bvox_load<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
     bvox_update<T, BND_UPDATE, MAXS>(b.step[parity], g - b.first_bnd, v);
